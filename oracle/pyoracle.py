@@ -1,0 +1,114 @@
+"""ctypes bindings of the CPU oracle (test infrastructure only).
+
+Two libraries with the same flat-array conventions:
+  * ``liboracle.so``      -- this project's restatement (oracle_capi.cpp);
+  * ``_ref/libphcref.so`` -- PHCpack's own host code behind ref_harness.cpp,
+    present only where it was built from the reference tree.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libphcref.so")
+REF_TREE = os.environ.get("PHC_REFERENCE_GPU", "/root/reference/src/GPU")
+
+_D = ctypes.POINTER(ctypes.c_double)
+_I = ctypes.POINTER(ctypes.c_int)
+
+
+def build(ref: bool = True) -> None:
+    """Compile liboracle.so, and _ref/libphcref.so where the reference tree
+    exists."""
+    targets = ["liboracle.so"]
+    if ref and os.path.isdir(REF_TREE):
+        targets.append("_ref/libphcref.so")
+    subprocess.run(["make", "-s", "-C", HERE, f"REF={REF_TREE}"] + targets, check=True)
+
+
+def _dp(a):
+    return a.ctypes.data_as(_D)
+
+
+def _ip(a):
+    return a.ctypes.data_as(_I)
+
+
+class Lib:
+    def __init__(self, path: str, prefix: str):
+        self.lib = ctypes.CDLL(path)
+        self.prefix = prefix
+
+    def _fn(self, name):
+        f = getattr(self.lib, f"{self.prefix}_{name}")
+        f.restype = ctypes.c_int
+        return f
+
+    def system_evaldiff(self, b) -> np.ndarray:
+        out = np.zeros(b.output_size())
+        rc = self._fn("system_evaldiff")(
+            b.prec, int(b.cplx), b.nsys, b.dim, b.deg, b.maxvar, _ip(b.mon_off), _ip(b.nvr), _ip(b.idx),
+            _ip(b.exps), _dp(b.cst), _dp(b.cff), _dp(b.input), _dp(out))
+        assert rc == 0
+        return out
+
+    def blocked_houseqr(self, prec, cplx, nrows, ncols, szt, nbt, A):
+        W = prec * (2 if cplx else 1)
+        A = np.ascontiguousarray(A, dtype=np.float64)
+        Q = np.zeros(nrows * nrows * W)
+        R = np.zeros(nrows * ncols * W)
+        rc = self._fn("blocked_houseqr")(prec, int(cplx), nrows, ncols, szt, nbt, _dp(A), _dp(Q), _dp(R))
+        assert rc == 0
+        return Q, R
+
+    def upper_tiled_solver(self, prec, cplx, dim, szt, nbt, U, b):
+        W = prec * (2 if cplx else 1)
+        U = np.array(U, dtype=np.float64, copy=True)
+        b = np.array(b, dtype=np.float64, copy=True)
+        x = np.zeros(dim * W)
+        rc = self._fn("upper_tiled_solver")(prec, int(cplx), dim, szt, nbt, _dp(U), _dp(b), _dp(x))
+        assert rc == 0
+        return x, U, b
+
+    def bals_solve(self, prec, cplx, dim, degp1, tailidx, mat, rhs, flags=(1, 0, 0, 0, 1)):
+        W = prec * (2 if cplx else 1)
+        mat = np.ascontiguousarray(mat, dtype=np.float64)
+        rhs = np.array(rhs, dtype=np.float64, copy=True)
+        sol = np.zeros(degp1 * dim * W)
+        Q = np.zeros(dim * dim * W)
+        R = np.zeros(dim * dim * W)
+        fl = np.array(flags, dtype=np.int32)
+        rc = self._fn("bals_solve")(prec, int(cplx), dim, degp1, tailidx, _dp(mat), _dp(rhs), _dp(sol), _dp(Q),
+                                    _dp(R), _ip(fl))
+        assert rc == 0
+        return sol, rhs, Q, R, fl
+
+
+_oracle = None
+_ref = None
+
+
+def oracle() -> Lib:
+    global _oracle
+    if _oracle is None:
+        if not os.path.exists(ORACLE_SO):
+            build(ref=False)
+        _oracle = Lib(ORACLE_SO, "orc")
+    return _oracle
+
+
+def reference() -> Lib | None:
+    """PHCpack's own host code, or None where it was never built."""
+    global _ref
+    if _ref is None:
+        if not os.path.exists(REF_SO) and os.path.isdir(REF_TREE):
+            build(ref=True)
+        if not os.path.exists(REF_SO):
+            return None
+        _ref = Lib(REF_SO, "ref")
+    return _ref
