@@ -1,0 +1,274 @@
+"""Workloads of bench.py: seeded synthetic inputs built on the device, one
+timed step per batch, the end-to-end host path, and the CPU baseline.
+
+The CPU baseline runs the reference's own host code (oracle/_ref, the
+reference sources compiled in place) where that library exists, else the
+oracle restatement; both are test infrastructure and are only timed here,
+never used by the measured GPU path.
+"""
+from __future__ import annotations
+
+import os
+import platform
+import threading
+import time
+
+import numpy as np
+
+from . import _lib
+from . import workloads as wl
+
+# The reference's cost convention for multiple-double operations
+# (Matrices/write_dbl2_qrtimeflops.cpp:51-61, write_dbl4_bstimeflops.cpp:31-61):
+# double-double add 20 flops, mul 23; quad-double add 89, mul 336; a complex
+# product costs four real ones (Newton/dbl2_systems_kernels.cu:29-37).
+MD_ADD = {1: 1, 2: 20, 4: 89}
+MD_MUL = {1: 1, 2: 23, 4: 336}
+
+
+def conv_flops(deg, prec, cplx):
+    n1 = deg + 1
+    muls = n1 * (n1 + 1) // 2
+    adds = deg * n1 // 2
+    f = muls * MD_MUL[prec] + adds * MD_ADD[prec]
+    return 4 * f if cplx else f
+
+
+def evaldiff_counts(nvr, exps):
+    """(convolutions, series additions) of the common-factor + forward /
+    backward / cross evaluation of each monomial."""
+    nvr = np.asarray(nvr)
+    excess = np.clip(np.asarray(exps) - 1, 0, None).sum(axis=1)
+    speel = np.where(nvr == 1, 1, np.where(nvr == 2, 3, 3 * nvr - 3))
+    return int((excess + speel).sum()), int((nvr + 1).sum())
+
+
+def cpu_info():
+    model = platform.processor() or ""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    model = ln.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return model, os.cpu_count() or 1
+
+
+# --------------------------------------------------------------- eval
+def config2_device(torch, dev, nsys=4096, dim=32, deg=31, nmon=32, maxvar=4, expmax=3, seed=2):
+    """The 4096-system complex double-double eval/diff workload, generated on
+    the device with a seeded torch generator (same distributions as
+    workloads.eval_batch)."""
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    n1 = deg + 1
+    total = nsys * dim * nmon
+    nvr = torch.randint(1, maxvar + 1, (total,), generator=g, device=dev, dtype=torch.int32)
+    idx = torch.empty((total, maxvar), dtype=torch.int32, device=dev)
+    chunk = 1 << 18
+    for c0 in range(0, total, chunk):
+        c1 = min(total, c0 + chunk)
+        r = torch.rand((c1 - c0, dim), generator=g, device=dev)
+        pick = torch.argsort(r, dim=1)[:, :maxvar].to(torch.int32)
+        k = nvr[c0:c1].unsqueeze(1)
+        col = torch.arange(maxvar, device=dev).unsqueeze(0)
+        big = torch.where(col < k, pick, torch.full_like(pick, 1 << 20))
+        srt = torch.sort(big, dim=1).values
+        idx[c0:c1] = torch.where(col < k, srt, torch.zeros_like(srt))
+    exps = torch.randint(1, expmax + 1, (total, maxvar), generator=g, device=dev, dtype=torch.int32)
+    col = torch.arange(maxvar, device=dev).unsqueeze(0)
+    exps = torch.where(col < nvr.unsqueeze(1), exps, torch.zeros_like(exps))
+    mon_off = torch.arange(0, total + 1, nmon, dtype=torch.int32, device=dev)
+
+    def dd_pair(hi):
+        lo = hi * (2.0 ** -53) * (torch.rand(hi.shape, generator=g, device=dev, dtype=torch.float64) * 2 - 1)
+        s = hi + lo
+        e = lo - (s - hi)
+        return torch.stack([s, e], dim=-1)
+
+    def unit(shape):
+        th = torch.rand(shape, generator=g, device=dev, dtype=torch.float64) * (2 * np.pi)
+        return torch.cat([dd_pair(torch.cos(th)), dd_pair(torch.sin(th))], dim=-1).reshape(-1)
+
+    cff = unit((total, n1))
+    cst = unit((nsys * dim, n1))
+    scale = (2.0 ** -torch.arange(n1, device=dev, dtype=torch.float64))
+    re = torch.randn((nsys * dim, n1), generator=g, device=dev, dtype=torch.float64) * scale
+    im = torch.randn((nsys * dim, n1), generator=g, device=dev, dtype=torch.float64) * scale
+    inp = torch.cat([dd_pair(re), dd_pair(im)], dim=-1).reshape(-1)
+    return dict(nsys=nsys, dim=dim, deg=deg, maxvar=maxvar, prec=2, cplx=True, mon_off=mon_off, nvr=nvr, idx=idx,
+                exps=exps, cst=cst, cff=cff, input=inp)
+
+
+class EvalWork:
+    metric = "systems/s, batched eval/diff of polynomial systems at power series (complex double-double)"
+    unit = "systems/s"
+    dtype = "f64 (complex double-double limbs)"
+    kernel_tag = "k_system_evaldiff_config2"
+    l2_note = None
+    dominant_launches_per_step = 1
+
+    def __init__(self, torch, dev, rank):
+        self.torch = torch
+        d = config2_device(torch, dev, seed=2 + rank)
+        self.d = d
+        S = (d["deg"] + 1) * 4
+        self.out = torch.empty(d["nsys"] * d["dim"] * (d["dim"] + 1) * S, dtype=torch.float64, device=dev)
+        self.units_per_step = d["nsys"]
+        nconv, nadd = evaldiff_counts(d["nvr"].cpu().numpy(), d["exps"].cpu().numpy())
+        self.dominant_flops_per_launch = float(nconv * conv_flops(d["deg"], 2, True)
+                                               + nadd * (d["deg"] + 1) * 2 * MD_ADD[2])
+        in_bytes = (d["cff"].numel() + d["cst"].numel() + d["input"].numel()) * 8
+        self.dominant_bytes_per_launch = float(in_bytes + self.out.numel() * 8)
+        self.flops_note = ("reference op weights: dd add 20, mul 23, complex x4 per convolution; "
+                           f"{nconv} convolutions of degree {d['deg']} per step")
+        self.config = {"workload": "eval/diff: 4096 systems, n=32, 32 monomials/polynomial over <=4 variables, "
+                                   "exponents {1,2,3}, unit-circle coefficients, degree 31, complex dd",
+                       "systems": d["nsys"], "dim": d["dim"], "degree": d["deg"]}
+        self.host = None
+
+    def _args(self, stream_ptr, out_ptr, host=None):
+        d = self.d
+        src = host if host is not None else d
+        return (d["prec"], 1, d["nsys"], d["dim"], d["deg"], d["maxvar"], _lib.ptr(src["mon_off"]),
+                _lib.ptr(src["nvr"]), _lib.ptr(src["idx"]), _lib.ptr(src["exps"]), _lib.ptr(src["cst"]),
+                _lib.ptr(src["cff"]), _lib.ptr(src["input"]), _lib.ptr(out_ptr), _lib.c_void_p(stream_ptr))
+
+    def step(self, stream):
+        _lib.call("phc_system_evaldiff", *self._args(stream.cuda_stream, self.out))
+        return 1
+
+    def e2e(self, stream, reps=2):
+        torch = self.torch
+        if self.host is None:
+            self.host = {k: (v.cpu().pin_memory() if hasattr(v, "cpu") else v) for k, v in self.d.items()}
+            self.host_out = torch.empty(self.out.numel(), dtype=torch.float64).pin_memory()
+        times = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            _lib.call("phc_system_evaldiff_host", *self._args(stream.cuda_stream, self.host_out, self.host))
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1) / 1e3)
+        t = float(np.median(times))
+        h2d = sum(v.numel() * v.element_size() for v in self.host.values() if hasattr(v, "numel"))
+        return {"value": self.units_per_step / t, "unit": self.unit, "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(self.host_out.numel() * 8), "path": "phc_system_evaldiff_host"}
+
+    def check(self):
+        """Spot check of the timed output against the oracle on 2 systems."""
+        try:
+            from oracle import pyoracle
+            sb = self.sample_batch(2)
+            ref = pyoracle.oracle().system_evaldiff(sb)
+            S = (sb.deg + 1) * 4
+            got = self.out[: 2 * sb.dim * (sb.dim + 1) * S].cpu().numpy()
+            err = np.abs(got.reshape(-1, 4)[:, 0] - ref.reshape(-1, 4)[:, 0]).max()
+            return {"oracle_systems": 2, "max_abs_hi_diff": float(err)}
+        except Exception as e:  # the check never decides the number
+            return {"error": str(e)[:200]}
+
+    def sample_batch(self, n):
+        d = self.d
+        S = (d["deg"] + 1) * 4
+        m = n * d["dim"] * 32
+        g = lambda t, k: t[:k].cpu().numpy()
+        return wl.SystemBatch(n, d["dim"], d["deg"], d["maxvar"], 2, True, g(d["mon_off"], n * d["dim"] + 1),
+                              g(d["nvr"], m), g(d["idx"], m), g(d["exps"], m), g(d["cst"], n * d["dim"] * S),
+                              g(d["cff"], m * S), g(d["input"], n * d["dim"] * S))
+
+
+def make(name, dev, rank):
+    import torch
+    if name == "eval":
+        return EvalWork(torch, dev, rank)
+    if name == "track":
+        from . import trackwork
+        return trackwork.TrackWork(torch, dev, rank)
+    if name == "qr":
+        from . import qrwork
+        return qrwork.QRWork(torch, dev, rank)
+    raise ValueError(name)
+
+
+# ---------------------------------------------------------- CPU baseline
+def _threads_run(fn, nitems, nthreads):
+    """Run fn(i) for i < nitems on nthreads Python threads (ctypes calls
+    release the GIL, so the C code runs in parallel)."""
+    nxt = [0]
+    lock = threading.Lock()
+
+    def worker():
+        while True:
+            with lock:
+                i = nxt[0]
+                nxt[0] += 1
+            if i >= nitems:
+                return
+            fn(i)
+
+    ts = [threading.Thread(target=worker) for _ in range(nthreads)]
+    t0 = time.perf_counter()
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join()
+    return time.perf_counter() - t0
+
+
+def eval_cpu_sample(seconds):
+    from oracle import pyoracle
+    lib = pyoracle.reference()
+    kind = "reference"
+    if lib is None:
+        lib, kind = pyoracle.oracle(), "port"
+    model, cores = cpu_info()
+    one = wl.config2(nsys=1, seed=99)
+    t = time.perf_counter()
+    lib.system_evaldiff(one)
+    t1 = time.perf_counter() - t
+    n = max(cores, int(seconds / max(t1, 1e-6) * cores * 0.8))
+    n = min(n, 64 * cores)
+    batches = [wl.config2(nsys=1, seed=1000 + i) for i in range(min(n, 4 * cores))]
+    el = _threads_run(lambda i: lib.system_evaldiff(batches[i % len(batches)]), n, cores)
+    return {"value": n / el, "unit": "systems/s", "cores": cores, "kind": kind,
+            "sample": f"{n} systems of the 4096-system workload (same shapes, seeded), {cores} threads, "
+                      f"CPU: {model}"}
+
+
+def cpu_baseline(workload, seconds):
+    try:
+        if workload == "eval":
+            return eval_cpu_sample(seconds)
+        if workload == "track":
+            from . import trackwork
+            return trackwork.cpu_sample(seconds)
+        if workload == "qr":
+            from . import qrwork
+            return qrwork.cpu_sample(seconds)
+    except Exception as e:
+        return {"value": None, "error": str(e)[:300]}
+    return None
+
+
+def reference_arm(args):
+    """bench.py --impl reference: the reference's CPU host implementation of
+    the path on this machine's cores, same metric and unit as the GPU arm."""
+    vals = []
+    res = None
+    per = max(2.0, min(20.0, 120.0 / max(1, args.steps + args.warmup)))
+    for k in range(args.warmup + args.steps):
+        res = cpu_baseline(args.workload, per)
+        if k >= args.warmup and res and res.get("value"):
+            vals.append(res["value"])
+    v = float(np.median(vals)) if vals else None
+    names = {"eval": EvalWork.metric, "track": "paths/s", "qr": "instances/s"}
+    unit = res.get("unit") if res else None
+    return {"impl": "reference", "metric": names.get(args.workload), "value": v, "unit": unit,
+            "n_gpus": 0, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "cpu_baseline": dict(res or {}, value=v),
+            "e2e": {"value": v, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "config": {"workload": args.workload}}

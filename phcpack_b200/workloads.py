@@ -109,6 +109,27 @@ class SystemBatch:
     def nmon(self):
         return int(self.mon_off[-1])
 
+    def validate(self):
+        """Raise ValueError on supports a kernel could not evaluate."""
+        npoly = self.nsys * self.dim
+        if self.mon_off.shape != (npoly + 1,) or self.mon_off[0] != 0 or (np.diff(self.mon_off) < 0).any():
+            raise ValueError("mon_off must be nondecreasing with nsys*dim+1 entries starting at 0")
+        nm = self.nmon
+        if self.nvr.shape[0] < nm or self.idx.reshape(-1).shape[0] < nm * self.maxvar:
+            raise ValueError("supports shorter than mon_off[-1] monomials")
+        k = self.nvr[:nm]
+        if (k < 1).any() or (k > self.maxvar).any():
+            raise ValueError("nvr out of [1, maxvar]")
+        idx = self.idx.reshape(-1, self.maxvar)[:nm]
+        ex = self.exps.reshape(-1, self.maxvar)[:nm]
+        used = np.arange(self.maxvar)[None, :] < k[:, None]
+        if ((idx < 0) | (idx >= self.dim))[used].any() or (ex < 1)[used].any():
+            raise ValueError("variable index or exponent out of range")
+        for m in np.nonzero(k > 1)[0][:100000]:
+            if len(set(idx[m, :k[m]].tolist())) != k[m]:
+                raise ValueError(f"monomial {m} repeats a variable (use exponents)")
+        return self
+
     def output_size(self):
         return self.nsys * self.dim * (self.dim + 1) * (self.deg + 1) * self.width
 

@@ -1,0 +1,34 @@
+"""The C-ABI library loads and exports every symbol include/*.h declares
+(no compute call: this runs without a GPU)."""
+import ctypes
+import glob
+import os
+import re
+
+from phcpack_b200 import _lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared():
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        text = open(h).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        for m in re.finditer(r"\b(?:int|void|const char\s*\*|double)\s+\**\s*(phc_\w+|GPU_\w+|gpu\w+)\s*\(", text):
+            names.add(m.group(1))
+    return sorted(names)
+
+
+def test_header_declares_entry_points():
+    assert "phc_system_evaldiff" in declared()
+
+
+def test_library_exports_all_declared_symbols():
+    lib = _lib.lib()
+    missing = [n for n in declared() if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_abi_version():
+    assert _lib.lib().phc_abi_version() == 1
