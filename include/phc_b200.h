@@ -58,6 +58,49 @@ int phc_system_evaldiff_host(int prec, int cplx, int nsys, int dim, int deg, int
                              const int *nvr, const int *idx, const int *exps, const double *cst,
                              const double *cff, const double *input, double *output, void *stream);
 
+/* ---------------------------------------------------------------- Matrices
+ * Batched dense linear algebra, one instance per CTA.  The device entry
+ * points take a workspace of ninst * phc_dense_workspace_bytes(...) bytes
+ * (WY panels, products, inverted diagonal tiles of R).
+ */
+long long phc_dense_workspace_bytes(int prec, int cplx, int n, int szt);
+
+/* A = Q R for ninst matrices A (nrows x ncols, ncols = szt*nbt <= nrows),
+ * Q nrows x nrows, R nrows x ncols.  Replaces Matrices/dbl2_baqr_kernels.h
+ * GPU_dbl2_blocked_houseqr (body at dbl2_baqr_kernels.cu:3520) and its
+ * cmplx2 / dbl4 / cmplx4 twins: Householder reflectors in PHCpack's
+ * convention, applied per column inside a tile, then the WY trailing updates
+ * R += Y (W^H R) and Q += (Q W) Y^H. */
+int phc_blocked_houseqr(int prec, int cplx, int ninst, int nrows, int ncols, int szt, const double *A, double *Q,
+                        double *R, double *work, void *stream);
+int phc_blocked_houseqr_host(int prec, int cplx, int ninst, int nrows, int ncols, int szt, const double *A,
+                             double *Q, double *R, void *stream);
+
+/* x = U^{-1} b for ninst upper triangular U (dim = szt*nbt) by inverting the
+ * diagonal tiles and block back substitution.  Replaces
+ * Matrices/dbl2_tabs_kernels.h GPU_dbl2_upper_tiled_solver (body at
+ * dbl2_tabs_kernels.cu:952); like it, overwrites the diagonal tiles of U
+ * with their inverses and b with the updated right hand sides.  work: dim*szt
+ * numbers per instance. */
+int phc_upper_tiled_solver(int prec, int cplx, int ninst, int dim, int szt, double *U, double *b, double *x,
+                           double *work, void *stream);
+int phc_upper_tiled_solver_host(int prec, int cplx, int ninst, int dim, int szt, double *U, double *b, double *x,
+                                void *stream);
+
+/* ------------------------------------------------------------------ Newton
+ * Block lower-triangular Toeplitz least squares sum_{j<=k} A_j x_{k-j} = b_k,
+ * k < degp1, for ninst instances (mat: degp1 matrices dim x dim; rhs, sol:
+ * degp1 vectors of dim; Q, R: dim x dim).  Replaces
+ * Newton/dbl2_bals_kernels.cu:554 GPU_dbl2_bals_solve (head :108, tail
+ * dbl2_tail_kernels.cu:154) and twins, with the reference's skip rules.
+ * flags: 5 ints per instance, in/out: zeroQ, noqr, upidx, bsidx, newtail.
+ * tailidx >= 1 starts the tail there for every instance; tailidx < 0 takes
+ * each instance's flags[4].  rhs is overwritten. */
+int phc_bals_solve(int prec, int cplx, int ninst, int dim, int degp1, int szt, int tailidx, const double *mat,
+                   double *rhs, double *sol, double *Q, double *R, int *flags, double *work, void *stream);
+int phc_bals_solve_host(int prec, int cplx, int ninst, int dim, int degp1, int szt, int tailidx, const double *mat,
+                        double *rhs, double *sol, double *Q, double *R, int *flags, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

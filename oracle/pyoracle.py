@@ -75,13 +75,13 @@ class Lib:
         assert rc == 0
         return x, U, b
 
-    def bals_solve(self, prec, cplx, dim, degp1, tailidx, mat, rhs, flags=(1, 0, 0, 0, 1)):
+    def bals_solve(self, prec, cplx, dim, degp1, tailidx, mat, rhs, flags=(1, 0, 0, 0, 1), Q=None, R=None):
         W = prec * (2 if cplx else 1)
         mat = np.ascontiguousarray(mat, dtype=np.float64)
         rhs = np.array(rhs, dtype=np.float64, copy=True)
         sol = np.zeros(degp1 * dim * W)
-        Q = np.zeros(dim * dim * W)
-        R = np.zeros(dim * dim * W)
+        Q = np.zeros(dim * dim * W) if Q is None else np.array(Q, dtype=np.float64, copy=True)
+        R = np.zeros(dim * dim * W) if R is None else np.array(R, dtype=np.float64, copy=True)
         fl = np.array(flags, dtype=np.int32)
         rc = self._fn("bals_solve")(prec, int(cplx), dim, degp1, tailidx, _dp(mat), _dp(rhs), _dp(sol), _dp(Q),
                                     _dp(R), _ip(fl))

@@ -110,9 +110,9 @@ class EvalWork:
     l2_note = None
     dominant_launches_per_step = 1
 
-    def __init__(self, torch, dev, rank):
+    def __init__(self, torch, dev, rank, nsys=4096):
         self.torch = torch
-        d = config2_device(torch, dev, seed=2 + rank)
+        d = config2_device(torch, dev, nsys=nsys, seed=2 + rank)
         self.d = d
         S = (d["deg"] + 1) * 4
         self.out = torch.empty(d["nsys"] * d["dim"] * (d["dim"] + 1) * S, dtype=torch.float64, device=dev)

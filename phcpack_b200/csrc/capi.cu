@@ -27,6 +27,14 @@ int system_evaldiff(int prec, int cplx, int nsys, int dim, int deg, int maxvar, 
                     const int *idx, const int *exps, const double *cst, const double *cff, const double *input,
                     double *output, cudaStream_t stream);
 
+long dense_work_doubles(int prec, int cplx, int n, int szt);
+int blocked_houseqr(int prec, int cplx, int ninst, int n, int ncols, int szt, const double *A, double *Q, double *R,
+                    double *work, cudaStream_t st);
+int upper_tiled_solver(int prec, int cplx, int ninst, int dim, int szt, double *U, double *b, double *x, double *work,
+                       cudaStream_t st);
+int bals_solve(int prec, int cplx, int ninst, int n, int degp1, int szt, int tailidx, const double *mat, double *rhs,
+               double *sol, double *Q, double *R, int *flags, double *work, cudaStream_t st);
+
 // device scratch owned for the duration of one host call
 struct dbuf {
   void *p = nullptr;
@@ -99,6 +107,130 @@ int phc_system_evaldiff_host(int prec, int cplx, int nsys, int dim, int deg, int
   rc = system_evaldiff(prec, cplx, nsys, dim, deg, maxvar, d_off, d_nvr, d_idx, d_exp, d_cst, d_cff, d_in, d_out, st);
   if (rc) return rc;
   PHC_CUDA(cudaMemcpyAsync(output, d_out, b_out, cudaMemcpyDeviceToHost, st));
+  PHC_CUDA(cudaStreamSynchronize(st));
+  return PHC_OK;
+}
+
+long long phc_dense_workspace_bytes(int prec, int cplx, int n, int szt) {
+  if (!prec_ok(prec) || n < 1 || szt < 1) return -1;
+  return (long long)dense_work_doubles(prec, cplx, n, szt) * (long long)sizeof(double);
+}
+
+int phc_blocked_houseqr(int prec, int cplx, int ninst, int nrows, int ncols, int szt, const double *A, double *Q,
+                        double *R, double *work, void *stream) {
+  return blocked_houseqr(prec, cplx, ninst, nrows, ncols, szt, A, Q, R, work, (cudaStream_t)stream);
+}
+
+int phc_upper_tiled_solver(int prec, int cplx, int ninst, int dim, int szt, double *U, double *b, double *x,
+                           double *work, void *stream) {
+  return upper_tiled_solver(prec, cplx, ninst, dim, szt, U, b, x, work, (cudaStream_t)stream);
+}
+
+int phc_bals_solve(int prec, int cplx, int ninst, int dim, int degp1, int szt, int tailidx, const double *mat,
+                   double *rhs, double *sol, double *Q, double *R, int *flags, double *work, void *stream) {
+  return bals_solve(prec, cplx, ninst, dim, degp1, szt, tailidx, mat, rhs, sol, Q, R, flags, work,
+                    (cudaStream_t)stream);
+}
+
+}  // extern "C"
+
+// ---- host-buffer variants: stage, run, copy back, synchronise
+namespace {
+struct staged {
+  dbuf buf;
+  char *p = nullptr;
+  size_t used = 0, cap = 0;
+  int alloc(size_t n) {
+    cap = n;
+    int rc = buf.alloc(n);
+    p = (char *)buf.p;
+    return rc;
+  }
+  template <class X> X *take(size_t count) {
+    size_t b = (count * sizeof(X) + 255) & ~size_t(255);
+    X *r = (X *)(p + used);
+    used += b;
+    return r;
+  }
+};
+inline size_t al(size_t n) { return (n + 255) & ~size_t(255); }
+}  // namespace
+
+extern "C" {
+
+int phc_blocked_houseqr_host(int prec, int cplx, int ninst, int nrows, int ncols, int szt, const double *A,
+                             double *Q, double *R, void *stream) {
+  PHC_REQUIRE(prec_ok(prec) && ninst >= 0 && nrows >= 1 && szt >= 1, "blocked_houseqr_host: bad sizes");
+  if (ninst == 0) return PHC_OK;
+  const size_t W = width_of(prec, cplx);
+  const size_t nA = (size_t)ninst * nrows * ncols * W, nQ = (size_t)ninst * nrows * nrows * W;
+  const size_t nw = (size_t)ninst * dense_work_doubles(prec, cplx, nrows, szt);
+  staged s;
+  int rc = s.alloc(al(nA * 8) + al(nQ * 8) + al(nA * 8) + al(nw * 8));
+  if (rc) return rc;
+  double *dA = s.take<double>(nA), *dQ = s.take<double>(nQ), *dR = s.take<double>(nA), *dW = s.take<double>(nw);
+  cudaStream_t st = (cudaStream_t)stream;
+  PHC_CUDA(cudaMemcpyAsync(dA, A, nA * 8, cudaMemcpyHostToDevice, st));
+  rc = blocked_houseqr(prec, cplx, ninst, nrows, ncols, szt, dA, dQ, dR, dW, st);
+  if (rc) return rc;
+  PHC_CUDA(cudaMemcpyAsync(Q, dQ, nQ * 8, cudaMemcpyDeviceToHost, st));
+  PHC_CUDA(cudaMemcpyAsync(R, dR, nA * 8, cudaMemcpyDeviceToHost, st));
+  PHC_CUDA(cudaStreamSynchronize(st));
+  return PHC_OK;
+}
+
+int phc_upper_tiled_solver_host(int prec, int cplx, int ninst, int dim, int szt, double *U, double *b, double *x,
+                                void *stream) {
+  PHC_REQUIRE(prec_ok(prec) && ninst >= 0 && dim >= 1 && szt >= 1, "upper_tiled_solver_host: bad sizes");
+  if (ninst == 0) return PHC_OK;
+  const size_t W = width_of(prec, cplx);
+  const size_t nU = (size_t)ninst * dim * dim * W, nb = (size_t)ninst * dim * W;
+  const size_t nw = (size_t)ninst * dim * szt * W;
+  staged s;
+  int rc = s.alloc(al(nU * 8) + 2 * al(nb * 8) + al(nw * 8));
+  if (rc) return rc;
+  double *dU = s.take<double>(nU), *db = s.take<double>(nb), *dx = s.take<double>(nb), *dW = s.take<double>(nw);
+  cudaStream_t st = (cudaStream_t)stream;
+  PHC_CUDA(cudaMemcpyAsync(dU, U, nU * 8, cudaMemcpyHostToDevice, st));
+  PHC_CUDA(cudaMemcpyAsync(db, b, nb * 8, cudaMemcpyHostToDevice, st));
+  rc = upper_tiled_solver(prec, cplx, ninst, dim, szt, dU, db, dx, dW, st);
+  if (rc) return rc;
+  PHC_CUDA(cudaMemcpyAsync(U, dU, nU * 8, cudaMemcpyDeviceToHost, st));
+  PHC_CUDA(cudaMemcpyAsync(b, db, nb * 8, cudaMemcpyDeviceToHost, st));
+  PHC_CUDA(cudaMemcpyAsync(x, dx, nb * 8, cudaMemcpyDeviceToHost, st));
+  PHC_CUDA(cudaStreamSynchronize(st));
+  return PHC_OK;
+}
+
+int phc_bals_solve_host(int prec, int cplx, int ninst, int dim, int degp1, int szt, int tailidx, const double *mat,
+                        double *rhs, double *sol, double *Q, double *R, int *flags, void *stream) {
+  PHC_REQUIRE(prec_ok(prec) && ninst >= 0 && dim >= 1 && szt >= 1 && degp1 >= 1, "bals_solve_host: bad sizes");
+  if (ninst == 0) return PHC_OK;
+  const size_t W = width_of(prec, cplx);
+  const size_t nm = (size_t)ninst * degp1 * dim * dim * W, nb = (size_t)ninst * degp1 * dim * W;
+  const size_t nq = (size_t)ninst * dim * dim * W, nf = (size_t)ninst * 5;
+  const size_t nw = (size_t)ninst * dense_work_doubles(prec, cplx, dim, szt);
+  staged s;
+  int rc = s.alloc(al(nm * 8) + 2 * al(nb * 8) + 2 * al(nq * 8) + al(nf * 4) + al(nw * 8));
+  if (rc) return rc;
+  double *dm = s.take<double>(nm), *db = s.take<double>(nb), *dx = s.take<double>(nb);
+  double *dQ = s.take<double>(nq), *dR = s.take<double>(nq);
+  int *df = s.take<int>(nf);
+  double *dW = s.take<double>(nw);
+  cudaStream_t st = (cudaStream_t)stream;
+  PHC_CUDA(cudaMemcpyAsync(dm, mat, nm * 8, cudaMemcpyHostToDevice, st));
+  PHC_CUDA(cudaMemcpyAsync(db, rhs, nb * 8, cudaMemcpyHostToDevice, st));
+  PHC_CUDA(cudaMemcpyAsync(dx, sol, nb * 8, cudaMemcpyHostToDevice, st));
+  PHC_CUDA(cudaMemcpyAsync(dQ, Q, nq * 8, cudaMemcpyHostToDevice, st));
+  PHC_CUDA(cudaMemcpyAsync(dR, R, nq * 8, cudaMemcpyHostToDevice, st));
+  PHC_CUDA(cudaMemcpyAsync(df, flags, nf * 4, cudaMemcpyHostToDevice, st));
+  rc = bals_solve(prec, cplx, ninst, dim, degp1, szt, tailidx, dm, db, dx, dQ, dR, df, dW, st);
+  if (rc) return rc;
+  PHC_CUDA(cudaMemcpyAsync(rhs, db, nb * 8, cudaMemcpyDeviceToHost, st));
+  PHC_CUDA(cudaMemcpyAsync(sol, dx, nb * 8, cudaMemcpyDeviceToHost, st));
+  PHC_CUDA(cudaMemcpyAsync(Q, dQ, nq * 8, cudaMemcpyDeviceToHost, st));
+  PHC_CUDA(cudaMemcpyAsync(R, dR, nq * 8, cudaMemcpyDeviceToHost, st));
+  PHC_CUDA(cudaMemcpyAsync(flags, df, nf * 4, cudaMemcpyDeviceToHost, st));
   PHC_CUDA(cudaStreamSynchronize(st));
   return PHC_OK;
 }

@@ -1,0 +1,213 @@
+// dense.cu -- batched kernels of the Matrices and Newton layers: blocked
+// Householder QR, tiled back substitution and the block-Toeplitz least
+// squares solve, one CTA per instance.
+#include "common.cuh"
+#include "dense.cuh"
+
+namespace phc {
+
+static const int kDenseThreads = 256;
+
+template <class N>
+__global__ void __launch_bounds__(kDenseThreads)
+    k_blocked_houseqr(int n, int ncols, int szt, const double *__restrict__ A, double *__restrict__ Q,
+                      double *__restrict__ Rm, double *__restrict__ work) {
+  extern __shared__ __align__(16) double sm[];
+  const int W = N::width;
+  const long inst = blockIdx.x;
+  dense_smem S = carve<N>(sm, n, szt);
+  const double *a = A + inst * n * ncols * W;
+  double *q = Q + inst * n * n * W;
+  double *r = Rm + inst * n * ncols * W;
+  for (long t = threadIdx.x; t < (long)n * ncols * W; t += blockDim.x) r[t] = a[t];
+  __syncthreads();
+  block_houseqr<N>(n, ncols, szt, q, r, work + inst * dense_work_numbers(n, szt) * W, S);
+}
+
+// Like Matrices/dbl2_tabs_kernels.cu:952 (GPU_dbl2_upper_tiled_solver): b is
+// overwritten by the updated right hand sides and the diagonal tiles of U by
+// their inverses.
+template <class N>
+__global__ void __launch_bounds__(kDenseThreads)
+    k_upper_tiled_solver(int dim, int szt, double *__restrict__ U, double *__restrict__ b, double *__restrict__ x,
+                         double *__restrict__ work) {
+  const int W = N::width;
+  const long inst = blockIdx.x;
+  double *u = U + inst * dim * dim * W;
+  double *bb = b + inst * dim * W;
+  double *xx = x + inst * dim * W;
+  double *tinv = work + inst * (long)dim * szt * W;
+  block_invert_tiles<N>(dim, szt, u, dim, tinv);
+  block_tiled_backsub<N>(dim, szt, u, dim, tinv, bb, xx);
+  const int nbt = dim / szt;
+  for (int t = threadIdx.x; t < nbt * szt * szt; t += blockDim.x) {
+    const int tile = t / (szt * szt), i = (t / szt) % szt, j = t % szt;
+    stn_at<N>(u, (long)(tile * szt + i) * dim + tile * szt + j, ldn_at<N>(tinv, t));
+  }
+}
+
+// Block lower-triangular Toeplitz least squares, one instance per CTA:
+// Newton/dbl2_bals_kernels.cu:554 (GPU_dbl2_bals_solve) with the head at
+// :108 and the tail at dbl2_tail_kernels.cu:154; skip rules of
+// Newton/dbl2_bals_host.cpp:15,228 (no QR when |b_0| < 1e-28 unless zeroQ,
+// no update with a solution block below 1e-28, no back substitution for a
+// right hand side below 1e-28).
+// flags per instance: zeroQ, noqr, upidx, bsidx, newtail; with tailidx < 0
+// the tail starts at the instance's flags[4].
+template <class N>
+__global__ void __launch_bounds__(kDenseThreads)
+    k_bals_solve(int n, int degp1, int szt, int tailidx, const double *__restrict__ mat, double *__restrict__ rhs,
+                 double *__restrict__ sol, double *__restrict__ Q, double *__restrict__ Rm, int *__restrict__ flags,
+                 double *__restrict__ work) {
+  extern __shared__ __align__(16) double sm[];
+  typedef typename N::T T;
+  const int W = N::width;
+  const long inst = blockIdx.x;
+  dense_smem S = carve<N>(sm, n, szt);
+  const long nn = (long)n * n;
+  const double *A = mat + inst * degp1 * nn * W;
+  double *b = rhs + inst * degp1 * n * W;
+  double *x = sol + inst * degp1 * n * W;
+  double *q = Q + inst * nn * W;
+  double *r = Rm + inst * nn * W;
+  int *fl = flags + inst * 5;
+  double *wk = work + inst * dense_work_numbers(n, szt) * W;
+  double *tinv = wk + 4L * n * szt * W;
+  int zeroQ = fl[0], noqr = fl[1];
+  const int tail0 = max(1, tailidx >= 0 ? tailidx : fl[4]);
+  bool tinv_ok = false;
+  if (!(noqr && !zeroQ)) {
+    const double nrm = block_maxnorm<N>(n, b, S.red);
+    if (nrm < 1.0e-28) {
+      noqr = zeroQ ? 0 : 1;
+      if (noqr)
+        for (int i = threadIdx.x; i < n; i += blockDim.x) stn_at<N>(x, i, N::zero());
+    }
+    if (!noqr) {
+      for (long t = threadIdx.x; t < nn * W; t += blockDim.x) r[t] = A[t];
+      __syncthreads();
+      block_houseqr<N>(n, n, szt, q, r, wk, S);
+      zeroQ = 0;
+      block_invert_tiles<N>(n, szt, r, n, tinv);
+      tinv_ok = true;
+      block_qhb<N>(n, q, b, S.w);
+      block_tiled_backsub<N>(n, szt, r, n, tinv, S.w, S.x);
+      for (int i = threadIdx.x; i < n; i += blockDim.x) stn_at<N>(x, i, ldn_at<N>(S.x, i));
+      __syncthreads();
+    }
+  }
+  int up = 0, bs = 0, newtail = tail0;
+  if (degp1 > 1) {
+    if (!tinv_ok) block_invert_tiles<N>(n, szt, r, n, tinv);
+    bool first = true;
+    newtail = degp1;
+    for (int i = tail0; i < degp1; ++i) {
+      const double *xp = x + (long)(i - 1) * n * W;
+      double nrm = block_maxnorm<N>(n, xp, S.red);
+      if (nrm < 1.0e-28) {
+        ++up;
+      } else {
+        for (int l = threadIdx.x; l < n; l += blockDim.x) stn_at<N>(S.x, l, ldn_at<N>(xp, l));
+        __syncthreads();
+        block_tail_update<N>(n, degp1, i, A, b, S.x);
+      }
+      const double *bi = b + (long)i * n * W;
+      nrm = block_maxnorm<N>(n, bi, S.red);
+      double *xi = x + (long)i * n * W;
+      if (nrm < 1.0e-28) {
+        ++bs;
+        for (int l = threadIdx.x; l < n; l += blockDim.x) stn_at<N>(xi, l, N::zero());
+        __syncthreads();
+      } else {
+        if (first) {
+          newtail = i;
+          first = false;
+        }
+        block_qhb<N>(n, q, bi, S.w);
+        block_tiled_backsub<N>(n, szt, r, n, tinv, S.w, S.x);
+        for (int l = threadIdx.x; l < n; l += blockDim.x) stn_at<N>(xi, l, ldn_at<N>(S.x, l));
+        __syncthreads();
+      }
+    }
+  }
+  if (threadIdx.x == 0) {
+    fl[0] = zeroQ;
+    fl[1] = noqr;
+    if (degp1 > 1) {
+      fl[2] = up;
+      fl[3] = bs;
+    }
+    fl[4] = newtail;
+  }
+}
+
+template <class N>
+static int qr_launch(int ninst, int n, int ncols, int szt, const double *A, double *Q, double *R, double *work,
+                     cudaStream_t st) {
+  const long smem = dense_smem_doubles(n, szt, N::width) * sizeof(double);
+  PHC_CUDA(cudaFuncSetAttribute(k_blocked_houseqr<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_blocked_houseqr<N><<<ninst, kDenseThreads, smem, st>>>(n, ncols, szt, A, Q, R, work);
+  PHC_CHECK_LAUNCH();
+  return PHC_OK;
+}
+
+template <class N>
+static int tabs_launch(int ninst, int dim, int szt, double *U, double *b, double *x, double *work, cudaStream_t st) {
+  k_upper_tiled_solver<N><<<ninst, kDenseThreads, 0, st>>>(dim, szt, U, b, x, work);
+  PHC_CHECK_LAUNCH();
+  return PHC_OK;
+}
+
+template <class N>
+static int bals_launch(int ninst, int n, int degp1, int szt, int tailidx, const double *mat, double *rhs, double *sol,
+                       double *Q, double *R, int *flags, double *work, cudaStream_t st) {
+  const long smem = dense_smem_doubles(n, szt, N::width) * sizeof(double);
+  PHC_CUDA(cudaFuncSetAttribute(k_bals_solve<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_bals_solve<N><<<ninst, kDenseThreads, smem, st>>>(n, degp1, szt, tailidx, mat, rhs, sol, Q, R, flags, work);
+  PHC_CHECK_LAUNCH();
+  return PHC_OK;
+}
+
+#define PHC_DISPATCH(prec, cplx, CALL)                 \
+  do {                                                 \
+    if (!(cplx)) {                                     \
+      if ((prec) == 1) { typedef md::num<double, false> N; return CALL; } \
+      if ((prec) == 2) { typedef md::num<md::dd, false> N; return CALL; } \
+      { typedef md::num<md::qd, false> N; return CALL; } \
+    } else {                                           \
+      if ((prec) == 1) { typedef md::num<double, true> N; return CALL; } \
+      if ((prec) == 2) { typedef md::num<md::dd, true> N; return CALL; } \
+      { typedef md::num<md::qd, true> N; return CALL; } \
+    }                                                  \
+  } while (0)
+
+long dense_work_doubles(int prec, int cplx, int n, int szt) {
+  return dense_work_numbers(n, szt) * width_of(prec, cplx);
+}
+
+int blocked_houseqr(int prec, int cplx, int ninst, int n, int ncols, int szt, const double *A, double *Q, double *R,
+                    double *work, cudaStream_t st) {
+  PHC_REQUIRE(prec_ok(prec), "blocked_houseqr: precision %d", prec);
+  PHC_REQUIRE(n >= 1 && szt >= 1 && ncols % szt == 0 && ncols <= n && ncols >= 1, "blocked_houseqr: need ncols = szt*nbt <= n");
+  if (ninst == 0) return PHC_OK;
+  PHC_DISPATCH(prec, cplx, qr_launch<N>(ninst, n, ncols, szt, A, Q, R, work, st));
+}
+
+int upper_tiled_solver(int prec, int cplx, int ninst, int dim, int szt, double *U, double *b, double *x, double *work,
+                       cudaStream_t st) {
+  PHC_REQUIRE(prec_ok(prec), "upper_tiled_solver: precision %d", prec);
+  PHC_REQUIRE(dim >= 1 && szt >= 1 && dim % szt == 0, "upper_tiled_solver: need dim = szt*nbt");
+  if (ninst == 0) return PHC_OK;
+  PHC_DISPATCH(prec, cplx, tabs_launch<N>(ninst, dim, szt, U, b, x, work, st));
+}
+
+int bals_solve(int prec, int cplx, int ninst, int n, int degp1, int szt, int tailidx, const double *mat, double *rhs,
+               double *sol, double *Q, double *R, int *flags, double *work, cudaStream_t st) {
+  PHC_REQUIRE(prec_ok(prec), "bals_solve: precision %d", prec);
+  PHC_REQUIRE(n >= 1 && szt >= 1 && n % szt == 0 && degp1 >= 1, "bals_solve: need n = szt*nbt, degp1 >= 1");
+  PHC_REQUIRE(tailidx != 0 && tailidx <= degp1, "bals_solve: tailidx %d not in [1, degp1=%d] (or < 0: per instance)", tailidx, degp1);
+  if (ninst == 0) return PHC_OK;
+  PHC_DISPATCH(prec, cplx, bals_launch<N>(ninst, n, degp1, szt, tailidx, mat, rhs, sol, Q, R, flags, work, st));
+}
+
+}  // namespace phc

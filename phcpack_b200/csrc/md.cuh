@@ -304,6 +304,8 @@ template <class R, bool C> struct num;
 
 template <class R> struct num<R, false> {
   typedef R T;
+  typedef R real;
+  static const bool is_complex = false;
   typedef real_traits<R> tr;
   static const int width = tr::limbs;
   MD_INL static T zero() { return tr::zero(); }
@@ -325,6 +327,8 @@ template <class R> struct num<R, false> {
 
 template <class R> struct num<R, true> {
   typedef cx<R> T;
+  typedef R real;
+  static const bool is_complex = true;
   typedef real_traits<R> tr;
   static const int width = 2 * tr::limbs;
   MD_INL static T mkc(const R &a, const R &b) { T r; r.re = a; r.im = b; return r; }
