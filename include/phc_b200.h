@@ -101,6 +101,27 @@ int phc_bals_solve(int prec, int cplx, int ninst, int dim, int degp1, int szt, i
 int phc_bals_solve_host(int prec, int cplx, int ninst, int dim, int degp1, int szt, int tailidx, const double *mat,
                         double *rhs, double *sol, double *Q, double *R, int *flags, void *stream);
 
+/* One Newton step on power series for nsys systems (row form) at working
+ * degree deg <= maxdeg: evaluate and differentiate (phc_system_evaldiff),
+ * linearise (matrix series -> series of matrices, rhs = -f), solve
+ * (phc_bals_solve with each system's tail index in flags[4]), update
+ * x[i][j] += dx[j][i] for j >= newtail - 1.  series, cst, cff are stored with
+ * capacity maxdeg+1 per series.  Replaces Newton/dbl2_newton_method.h:406
+ * dbl2_row_newton_qrstep (GPU mode) and its cmplx / dbl4 twins.  work:
+ * phc_newton_workspace_bytes(...) bytes.  flags start at zeroQ=1, noqr=0,
+ * tail=1. */
+long long phc_newton_workspace_bytes(int prec, int cplx, int nsys, int dim, int deg, int szt, long long nmon);
+int phc_newton_step(int prec, int cplx, int nsys, int dim, int deg, int maxdeg, int szt, int maxvar,
+                    const int *mon_off, long long nmon, const int *nvr, const int *idx, const int *exps,
+                    const double *cst, const double *cff, double *series, double *Q, double *R, int *flags,
+                    double *work, void *stream);
+/* The Newton loop of Newton/dbl2_newton_method.cpp:1455-1492 on host
+ * arrays: nsteps steps, schedule 0 = fixed degree deg, 1 = the reference's
+ * working-degree schedule with its stop rule. */
+int phc_newton_host(int prec, int cplx, int nsys, int dim, int deg, int szt, int maxvar, const int *mon_off,
+                    const int *nvr, const int *idx, const int *exps, const double *cst, const double *cff,
+                    double *series, int nsteps, int schedule, int *flags, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

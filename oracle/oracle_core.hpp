@@ -376,6 +376,19 @@ template <class T> static void qrbs(int n, const T *Q, const T *Rm, const T *b, 
   backward(n, Rm, n, w, x);
 }
 
+// Skip thresholds of the reference's least-squares solvers:
+// Newton/dbl_bals_host.cpp:36,199 (double: |b_0| + 1 == 1 for the head,
+// 1e-15 in the tail), dbl2_bals_host.cpp:43,254 (1e-28), dbl4_bals_host.cpp:51,335
+// (1e-56).
+template <class T> static double skip_tol() {
+  const int L = limbs<typename real_of<T>::type>::n;
+  return L == 1 ? 1.0e-15 : (L == 2 ? 1.0e-28 : 1.0e-56);
+}
+template <class T> static bool head_tiny(double nrm) {
+  const int L = limbs<typename real_of<T>::type>::n;
+  return L == 1 ? (nrm + 1.0 == 1.0) : (nrm < skip_tol<T>());
+}
+
 struct bals_state {
   int zeroQ, noqr, upidx, bsidx, newtail;
 };
@@ -384,7 +397,8 @@ struct bals_state {
 // Newton/dbl2_bals_host.cpp:479 (CPU_dbl2_qrbs_solve) with the head at :15
 // and the tail at :228, including the skip rules: no QR when |b_0| < 1e-28
 // unless zeroQ, no update with x_{i-1} when |x_{i-1}| < 1e-28, no back
-// substitution (x_i = 0) when |b_i| < 1e-28.  rhs is overwritten.
+// substitution (x_i = 0) when |b_i| < 1e-28 (thresholds per precision in
+// skip_tol).  rhs is overwritten.
 template <class T>
 static void bals_solve(int dim, int degp1, int tailidx, const T *mat, T *rhs, T *sol, T *Q, T *Rm,
                        bals_state *st) {
@@ -392,7 +406,7 @@ static void bals_solve(int dim, int degp1, int tailidx, const T *mat, T *rhs, T 
   std::vector<T> w(dim);
   if (!(st->noqr && !st->zeroQ)) {
     double nrm = maxnorm(dim, rhs);
-    if (nrm < 1.0e-28) st->noqr = st->zeroQ ? 0 : 1;
+    if (head_tiny<T>(nrm)) st->noqr = st->zeroQ ? 0 : 1;
     if (!st->noqr) {
       houseqr(dim, dim, mat, Q, Rm);
       st->zeroQ = 0;
@@ -405,7 +419,7 @@ static void bals_solve(int dim, int degp1, int tailidx, const T *mat, T *rhs, T 
     st->newtail = degp1;
     for (int i = tailidx; i < degp1; ++i) {
       const T *xi = sol + (long)(i - 1) * dim;
-      if (maxnorm(dim, xi) < 1.0e-28) {
+      if (maxnorm(dim, xi) < skip_tol<T>()) {
         ++skipup;
       } else {
         for (int j = i; j < degp1; ++j) {
@@ -420,7 +434,7 @@ static void bals_solve(int dim, int degp1, int tailidx, const T *mat, T *rhs, T 
       }
       T *x = sol + (long)i * dim;
       T *b = rhs + (long)i * dim;
-      if (maxnorm(dim, b) < 1.0e-28) {
+      if (maxnorm(dim, b) < skip_tol<T>()) {
         ++skipbs;
         for (int j = 0; j < dim; ++j) x[j] = T();
       } else {

@@ -112,3 +112,38 @@ def reference() -> Lib | None:
             return None
         _ref = Lib(REF_SO, "ref")
     return _ref
+
+
+def newton_steps(lib: Lib, b, deg, nsteps, schedule=0):
+    """Newton on power series for every system of batch b (series of degree
+    deg in b.input, updated copy returned) with the oracle's single-system
+    step (oracle_capi.cpp newton_t); flags per system as in the C ABI."""
+    W = b.width
+    n1 = deg + 1
+    out = np.array(b.input, dtype=np.float64, copy=True)
+    flags_all = []
+    f = lib._fn("newton_step")
+    for s in range(b.nsys):
+        m0, m1 = int(b.mon_off[s * b.dim]), int(b.mon_off[(s + 1) * b.dim])
+        off = (b.mon_off[s * b.dim:(s + 1) * b.dim + 1] - m0).astype(np.int32)
+        ser = np.ascontiguousarray(out[s * b.dim * n1 * W:(s + 1) * b.dim * n1 * W])
+        cst = np.ascontiguousarray(b.cst[s * b.dim * n1 * W:(s + 1) * b.dim * n1 * W])
+        cff = np.ascontiguousarray(b.cff[m0 * n1 * W:m1 * n1 * W])
+        nvr = np.ascontiguousarray(b.nvr[m0:m1])
+        idx = np.ascontiguousarray(b.idx.reshape(-1, b.maxvar)[m0:m1])
+        exps = np.ascontiguousarray(b.exps.reshape(-1, b.maxvar)[m0:m1])
+        Q = np.zeros(b.dim * b.dim * W)
+        R = np.zeros(b.dim * b.dim * W)
+        fl = np.array([1, 0, 0, 0, 1], np.int32)
+        wrk = 0 if schedule else deg
+        for _ in range(nsteps):
+            rc = f(b.prec, int(b.cplx), b.dim, wrk, deg, b.maxvar, _ip(off), _ip(nvr), _ip(idx), _ip(exps), _dp(cst),
+                   _dp(cff), _dp(ser), _dp(Q), _dp(R), _ip(fl))
+            assert rc == 0
+            if schedule:
+                if fl[4] >= deg:
+                    break
+                wrk = min(deg, wrk + 1 + wrk // 2)
+        out[s * b.dim * n1 * W:(s + 1) * b.dim * n1 * W] = ser
+        flags_all.append(fl.copy())
+    return out, np.concatenate(flags_all)

@@ -35,6 +35,11 @@ int upper_tiled_solver(int prec, int cplx, int ninst, int dim, int szt, double *
 int bals_solve(int prec, int cplx, int ninst, int n, int degp1, int szt, int tailidx, const double *mat, double *rhs,
                double *sol, double *Q, double *R, int *flags, double *work, cudaStream_t st);
 
+long newton_work_doubles(int prec, int cplx, int nsys, int dim, int deg, int maxdeg, int szt, long nmon);
+int newton_step(int prec, int cplx, int nsys, int dim, int deg, int maxdeg, int szt, int maxvar, const int *mon_off,
+                long nmon, const int *nvr, const int *idx, const int *exps, const double *cst, const double *cff,
+                double *series, double *Q, double *R, int *flags, double *work, cudaStream_t st);
+
 // device scratch owned for the duration of one host call
 struct dbuf {
   void *p = nullptr;
@@ -231,6 +236,88 @@ int phc_bals_solve_host(int prec, int cplx, int ninst, int dim, int degp1, int s
   PHC_CUDA(cudaMemcpyAsync(Q, dQ, nq * 8, cudaMemcpyDeviceToHost, st));
   PHC_CUDA(cudaMemcpyAsync(R, dR, nq * 8, cudaMemcpyDeviceToHost, st));
   PHC_CUDA(cudaMemcpyAsync(flags, df, nf * 4, cudaMemcpyDeviceToHost, st));
+  PHC_CUDA(cudaStreamSynchronize(st));
+  return PHC_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------ Newton
+extern "C" {
+
+long long phc_newton_workspace_bytes(int prec, int cplx, int nsys, int dim, int deg, int szt, long long nmon) {
+  if (!prec_ok(prec) || nsys < 0 || dim < 1 || deg < 0 || szt < 1) return -1;
+  return (long long)newton_work_doubles(prec, cplx, nsys, dim, deg, deg, szt, (long)nmon) * 8;
+}
+
+int phc_newton_step(int prec, int cplx, int nsys, int dim, int deg, int maxdeg, int szt, int maxvar,
+                    const int *mon_off, long long nmon, const int *nvr, const int *idx, const int *exps,
+                    const double *cst, const double *cff, double *series, double *Q, double *R, int *flags,
+                    double *work, void *stream) {
+  return newton_step(prec, cplx, nsys, dim, deg, maxdeg, szt, maxvar, mon_off, (long)nmon, nvr, idx, exps, cst, cff,
+                     series, Q, R, flags, work, (cudaStream_t)stream);
+}
+
+// Newton's method on power series for a batch of systems, host arrays in and
+// out, the loop of Newton/dbl2_newton_method.cpp:1455-1492: at most nsteps
+// steps; schedule 0 keeps the working degree at deg, schedule 1 follows the
+// reference's 0, 1, 2, 4, 7, 11, ... (wrkdeg += 1 + wrkdeg/2, capped at deg)
+// and stops once every system's tail index reached deg.  series: nsys*dim
+// series of degree deg (updated in place); flags: 5 ints per system out.
+int phc_newton_host(int prec, int cplx, int nsys, int dim, int deg, int szt, int maxvar, const int *mon_off,
+                    const int *nvr, const int *idx, const int *exps, const double *cst, const double *cff,
+                    double *series, int nsteps, int schedule, int *flags, void *stream) {
+  PHC_REQUIRE(prec_ok(prec) && nsys >= 0 && dim >= 1 && deg >= 0 && szt >= 1 && dim % szt == 0,
+              "newton_host: bad sizes");
+  if (nsys == 0) return PHC_OK;
+  const size_t W = width_of(prec, cplx);
+  const long npoly = (long)nsys * dim;
+  const long nmon = mon_off[npoly];
+  const size_t S = (size_t)(deg + 1) * W;
+  const size_t nwork = (size_t)newton_work_doubles(prec, cplx, nsys, dim, deg, deg, szt, nmon);
+  staged s;
+  int rc = s.alloc(al((npoly + 1) * 4) + al(nmon * 4) + 2 * al(nmon * maxvar * 4) + 2 * al(npoly * S * 8) +
+                   al(nmon * S * 8) + 2 * al((size_t)nsys * dim * dim * W * 8) + al(nsys * 20) + al(nwork * 8));
+  if (rc) return rc;
+  int *d_off = s.take<int>(npoly + 1), *d_nvr = s.take<int>(nmon);
+  int *d_idx = s.take<int>(nmon * maxvar), *d_exp = s.take<int>(nmon * maxvar);
+  double *d_cst = s.take<double>(npoly * S), *d_ser = s.take<double>(npoly * S), *d_cff = s.take<double>(nmon * S);
+  double *d_Q = s.take<double>((size_t)nsys * dim * dim * W), *d_R = s.take<double>((size_t)nsys * dim * dim * W);
+  int *d_fl = s.take<int>((size_t)nsys * 5);
+  double *d_w = s.take<double>(nwork);
+  cudaStream_t st = (cudaStream_t)stream;
+  PHC_CUDA(cudaMemcpyAsync(d_off, mon_off, (npoly + 1) * 4, cudaMemcpyHostToDevice, st));
+  PHC_CUDA(cudaMemcpyAsync(d_nvr, nvr, nmon * 4, cudaMemcpyHostToDevice, st));
+  PHC_CUDA(cudaMemcpyAsync(d_idx, idx, nmon * maxvar * 4, cudaMemcpyHostToDevice, st));
+  PHC_CUDA(cudaMemcpyAsync(d_exp, exps, nmon * maxvar * 4, cudaMemcpyHostToDevice, st));
+  PHC_CUDA(cudaMemcpyAsync(d_cst, cst, npoly * S * 8, cudaMemcpyHostToDevice, st));
+  PHC_CUDA(cudaMemcpyAsync(d_cff, cff, nmon * S * 8, cudaMemcpyHostToDevice, st));
+  PHC_CUDA(cudaMemcpyAsync(d_ser, series, npoly * S * 8, cudaMemcpyHostToDevice, st));
+  for (long i = 0; i < nsys; ++i) {
+    flags[5 * i + 0] = 1;  // zeroQ
+    flags[5 * i + 1] = 0;  // noqr
+    flags[5 * i + 2] = 0;
+    flags[5 * i + 3] = 0;
+    flags[5 * i + 4] = 1;  // tail index
+  }
+  PHC_CUDA(cudaMemcpyAsync(d_fl, flags, (size_t)nsys * 20, cudaMemcpyHostToDevice, st));
+  int wrkdeg = schedule ? 0 : deg;
+  for (int step = 0; step < nsteps; ++step) {
+    rc = newton_step(prec, cplx, nsys, dim, wrkdeg, deg, szt, maxvar, d_off, nmon, d_nvr, d_idx, d_exp, d_cst, d_cff,
+                     d_ser, d_Q, d_R, d_fl, d_w, st);
+    if (rc) return rc;
+    if (schedule) {
+      PHC_CUDA(cudaMemcpyAsync(flags, d_fl, (size_t)nsys * 20, cudaMemcpyDeviceToHost, st));
+      PHC_CUDA(cudaStreamSynchronize(st));
+      bool done = true;
+      for (long i = 0; i < nsys; ++i) done = done && flags[5 * i + 4] >= deg;
+      if (done) break;
+      wrkdeg = wrkdeg + 1 + wrkdeg / 2;
+      if (wrkdeg > deg) wrkdeg = deg;
+    }
+  }
+  PHC_CUDA(cudaMemcpyAsync(series, d_ser, npoly * S * 8, cudaMemcpyDeviceToHost, st));
+  PHC_CUDA(cudaMemcpyAsync(flags, d_fl, (size_t)nsys * 20, cudaMemcpyDeviceToHost, st));
   PHC_CUDA(cudaStreamSynchronize(st));
   return PHC_OK;
 }

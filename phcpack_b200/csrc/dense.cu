@@ -51,7 +51,7 @@ __global__ void __launch_bounds__(kDenseThreads)
 // :108 and the tail at dbl2_tail_kernels.cu:154; skip rules of
 // Newton/dbl2_bals_host.cpp:15,228 (no QR when |b_0| < 1e-28 unless zeroQ,
 // no update with a solution block below 1e-28, no back substitution for a
-// right hand side below 1e-28).
+// right hand side below 1e-28; 1e-15 and 1e-56 in double and quad-double).
 // flags per instance: zeroQ, noqr, upidx, bsidx, newtail; with tailidx < 0
 // the tail starts at the instance's flags[4].
 template <class N>
@@ -78,7 +78,7 @@ __global__ void __launch_bounds__(kDenseThreads)
   bool tinv_ok = false;
   if (!(noqr && !zeroQ)) {
     const double nrm = block_maxnorm<N>(n, b, S.red);
-    if (nrm < 1.0e-28) {
+    if (head_tiny<N>(nrm)) {
       noqr = zeroQ ? 0 : 1;
       if (noqr)
         for (int i = threadIdx.x; i < n; i += blockDim.x) stn_at<N>(x, i, N::zero());
@@ -104,7 +104,7 @@ __global__ void __launch_bounds__(kDenseThreads)
     for (int i = tail0; i < degp1; ++i) {
       const double *xp = x + (long)(i - 1) * n * W;
       double nrm = block_maxnorm<N>(n, xp, S.red);
-      if (nrm < 1.0e-28) {
+      if (nrm < skip_tol<N>()) {
         ++up;
       } else {
         for (int l = threadIdx.x; l < n; l += blockDim.x) stn_at<N>(S.x, l, ldn_at<N>(xp, l));
@@ -114,7 +114,7 @@ __global__ void __launch_bounds__(kDenseThreads)
       const double *bi = b + (long)i * n * W;
       nrm = block_maxnorm<N>(n, bi, S.red);
       double *xi = x + (long)i * n * W;
-      if (nrm < 1.0e-28) {
+      if (nrm < skip_tol<N>()) {
         ++bs;
         for (int l = threadIdx.x; l < n; l += blockDim.x) stn_at<N>(xi, l, N::zero());
         __syncthreads();

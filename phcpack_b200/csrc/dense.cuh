@@ -74,6 +74,19 @@ __device__ double block_maxnorm(int n, const double *v, double *red) {
   return block_max(a, red);
 }
 
+// Skip thresholds of the reference's least-squares solvers per precision:
+// Newton/dbl_bals_host.cpp:36,199 (double: |b_0| + 1 == 1 in the head,
+// 1e-15 in the tail), dbl2_bals_host.cpp:43,254 (1e-28),
+// dbl4_bals_host.cpp:51,335 (1e-56).
+template <class N>
+__device__ __forceinline__ double skip_tol() {
+  return N::tr::limbs == 1 ? 1.0e-15 : (N::tr::limbs == 2 ? 1.0e-28 : 1.0e-56);
+}
+template <class N>
+__device__ __forceinline__ bool head_tiny(double nrm) {
+  return N::tr::limbs == 1 ? (__dadd_rn(nrm, 1.0) == 1.0) : (nrm < skip_tol<N>());
+}
+
 // Shared-memory layout of one CTA (in doubles), sized by dense_smem_doubles.
 struct dense_smem {
   double *v;     // Householder vector, n numbers
