@@ -122,6 +122,68 @@ int phc_newton_host(int prec, int cplx, int nsys, int dim, int deg, int szt, int
                     const int *nvr, const int *idx, const int *exps, const double *cst, const double *cff,
                     double *series, int nsteps, int schedule, int *flags, void *stream);
 
+/* ------------------------------------------------------------------ Track
+ * Batched series-Pade path tracking of homotopies
+ *   h(x, t) = sum over terms (a + b t) x^e,  t from 0 to 1,
+ * which covers (1 - t) gamma q(x) + t p(x) (a = gamma c_q, b = c_p - gamma c_q).
+ * Replaces the tracker behind the Ada/phcpy C interface:
+ * Ada/PHCtoC/gpumanypaths_dd.h:27 gpumanypaths_dd (and _d, _qd), whose
+ * internal GPU_Path_mult (Path/Path_GPU/path_gpu.h:38) tracks many paths and
+ * returns per-path success flags, with the algorithm of the Ada series-Pade
+ * tracker (Curves/predictor_corrector_trackers.adb:51).
+ *
+ * Systems: nsys systems; system s has dim[s] variables and equations;
+ *   distinct monomials mono_off[s] .. mono_off[s+1]-1, monomial m has
+ *   mono_nvr[m] (0 = the constant 1) distinct variables mono_idx[m*maxvar+v]
+ *   with exponents mono_exp[m*maxvar+v];
+ *   equations eq_off[s] .. eq_off[s+1]-1 (dim[s] of them), equation e has
+ *   terms term_off[e] .. term_off[e+1]-1, term r is (a + b t) times monomial
+ *   term_mono[r] (global id), a = term_a[2r] + i term_a[2r+1], b likewise.
+ * Jacobian gather lists (from phc_track_prepare): for (equation e, variable
+ *   j) the entries jg_off[e*maxdim+j] .. jg_off[e*maxdim+j+1]-1 of jg_term,
+ *   jg_slot.
+ * Paths: path p belongs to system path_sys[p] and starts at x0 (maxdim complex
+ *   doubles per path).
+ * ipar: deg (series degree K), numdeg (L), dendeg (M), nit (series Newton
+ *   steps), corsteps, maxsteps, refine_steps.
+ * dpar: pbeta, alpha, maxsize, minsize, tolres, epsilon, restol (endpoint
+ *   residual bound), learn_scale (multiplies learned proposals; 0 = 1).
+ * pmode: predictor precision 1 (double) or 2 (double-double); the corrector
+ *   is double-double; rmode: refinement precision 2 or 4 (quad-double).
+ * step_mode 1 with a model (phc_mlp_*) uses the learned step proposer; a
+ *   proposal whose feedback or corrector fails is redone with the plain step.
+ * Output per path: xend maxdim complex quad-doubles (lower limbs zero below
+ *   rmode), info[3p..3p+2] = status (0 success, 1 step below minsize,
+ *   2 maxsteps reached, 3 endpoint residual above restol), steps, rejected
+ *   steps; dinfo[2p..2p+1] = final t, endpoint residual.
+ * log: when not NULL, each accepted step appends 32 floats (24 features,
+ *   accepted step, plain step, proposed step, t) up to log_cap records;
+ *   *log_count counts them.  queue: one device int (the work-queue counter).
+ * one_per_launch != 0 tracks one path per launch (one CTA), back to back:
+ *   the plain arrangement the batched kernel is measured against. */
+long long phc_track_gather_count(int nsys, const int *mono_off, const int *mono_nvr, const int *eq_off,
+                                 const int *term_off, const int *term_mono);
+int phc_track_prepare(int nsys, const int *dim, int maxvar, const int *mono_off, const int *mono_nvr,
+                      const int *mono_idx, const int *eq_off, const int *term_off, const int *term_mono, int maxdim,
+                      int *jg_off, int *jg_term, int *jg_slot);
+long long phc_track_smem_bytes(int maxdim, int deg, int dendeg, int nmono_max, int maxvar, int pmode, int rmode);
+int phc_track(int nsys, const int *dim, int maxvar, int maxdim, int nmono_max, const int *mono_off,
+              const int *mono_nvr, const int *mono_idx, const int *mono_exp, const int *eq_off, const int *term_off,
+              const int *term_mono, const double *term_a, const double *term_b, const int *jg_off,
+              const int *jg_term, const int *jg_slot, int npaths, const int *path_sys, const double *x0,
+              const int *ipar, const double *dpar, int pmode, int rmode, int step_mode, const void *model,
+              double *xend, int *info, double *dinfo, float *log, int log_cap, int *log_count, int *queue,
+              int one_per_launch, void *stream);
+/* Host arrays in and out; returns the number of paths not classified as
+ * success (>= 0) or an error (< 0). */
+int phc_track_host(int nsys, const int *dim, int maxvar, const int *mono_off, const int *mono_nvr,
+                   const int *mono_idx, const int *mono_exp, const int *eq_off, const int *term_off,
+                   const int *term_mono, const double *term_a, const double *term_b, int npaths,
+                   const int *path_sys, const double *x0, const int *ipar, const double *dpar, int pmode, int rmode,
+                   int step_mode, const void *model, double *xend, int *info, double *dinfo, void *stream);
+/* Size in bytes of a learned step model (24 -> 128 -> 128 -> 1, BF16). */
+long long phc_mlp_model_bytes(void);
+
 #ifdef __cplusplus
 }
 #endif

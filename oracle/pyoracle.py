@@ -147,3 +147,19 @@ def newton_steps(lib: Lib, b, deg, nsteps, schedule=0):
         out[s * b.dim * n1 * W:(s + 1) * b.dim * n1 * W] = ser
         flags_all.append(fl.copy())
     return out, np.concatenate(flags_all)
+
+
+def track(lib: Lib, pb, ipar, dpar, pmode=1, rmode=2, nthreads=1):
+    """Track the paths of a homotopy TrackProblem on the CPU (the tracker
+    restatement of tracker_oracle.cpp).  Returns (xend, info, dinfo) with
+    the layout of the C ABI."""
+    xend = np.zeros(pb.npaths * pb.maxdim * 8)
+    info = np.zeros(pb.npaths * 3, np.int32)
+    dinfo = np.zeros(pb.npaths * 2)
+    f = lib._fn("track")
+    rc = f(pb.nsys, _ip(pb.dim), pb.maxvar, _ip(pb.mono_off), _ip(pb.mono_nvr), _ip(pb.mono_idx), _ip(pb.mono_exp),
+           _ip(pb.eq_off), _ip(pb.term_off), _ip(pb.term_mono), _dp(pb.term_a), _dp(pb.term_b), pb.npaths,
+           _ip(pb.path_sys), pb.maxdim, _dp(pb.x0), _ip(ipar), _dp(dpar), pmode, rmode, nthreads, _dp(xend),
+           _ip(info), _dp(dinfo))
+    assert rc == 0
+    return xend, info, dinfo

@@ -1,1 +1,488 @@
-// placeholder
+// tracker_oracle.cpp -- CPU restatement of the series-Pade path tracker.
+//
+// TEST INFRASTRUCTURE ONLY: the checker of the GPU tracker and the CPU
+// baseline of bench.py.  Never part of the product path.
+//
+// The reference's series-Pade tracker is Ada code (not compilable here):
+//   Curves/predictor_corrector_trackers.adb:51-77  Track_One_Path
+//   Curves/predictor_corrector_loops.adb:37-85     Predictor_Corrector_Loop
+//   Curves/standard_predictor_convolutions.adb:1142-1185 LU_Prediction,
+//                                              :958-993   Predictor_Feedback
+//   Curves/standard_rational_approximations.ads:67-145 Pade, Evaluate
+//   Math_Lib/Circuits/convergence_radius_estimates.adb:138,354 Fabry
+//   Solutions/standard_mixed_residuals.adb:472 Mixed_Residual
+//   Curves/homotopy_continuation_parameters.adb:6-24 defaults
+// restated here on top of this oracle's multiple-double arithmetic.  What is
+// restated and what is left out:
+//  * predictor: Newton on power series in s = t - t0 to degree K (working
+//    degree doubling 1, 3, 7, ... K), each step a block-Toeplitz solve with
+//    the QR of J_0; [L/M] Pade approximant per component; pole step
+//    pbeta * r with r the smallest Fabry radius |c_{K-3}/c_{K-2}| (offset 2
+//    as in Newton_Fabry); step = min(pole step, maxsize), cut at t = 1;
+//  * the Hessian curvature step (Hesse_Pade, singular values of Hessians)
+//    is left out: the predictor feedback and the corrector bound the step;
+//  * predictor feedback: halve the step until the mixed residual of the
+//    Pade prediction is below alpha (fail below minsize);
+//  * corrector: at most corsteps Newton steps at the new t, converged when
+//    max |dx_i| <= tolres, followed by one extra step; on failure halve the
+//    step and re-evaluate the Pade approximant (fail below minsize);
+//  * stop when |1 - t| < epsilon; refine the endpoint at t = 1 and classify
+//    success when the max-norm residual is at most restol.
+// The homotopy is h(x, t) = sum_terms (a + b t) x^e, which covers
+// (1 - t) gamma q(x) + t p(x) with a = gamma c_q, b = c_p - gamma c_q.
+#include <vector>
+#include <thread>
+#include <atomic>
+#include <cmath>
+#include <algorithm>
+#include "oracle_core.hpp"
+
+using namespace orc;
+
+namespace {
+
+struct TrackSys {
+  int nsys, maxvar;
+  const int *dim;       // [nsys]
+  const int *mono_off;  // [nsys+1], global monomial ids
+  const int *mono_nvr;  // [nmono]
+  const int *mono_idx;  // [nmono*maxvar]
+  const int *mono_exp;  // [nmono*maxvar]
+  const int *eq_off;    // [nsys+1], global equation ids
+  const int *term_off;  // [neq+1]
+  const int *term_mono; // [nterm]
+  const double *term_a; // [nterm*2] complex double
+  const double *term_b; // [nterm*2]
+};
+
+struct TrackPar {
+  int deg, numdeg, dendeg, nit, corsteps, maxsteps, refine_steps;
+  double pbeta, alpha, maxsize, minsize, tolres, epsilon, restol;
+};
+
+template <class R> static cx<R> cplx(double re, double im) { return cx<R>(R(re), R(im)); }
+
+// Evaluate h and, when jac != nullptr, J at a vector of series x (dim
+// series of degree w) at t = t0 + s: value series h[i][k], Jacobian series
+// jac[k][i][j].  Per distinct monomial: common factor, then products of the
+// distinct variables (the reference's common-factor + Speelpenning method
+// restated for a monomial without coefficient); per term the coefficient
+// series (a + b t0) + b s multiplies the monomial and its partials.
+template <class T>
+static void hom_eval(const TrackSys &S, int s, int w, double t0, const std::vector<std::vector<T> > &x,
+                     std::vector<std::vector<T> > &h, std::vector<T> *jac) {
+  typedef typename real_of<T>::type R;
+  const int n = S.dim[s];
+  const int n1 = w + 1;
+  const int m0 = S.mono_off[s], m1 = S.mono_off[s + 1];
+  const int nm = m1 - m0;
+  // V[m] value, G[m][v] partial w.r.t. slot v (exponent included)
+  std::vector<std::vector<T> > V(nm, std::vector<T>(n1));
+  std::vector<std::vector<std::vector<T> > > G(nm);
+  std::vector<T> tmp(n1), acc(n1);
+  for (int m = 0; m < nm; ++m) {
+    const int gm = m0 + m;
+    const int k = S.mono_nvr[gm];
+    const int *ix = S.mono_idx + (long)gm * S.maxvar;
+    const int *ex = S.mono_exp + (long)gm * S.maxvar;
+    std::vector<T> F(n1);
+    F[0] = T(R(1.0));
+    for (int v = 0; v < k; ++v)
+      for (int e = 1; e < ex[v]; ++e) {
+        conv(w, x[ix[v]].data(), F.data(), tmp.data());
+        F = tmp;
+      }
+    G[m].assign(k, std::vector<T>(n1));
+    if (k == 0) {
+      V[m] = F;
+      continue;
+    }
+    // partial v = F * prod_{u != v} x_u ; value = partial_0 * x_0
+    for (int v = 0; v < k; ++v) {
+      acc = F;
+      for (int u = 0; u < k; ++u) {
+        if (u == v) continue;
+        conv(w, acc.data(), x[ix[u]].data(), tmp.data());
+        acc = tmp;
+      }
+      if (v == 0) conv(w, acc.data(), x[ix[0]].data(), V[m].data());
+      for (int i = 0; i < n1; ++i) G[m][v][i] = mul_d(acc[i], (double)ex[v]);
+    }
+  }
+  h.assign(n, std::vector<T>(n1));
+  if (jac) jac->assign((long)n1 * n * n, T());
+  const int e0 = S.eq_off[s];
+  for (int i = 0; i < n; ++i) {
+    const int eq = e0 + i;
+    for (int tr = S.term_off[eq]; tr < S.term_off[eq + 1]; ++tr) {
+      const int m = S.term_mono[tr] - m0;
+      const T a = cplx<R>(S.term_a[2 * tr], S.term_a[2 * tr + 1]);
+      const T b = cplx<R>(S.term_b[2 * tr], S.term_b[2 * tr + 1]);
+      const T c0 = a + b * T(R(t0));
+      for (int kk = 0; kk < n1; ++kk) {
+        T v = c0 * V[m][kk];
+        if (kk > 0) v = v + b * V[m][kk - 1];
+        h[i][kk] = h[i][kk] + v;
+      }
+      if (jac) {
+        const int gm = m0 + m;
+        const int k = S.mono_nvr[gm];
+        const int *ix = S.mono_idx + (long)gm * S.maxvar;
+        for (int vv = 0; vv < k; ++vv) {
+          const int j = ix[vv];
+          for (int kk = 0; kk < n1; ++kk) {
+            T v = c0 * G[m][vv][kk];
+            if (kk > 0) v = v + b * G[m][vv][kk - 1];
+            T &dst = (*jac)[((long)kk * n + i) * n + j];
+            dst = dst + v;
+          }
+        }
+      }
+    }
+  }
+}
+
+// |h_i| evaluated with |coefficients(t)| at |x| (real, in double), for the
+// mixed residual of Solutions/standard_mixed_residuals.adb:472
+template <class T>
+static void hom_abs_eval(const TrackSys &S, int s, double t, const std::vector<double> &ax, std::vector<double> &r) {
+  const int n = S.dim[s];
+  r.assign(n, 0.0);
+  const int e0 = S.eq_off[s];
+  for (int i = 0; i < n; ++i)
+    for (int tr = S.term_off[e0 + i]; tr < S.term_off[e0 + i + 1]; ++tr) {
+      const int gm = S.term_mono[tr];
+      const double cr = S.term_a[2 * tr] + S.term_b[2 * tr] * t;
+      const double ci = S.term_a[2 * tr + 1] + S.term_b[2 * tr + 1] * t;
+      double v = std::hypot(cr, ci);
+      for (int u = 0; u < S.mono_nvr[gm]; ++u)
+        v *= std::pow(ax[S.mono_idx[(long)gm * S.maxvar + u]], S.mono_exp[(long)gm * S.maxvar + u]);
+      r[i] += v;
+    }
+}
+
+template <class R> static double cabs(const cx<R> &a) { return std::hypot(to_double(a.re), to_double(a.im)); }
+
+// Solve A x = b (n x n complex) by the Householder QR of this oracle
+template <class T> struct qr_solver {
+  int n;
+  std::vector<T> Q, Rm, w;
+  void factor(int n_, const std::vector<T> &A) {
+    n = n_;
+    Q.assign((long)n * n, T());
+    Rm.assign((long)n * n, T());
+    w.assign(n, T());
+    houseqr(n, n, A.data(), Q.data(), Rm.data());
+  }
+  void solve(const T *b, T *x) { qrbs(n, Q.data(), Rm.data(), b, x, w.data()); }
+};
+
+// Newton on power series (the predictor): x[i] series of degree K, on
+// entry the constant terms hold the current point
+template <class T>
+static void series_newton(const TrackSys &S, int s, const TrackPar &P, double t0, std::vector<std::vector<T> > &x) {
+  const int n = S.dim[s];
+  const int K = P.deg;
+  std::vector<std::vector<T> > h;
+  std::vector<T> jac, rhs(n), dx((long)(K + 1) * n), A((long)n * n);
+  qr_solver<T> qr;
+  for (int it = 0; it < P.nit; ++it) {
+    int w = (2 << it) - 1;
+    if (w > K) w = K;
+    std::vector<std::vector<T> > xw(n, std::vector<T>(w + 1));
+    for (int i = 0; i < n; ++i)
+      for (int k = 0; k <= w; ++k) xw[i][k] = x[i][k];
+    hom_eval(S, s, w, t0, xw, h, &jac);
+    for (int l = 0; l < n * n; ++l) A[l] = jac[l];
+    qr.factor(n, A);
+    for (int k = 0; k <= w; ++k) {
+      for (int i = 0; i < n; ++i) {
+        T acc = -h[i][k];
+        for (int j = 1; j <= k; ++j)
+          for (int l = 0; l < n; ++l) acc = acc - jac[((long)j * n + i) * n + l] * dx[(long)(k - j) * n + l];
+        rhs[i] = acc;
+      }
+      qr.solve(rhs.data(), dx.data() + (long)k * n);
+    }
+    for (int i = 0; i < n; ++i)
+      for (int k = 0; k <= w; ++k) x[i][k] = x[i][k] + dx[(long)k * n + i];
+  }
+}
+
+// [L/M] Pade approximant of the series c[0..L+M]: denominator from
+// sum_{j=1..M} c_{L+i-j} q_j = -c_{L+i}, i = 1..M, by Gaussian elimination
+// with partial pivoting; numerator p_i = sum_{j<=min(i,M)} q_j c_{i-j}
+// (Curves/standard_rational_approximations.ads:67-100).  A singular
+// denominator system falls back to the Taylor polynomial (q = 1, p = c).
+template <class T>
+static bool pade(int L, int M, const std::vector<T> &c, std::vector<T> &p, std::vector<T> &q) {
+  typedef typename real_of<T>::type R;
+  q.assign(M + 1, T());
+  q[0] = T(R(1.0));
+  p.assign(L + M + 1, T());
+  bool ok = true;
+  if (M > 0) {
+    std::vector<T> A((long)M * M), b(M);
+    for (int i = 1; i <= M; ++i) {
+      for (int j = 1; j <= M; ++j) {
+        const int k = L + i - j;
+        A[(i - 1) * M + (j - 1)] = k >= 0 ? c[k] : T();
+      }
+      b[i - 1] = -c[L + i];
+    }
+    for (int col = 0; col < M && ok; ++col) {
+      int piv = col;
+      double best = cabs(A[col * M + col]);
+      for (int r = col + 1; r < M; ++r)
+        if (cabs(A[r * M + col]) > best) { best = cabs(A[r * M + col]); piv = r; }
+      if (best == 0.0) { ok = false; break; }
+      if (piv != col) {
+        for (int j = 0; j < M; ++j) std::swap(A[piv * M + j], A[col * M + j]);
+        std::swap(b[piv], b[col]);
+      }
+      for (int r = col + 1; r < M; ++r) {
+        const T f = A[r * M + col] / A[col * M + col];
+        for (int j = col; j < M; ++j) A[r * M + j] = A[r * M + j] - f * A[col * M + j];
+        b[r] = b[r] - f * b[col];
+      }
+    }
+    if (ok) {
+      for (int i = M - 1; i >= 0; --i) {
+        T acc = b[i];
+        for (int j = i + 1; j < M; ++j) acc = acc - A[i * M + j] * q[j + 1];
+        q[i + 1] = acc / A[i * M + i];
+      }
+    }
+  }
+  if (!ok) {
+    q.assign(M + 1, T());
+    q[0] = T(R(1.0));
+    for (int i = 0; i <= L + M; ++i) p[i] = c[i];
+    return false;
+  }
+  for (int i = 0; i <= L; ++i) {
+    T acc;
+    for (int j = 0; j <= std::min(i, M); ++j) acc = acc + q[j] * c[i - j];
+    p[i] = acc;
+  }
+  for (int i = L + 1; i <= L + M; ++i) p[i] = T();
+  return true;
+}
+
+template <class T> static T horner(const std::vector<T> &a, int deg, const T &z) {
+  T acc = a[deg];
+  for (int i = deg - 1; i >= 0; --i) acc = acc * z + a[i];
+  return acc;
+}
+
+// Newton at a point (the corrector / refinement), returns converged
+template <class T>
+static bool point_newton(const TrackSys &S, int s, double t, std::vector<T> &x, int maxit, double tol, int extra,
+                         double *lastdx) {
+  const int n = S.dim[s];
+  std::vector<std::vector<T> > xs(n, std::vector<T>(1)), h;
+  std::vector<T> jac, rhs(n), dx(n);
+  qr_solver<T> qr;
+  bool conv = false;
+  int extra_left = extra;
+  *lastdx = 1e300;
+  for (int it = 0; it < maxit + extra; ++it) {
+    if (it >= maxit && !conv) break;
+    for (int i = 0; i < n; ++i) xs[i][0] = x[i];
+    hom_eval(S, s, 0, t, xs, h, &jac);
+    qr.factor(n, jac);
+    for (int i = 0; i < n; ++i) rhs[i] = -h[i][0];
+    qr.solve(rhs.data(), dx.data());
+    double m = 0.0;
+    for (int i = 0; i < n; ++i) {
+      x[i] = x[i] + dx[i];
+      const double a = cabs(dx[i]);
+      m = (a > m || std::isnan(a)) ? a : m;
+    }
+    *lastdx = m;
+    if (std::isnan(m)) return false;
+    if (conv) {
+      if (--extra_left <= 0) break;
+    } else if (m <= tol) {
+      conv = true;
+      if (extra_left <= 0) break;
+    }
+  }
+  return conv;
+}
+
+template <class T> static double maxres(const TrackSys &S, int s, double t, const std::vector<T> &x) {
+  const int n = S.dim[s];
+  std::vector<std::vector<T> > xs(n, std::vector<T>(1)), h;
+  for (int i = 0; i < n; ++i) xs[i][0] = x[i];
+  hom_eval<T>(S, s, 0, t, xs, h, nullptr);
+  double r = 0.0;
+  for (int i = 0; i < n; ++i) r = std::max(r, cabs(h[i][0]));
+  return r;
+}
+
+template <class PT, class CT> static void convert(const CT &a, PT &b);
+template <> void convert(const cx<dd> &a, cx<double> &b) { b = cx<double>(a.re.hi + a.re.lo, a.im.hi + a.im.lo); }
+template <> void convert(const cx<dd> &a, cx<dd> &b) { b = a; }
+template <> void convert(const cx<double> &a, cx<dd> &b) { b = cx<dd>(dd(a.re), dd(a.im)); }
+template <> void convert(const cx<dd> &a, cx<qd> &b) { b = cx<qd>(qd(a.re), qd(a.im)); }
+template <> void convert(const cx<qd> &a, cx<qd> &b) { b = a; }
+
+struct PathOut {
+  int status, nsteps, nreject;
+  double t, residual;
+};
+
+// Track one path.  PT: predictor numbers, CT: corrector numbers, RT:
+// refinement numbers.
+template <class PT, class CT, class RT>
+static PathOut track_path(const TrackSys &S, int s, const TrackPar &P, const double *x0, double *xend) {
+  const int n = S.dim[s];
+  const int K = P.deg;
+  PathOut o{0, 0, 0, 0.0, 0.0};
+  std::vector<CT> x(n);
+  for (int i = 0; i < n; ++i) convert(cx<double>(x0[2 * i], x0[2 * i + 1]), x[i]);
+  double t = 0.0, dxn;
+  point_newton(S, s, 0.0, x, P.corsteps, P.tolres, 1, &dxn);
+  std::vector<std::vector<PT> > xs(n, std::vector<PT>(K + 1));
+  std::vector<std::vector<PT> > num(n), den(n);
+  std::vector<CT> xc(n);
+  std::vector<PT> xp(n);
+  std::vector<double> ax(n), rabs;
+  std::vector<int> pdeg(n), qdeg(n);
+  bool failed = false;
+  int k;
+  for (k = 0; k < P.maxsteps; ++k) {
+    for (int i = 0; i < n; ++i) {
+      xs[i].assign(K + 1, PT());
+      convert(x[i], xs[i][0]);
+    }
+    series_newton(S, s, P, t, xs);
+    double r = 1e300;
+    bool rfail = true;
+    for (int i = 0; i < n; ++i) {
+      const bool ok = pade(P.numdeg, P.dendeg, xs[i], num[i], den[i]);
+      pdeg[i] = ok ? P.numdeg : K;  // the fallback is the Taylor polynomial
+      qdeg[i] = ok ? P.dendeg : 0;
+      const double cden = cabs(xs[i][K - 2]);
+      if (cden != 0.0) {
+        const double ri = cabs(xs[i][K - 3]) / cden;
+        if (ri < r) r = ri;
+        rfail = false;
+      }
+    }
+    double step = rfail ? P.maxsize : P.pbeta * r;
+    if (step > P.maxsize) step = P.maxsize;
+    if (t + step > 1.0) step = 1.0 - t;
+    // predictor feedback on the mixed residual
+    auto predict = [&](double st) {
+      const PT z = PT(typename real_of<PT>::type(st));
+      for (int i = 0; i < n; ++i) xp[i] = horner(num[i], pdeg[i], z) / horner(den[i], qdeg[i], z);
+    };
+    double mixres;
+    for (;;) {
+      predict(step);
+      std::vector<std::vector<PT> > xs0(n, std::vector<PT>(1)), hv;
+      for (int i = 0; i < n; ++i) {
+        xs0[i][0] = xp[i];
+        ax[i] = cabs(xp[i]);
+      }
+      hom_eval<PT>(S, s, 0, t + step, xs0, hv, nullptr);
+      hom_abs_eval<PT>(S, s, t + step, ax, rabs);
+      mixres = 0.0;
+      for (int i = 0; i < n; ++i) mixres += cabs(hv[i][0]) / (rabs[i] + 1.0);
+      mixres /= n;
+      if (mixres < P.alpha) break;
+      step *= 0.5;
+      ++o.nreject;
+      if (step < P.minsize) break;
+    }
+    if (step < P.minsize) { failed = true; break; }
+    // corrector with step halving
+    for (;;) {
+      for (int i = 0; i < n; ++i) convert(xp[i], xc[i]);
+      if (point_newton(S, s, t + step, xc, P.corsteps, P.tolres, 1, &dxn)) break;
+      step *= 0.5;
+      ++o.nreject;
+      if (step < P.minsize) break;
+      predict(step);
+    }
+    if (step < P.minsize) { failed = true; break; }
+    x = xc;
+    t += step;
+    if (std::fabs(1.0 - t) < P.epsilon) { ++k; break; }
+  }
+  o.nsteps = k;
+  o.t = t;
+  std::vector<RT> xr(n);
+  for (int i = 0; i < n; ++i) convert(x[i], xr[i]);
+  if (!failed && std::fabs(1.0 - t) < P.epsilon) {
+    point_newton(S, s, 1.0, xr, P.refine_steps, 0.0, 0, &dxn);
+    o.residual = maxres(S, s, 1.0, xr);
+    o.status = (o.residual <= P.restol) ? 0 : 3;
+  } else {
+    o.residual = maxres(S, s, t, xr);
+    o.status = failed ? 1 : 2;
+  }
+  for (int i = 0; i < n; ++i) store(xend + (long)i * limbs<cx<qd> >::n, cx<qd>());
+  for (int i = 0; i < n; ++i) {
+    cx<qd> q;
+    convert(xr[i], q);
+    store(xend + (long)i * limbs<cx<qd> >::n, q);
+  }
+  return o;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Track npaths paths with nthreads host threads.  pmode: predictor
+// precision (1 double, 2 double-double); rmode: refinement precision
+// (2 dd, 4 qd); the corrector is double-double.  x0: start points, maxdim
+// complex doubles per path; xend: maxdim complex quad-doubles per path
+// (lower limbs zero below the refinement precision); info: per path
+// status, nsteps, nreject; dinfo: per path t, residual.
+int orc_track(int nsys, const int *dim, int maxvar, const int *mono_off, const int *mono_nvr, const int *mono_idx,
+              const int *mono_exp, const int *eq_off, const int *term_off, const int *term_mono,
+              const double *term_a, const double *term_b, int npaths, const int *path_sys, int maxdim,
+              const double *x0, const int *ipar, const double *dpar, int pmode, int rmode, int nthreads,
+              double *xend, int *info, double *dinfo) {
+  TrackSys S{nsys, maxvar, dim, mono_off, mono_nvr, mono_idx, mono_exp, eq_off, term_off, term_mono, term_a, term_b};
+  TrackPar P;
+  P.deg = ipar[0]; P.numdeg = ipar[1]; P.dendeg = ipar[2]; P.nit = ipar[3];
+  P.corsteps = ipar[4]; P.maxsteps = ipar[5]; P.refine_steps = ipar[6];
+  P.pbeta = dpar[0]; P.alpha = dpar[1]; P.maxsize = dpar[2]; P.minsize = dpar[3];
+  P.tolres = dpar[4]; P.epsilon = dpar[5]; P.restol = dpar[6];
+  if (P.numdeg + P.dendeg != P.deg || P.deg < 3) return -1;
+  std::atomic<int> next(0);
+  auto work = [&]() {
+    for (;;) {
+      const int p = next.fetch_add(1);
+      if (p >= npaths) return;
+      const int s = path_sys[p];
+      PathOut o;
+      double *xe = xend + (long)p * maxdim * 8;
+      const double *xs = x0 + (long)p * maxdim * 2;
+      if (pmode == 1 && rmode == 2) o = track_path<cx<double>, cx<dd>, cx<dd> >(S, s, P, xs, xe);
+      else if (pmode == 1) o = track_path<cx<double>, cx<dd>, cx<qd> >(S, s, P, xs, xe);
+      else if (rmode == 2) o = track_path<cx<dd>, cx<dd>, cx<dd> >(S, s, P, xs, xe);
+      else o = track_path<cx<dd>, cx<dd>, cx<qd> >(S, s, P, xs, xe);
+      info[3 * p] = o.status;
+      info[3 * p + 1] = o.nsteps;
+      info[3 * p + 2] = o.nreject;
+      dinfo[2 * p] = o.t;
+      dinfo[2 * p + 1] = o.residual;
+    }
+  };
+  if (nthreads <= 1) {
+    work();
+  } else {
+    std::vector<std::thread> th;
+    for (int i = 0; i < nthreads; ++i) th.emplace_back(work);
+    for (auto &x : th) x.join();
+  }
+  return 0;
+}
+
+}  // extern "C"

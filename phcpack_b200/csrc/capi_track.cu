@@ -1,0 +1,181 @@
+// capi_track.cu -- C ABI of the path tracker (include/phc_b200.h).
+#include <vector>
+#include "common.cuh"
+#include "tracker.cuh"
+#include "mlp.cuh"
+#include "../../include/phc_b200.h"
+
+namespace phc {
+int track(const TrackDev &S, const TrackParDev &P, int nmono_max, int npaths, const int *path_sys, const double *x0,
+          int pmode, int rmode, const void *model, double *xend, int *info, double *dinfo, float *log, int log_cap,
+          int *log_count, int *queue, int one_per_launch, cudaStream_t st);
+long track_smem_bytes(int maxdim, int K, int M, int nmono_max, int maxvar, int pmode, int rmode);
+}  // namespace phc
+
+using namespace phc;
+
+static TrackParDev make_par(const int *ipar, const double *dpar, int step_mode) {
+  TrackParDev P;
+  P.deg = ipar[0];
+  P.numdeg = ipar[1];
+  P.dendeg = ipar[2];
+  P.nit = ipar[3];
+  P.corsteps = ipar[4];
+  P.maxsteps = ipar[5];
+  P.refine_steps = ipar[6];
+  P.step_mode = step_mode;
+  P.pbeta = dpar[0];
+  P.alpha = dpar[1];
+  P.maxsize = dpar[2];
+  P.minsize = dpar[3];
+  P.tolres = dpar[4];
+  P.epsilon = dpar[5];
+  P.restol = dpar[6];
+  P.learn_scale = dpar[7] > 0.0 ? dpar[7] : 1.0;
+  return P;
+}
+
+extern "C" {
+
+long long phc_track_gather_count(int nsys, const int *mono_off, const int *mono_nvr, const int *eq_off,
+                                 const int *term_off, const int *term_mono) {
+  (void)mono_off;
+  long long c = 0;
+  const int neq = eq_off[nsys];
+  for (int tr = 0; tr < term_off[neq]; ++tr) c += mono_nvr[term_mono[tr]];
+  return c;
+}
+
+int phc_track_prepare(int nsys, const int *dim, int maxvar, const int *mono_off, const int *mono_nvr,
+                      const int *mono_idx, const int *eq_off, const int *term_off, const int *term_mono, int maxdim,
+                      int *jg_off, int *jg_term, int *jg_slot) {
+  PHC_REQUIRE(nsys >= 0 && maxvar >= 1 && maxdim >= 1, "track_prepare: bad sizes");
+  const int neq = eq_off[nsys];
+  std::vector<std::vector<std::pair<int, int> > > lists((size_t)neq * maxdim);
+  for (int s = 0; s < nsys; ++s) {
+    PHC_REQUIRE(dim[s] >= 1 && dim[s] <= maxdim && eq_off[s + 1] - eq_off[s] == dim[s],
+                "track_prepare: system %d has %d equations for dimension %d", s, eq_off[s + 1] - eq_off[s], dim[s]);
+    for (int e = eq_off[s]; e < eq_off[s + 1]; ++e)
+      for (int tr = term_off[e]; tr < term_off[e + 1]; ++tr) {
+        const int m = term_mono[tr];
+        PHC_REQUIRE(m >= mono_off[s] && m < mono_off[s + 1], "track_prepare: term %d uses monomial %d of another system", tr, m);
+        PHC_REQUIRE(mono_nvr[m] >= 0 && mono_nvr[m] <= maxvar, "track_prepare: monomial %d has %d variables", m, mono_nvr[m]);
+        for (int v = 0; v < mono_nvr[m]; ++v) {
+          const int j = mono_idx[(long)m * maxvar + v];
+          PHC_REQUIRE(j >= 0 && j < dim[s], "track_prepare: variable %d out of range in monomial %d", j, m);
+          lists[(size_t)e * maxdim + j].push_back(std::make_pair(tr, v));
+        }
+      }
+  }
+  int q = 0;
+  for (size_t g = 0; g < lists.size(); ++g) {
+    jg_off[g] = q;
+    for (auto &pr : lists[g]) {
+      jg_term[q] = pr.first;
+      jg_slot[q] = pr.second;
+      ++q;
+    }
+  }
+  jg_off[lists.size()] = q;
+  return PHC_OK;
+}
+
+long long phc_track_smem_bytes(int maxdim, int deg, int dendeg, int nmono_max, int maxvar, int pmode, int rmode) {
+  return track_smem_bytes(maxdim, deg, dendeg, nmono_max, maxvar, pmode, rmode);
+}
+
+long long phc_mlp_model_bytes(void) { return mlp_model_bytes(); }
+
+int phc_track(int nsys, const int *dim, int maxvar, int maxdim, int nmono_max, const int *mono_off,
+              const int *mono_nvr, const int *mono_idx, const int *mono_exp, const int *eq_off, const int *term_off,
+              const int *term_mono, const double *term_a, const double *term_b, const int *jg_off,
+              const int *jg_term, const int *jg_slot, int npaths, const int *path_sys, const double *x0,
+              const int *ipar, const double *dpar, int pmode, int rmode, int step_mode, const void *model,
+              double *xend, int *info, double *dinfo, float *log, int log_cap, int *log_count, int *queue,
+              int one_per_launch, void *stream) {
+  TrackDev S{nsys, maxvar, maxdim, dim, mono_off, mono_nvr, mono_idx, mono_exp, eq_off, term_off, term_mono, term_a,
+             term_b, jg_off, jg_term, jg_slot};
+  return track(S, make_par(ipar, dpar, step_mode), nmono_max, npaths, path_sys, x0, pmode, rmode,
+               step_mode ? model : nullptr, xend, info, dinfo, log, log_cap, log_count, queue, one_per_launch,
+               (cudaStream_t)stream);
+}
+
+int phc_track_host(int nsys, const int *dim, int maxvar, const int *mono_off, const int *mono_nvr,
+                   const int *mono_idx, const int *mono_exp, const int *eq_off, const int *term_off,
+                   const int *term_mono, const double *term_a, const double *term_b, int npaths,
+                   const int *path_sys, const double *x0, const int *ipar, const double *dpar, int pmode, int rmode,
+                   int step_mode, const void *model, double *xend, int *info, double *dinfo, void *stream) {
+  PHC_REQUIRE(nsys >= 1 && npaths >= 0, "track_host: bad sizes");
+  int maxdim = 0, nmono_max = 0;
+  for (int s = 0; s < nsys; ++s) {
+    maxdim = dim[s] > maxdim ? dim[s] : maxdim;
+    nmono_max = (mono_off[s + 1] - mono_off[s]) > nmono_max ? (mono_off[s + 1] - mono_off[s]) : nmono_max;
+  }
+  const int neq = eq_off[nsys];
+  const int nterm = term_off[neq];
+  const int nmono = mono_off[nsys];
+  const long long njg = phc_track_gather_count(nsys, mono_off, mono_nvr, eq_off, term_off, term_mono);
+  std::vector<int> jg_off((size_t)neq * maxdim + 1), jg_term(njg > 0 ? njg : 1), jg_slot(njg > 0 ? njg : 1);
+  int rc = phc_track_prepare(nsys, dim, maxvar, mono_off, mono_nvr, mono_idx, eq_off, term_off, term_mono, maxdim,
+                             jg_off.data(), jg_term.data(), jg_slot.data());
+  if (rc) return rc;
+  // one device buffer for everything
+  std::vector<std::pair<const void *, size_t> > ins = {
+      {dim, nsys * 4ul}, {mono_off, (nsys + 1) * 4ul}, {mono_nvr, nmono * 4ul},
+      {mono_idx, (size_t)nmono * maxvar * 4}, {mono_exp, (size_t)nmono * maxvar * 4}, {eq_off, (nsys + 1) * 4ul},
+      {term_off, (neq + 1) * 4ul}, {term_mono, nterm * 4ul}, {term_a, nterm * 16ul}, {term_b, nterm * 16ul},
+      {jg_off.data(), jg_off.size() * 4}, {jg_term.data(), jg_term.size() * 4}, {jg_slot.data(), jg_slot.size() * 4},
+      {path_sys, npaths * 4ul}, {x0, (size_t)npaths * maxdim * 16}, {model, step_mode && model ? 1ul : 0ul}};
+  const size_t model_bytes = (size_t)mlp_model_bytes();
+  size_t total = 0;
+  std::vector<size_t> off;
+  for (size_t i = 0; i < ins.size(); ++i) {
+    off.push_back(total);
+    const size_t b = (i + 1 == ins.size()) ? (ins[i].second ? model_bytes : 0) : ins[i].second;
+    total += (b + 255) & ~size_t(255);
+  }
+  const size_t o_xend = total;
+  total += (((size_t)npaths * maxdim * 64) + 255) & ~size_t(255);
+  const size_t o_info = total;
+  total += (((size_t)npaths * 12) + 255) & ~size_t(255);
+  const size_t o_dinfo = total;
+  total += (((size_t)npaths * 16) + 255) & ~size_t(255);
+  const size_t o_q = total;
+  total += 256;
+  void *buf = nullptr;
+  PHC_CUDA(cudaMalloc(&buf, total));
+  char *b = (char *)buf;
+  cudaStream_t st = (cudaStream_t)stream;
+  int out = PHC_OK;
+  for (size_t i = 0; i < ins.size() && out == PHC_OK; ++i) {
+    const size_t nb = (i + 1 == ins.size()) ? (ins[i].second ? model_bytes : 0) : ins[i].second;
+    if (nb && cudaMemcpyAsync(b + off[i], ins[i].first, nb, cudaMemcpyHostToDevice, st) != cudaSuccess) {
+      set_error("track_host: copy to the device failed");
+      out = PHC_ERR_CUDA;
+    }
+  }
+  if (out == PHC_OK) {
+    auto I = [&](int i) { return (const int *)(b + off[i]); };
+    auto Dp = [&](int i) { return (const double *)(b + off[i]); };
+    out = phc_track(nsys, I(0), maxvar, maxdim, nmono_max, I(1), I(2), I(3), I(4), I(5), I(6), I(7), Dp(8), Dp(9),
+                    I(10), I(11), I(12), npaths, I(13), Dp(14), ipar, dpar, pmode, rmode, step_mode,
+                    step_mode && model ? (const void *)(b + off[15]) : nullptr, (double *)(b + o_xend),
+                    (int *)(b + o_info), (double *)(b + o_dinfo), nullptr, 0, nullptr, (int *)(b + o_q), 0, st);
+  }
+  if (out == PHC_OK) {
+    if (cudaMemcpyAsync(xend, b + o_xend, (size_t)npaths * maxdim * 64, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaMemcpyAsync(info, b + o_info, (size_t)npaths * 12, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaMemcpyAsync(dinfo, b + o_dinfo, (size_t)npaths * 16, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess) {
+      set_error("track_host: %s", cudaGetErrorString(cudaGetLastError()));
+      out = PHC_ERR_CUDA;
+    }
+  }
+  cudaFree(buf);
+  if (out < 0) return out;
+  int fails = 0;
+  for (int p = 0; p < npaths; ++p) fails += info[3 * p] != 0;
+  return fails;
+}
+
+}  // extern "C"

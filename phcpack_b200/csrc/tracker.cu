@@ -1,0 +1,537 @@
+// tracker.cu -- batched series-Pade path tracking on the GPU.
+//
+// A persistent kernel: each CTA repeatedly takes the next path from an
+// on-device work queue (one atomicAdd; no waiting on other CTAs) and tracks
+// it from t = 0 to t = 1, so paths of uneven length balance across the SMs.
+// Per step (the Ada Predictor_Corrector_Loop, predictor_corrector_loops.adb
+// :37-85, restated):
+//   predictor, in PN precision (double or double-double):
+//     Newton on power series in s = t - t0 to degree K, working degree
+//     1, 3, 7, ..., K, each step a block-Toeplitz solve with the QR of J_0
+//     (R^{-1} Q^H formed once per step);
+//     [L/M] Pade approximant per component; pole step pbeta * r, r the
+//     smallest Fabry radius |c_{K-3}/c_{K-2}|; step <= maxsize, cut at t = 1;
+//     predictor feedback: halve until the mixed residual < alpha;
+//   corrector, in double-double: at most corsteps Newton steps, converged
+//     when max |dx| <= tolres, plus one extra step; on failure halve the step;
+//   the step size comes from a learned model when one is given (step_mode
+//     1): a proposal whose corrector fails is rejected and the step is
+//     redone with the plain pole step;
+//   at t = 1: refinement in RN precision (double-double or quad-double) and
+//     classification by the max-norm residual.
+// Every loop is bounded (maxsteps, halvings down to minsize); nothing waits.
+#include "common.cuh"
+#include "tracker.cuh"
+#include "mlp.cuh"
+#include "../../include/phc_b200.h"
+
+namespace phc {
+
+
+struct TrackLayout {
+  long xs, V, G, hs, J, dx, rhs, Q, R, Ri, M, num, den, xp, xc, dxc, hc, Jc, Qc, Rc, Ric, Vc, Gc, wv, dense, feat, mag,
+      degs, hbuf, total;
+};
+
+__host__ __device__ inline TrackLayout track_layout(int n, int K, int M, int nm, int mv, int Wp, int Wr) {
+  TrackLayout L;
+  long o = 0;
+  auto take = [&](long doubles) {
+    long r = o;
+    o += (doubles + 1) & ~1L;  // keep 16-byte alignment
+    return r;
+  };
+  const long K1 = K + 1;
+  // state that lives through a whole step
+  L.xs = take(n * K1 * Wp);
+  L.xc = take(n * Wr);
+  L.num = take(n * K1 * Wp);
+  L.den = take(n * (M + 1) * Wp);
+  L.xp = take(n * Wp);
+  const int Wm = Wp > Wr ? Wp : Wr;
+  L.dense = take(dense_smem_doubles(n, n, Wm));
+  L.feat = take(32);
+  L.mag = take(n * K1);
+  L.degs = take(n);
+  L.hbuf = take(2 * 128 + 8);
+  // scratch of the series Newton and the predictor feedback ...
+  const long ov = o;
+  L.V = take(nm * K1 * Wp);
+  L.G = take(nm * mv * K1 * Wp);
+  L.hs = take(n * K1 * Wp);
+  L.J = take(K1 * n * n * Wp);
+  L.dx = take(K1 * n * Wp);
+  L.rhs = take(n * Wp);
+  L.Q = take(n * n * Wp);
+  L.R = take(n * n * Wp);
+  L.Ri = take(n * n * Wp);
+  L.M = take(n * n * Wp);
+  const long pend = o;
+  // ... overlaid by the scratch of the corrector and the refinement, which
+  // run after the Pade approximants are formed
+  o = ov;
+  L.dxc = take(n * Wr);
+  L.hc = take(n * Wr);
+  L.Jc = take(n * n * Wr);
+  L.Qc = take(n * n * Wr);
+  L.Rc = take(n * n * Wr);
+  L.Ric = take(n * n * Wr);
+  L.Vc = take(nm * Wr);
+  L.Gc = take(nm * mv * Wr);
+  L.wv = take(n * Wr);
+  L.total = o > pend ? o : pend;
+  return L;
+}
+
+template <class N>
+__device__ double cta_maxmag(int n, const double *v, double *red) {
+  double a = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const double m = N::mag(ldn_at<N>(v, i));
+    a = (m > a || m != m) ? m : a;  // NaN propagates
+  }
+  return block_max(a, red);
+}
+
+// Newton at a point in precision N (the corrector and the refinement):
+// x (shared, n numbers) updated in place; returns converged.  lastdx: the
+// last max |dx|.
+template <class N>
+__device__ bool point_newton(const TrackDev &S, int s, int n, double t, double *x, double *dx, double *h, double *Jm,
+                             double *Q, double *Rm, double *Ri, double *Vc, double *Gc, double *w, dense_smem &D,
+                             int maxit, double tol, int extra, double *lastdx) {
+  bool conv = false;
+  int extra_left = extra;
+  *lastdx = 1e300;
+  for (int it = 0; it < maxit + extra; ++it) {
+    if (it >= maxit && !conv) break;
+    hom_eval_cta<N>(S, s, 0, t, x, 1, Vc, Gc, h, Jm);
+    small_qr<N>(n, Q, Jm, Ri, D);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) stn_at<N>(h, i, N::neg(ldn_at<N>(h, i)));
+    __syncthreads();
+    cta_matvec_h<N>(n, Q, h, w);
+    cta_matvec<N>(n, Ri, w, dx);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) stn_at<N>(x, i, N::add(ldn_at<N>(x, i), ldn_at<N>(dx, i)));
+    __syncthreads();
+    const double m = cta_maxmag<N>(n, dx, D.red);
+    *lastdx = m;
+    if (!(m == m) || m > 1e300) return false;
+    if (conv) {
+      if (--extra_left <= 0) break;
+    } else if (m <= tol) {
+      conv = true;
+      if (extra_left <= 0) break;
+    }
+  }
+  return conv;
+}
+
+// max_i |h_i(x, t)| at a point, in precision N
+template <class N>
+__device__ double point_residual(const TrackDev &S, int s, int n, double t, const double *x, double *h, double *Vc,
+                                 double *Gc, dense_smem &D) {
+  hom_eval_cta<N>(S, s, 0, t, x, 1, Vc, Gc, h, nullptr);
+  return cta_maxmag<N>(n, h, D.red);
+}
+
+// Pade [L/M] of component i's series c (K+1 numbers), Gaussian elimination
+// with partial pivoting on the M x M system; Taylor fallback when singular.
+// Curves/standard_rational_approximations.ads:67-100.  Returns the numerator
+// degree used (L, or K for the fallback); the denominator degree is M or 0.
+template <class N>
+__device__ int pade_one(int L, int M, int K, const double *c, double *num, double *den) {
+  typedef typename N::T T;
+  T A[kTrackKmax * kTrackKmax / 4 + 16], b[kTrackKmax / 2 + 8], q[kTrackKmax / 2 + 9];
+  bool ok = true;
+  for (int i = 1; i <= M; ++i) {
+    for (int j = 1; j <= M; ++j) {
+      const int k = L + i - j;
+      A[(i - 1) * M + (j - 1)] = k >= 0 ? ldn_at<N>(c, k) : N::zero();
+    }
+    b[i - 1] = N::neg(ldn_at<N>(c, L + i));
+  }
+  for (int col = 0; col < M && ok; ++col) {
+    int piv = col;
+    double best = N::mag(A[col * M + col]);
+    for (int r = col + 1; r < M; ++r) {
+      const double m = N::mag(A[r * M + col]);
+      if (m > best) { best = m; piv = r; }
+    }
+    if (!(best > 0.0)) { ok = false; break; }
+    if (piv != col) {
+      for (int j = 0; j < M; ++j) { T tt = A[piv * M + j]; A[piv * M + j] = A[col * M + j]; A[col * M + j] = tt; }
+      T tt = b[piv]; b[piv] = b[col]; b[col] = tt;
+    }
+    for (int r = col + 1; r < M; ++r) {
+      const T f = N::div(A[r * M + col], A[col * M + col]);
+      for (int j = col; j < M; ++j) A[r * M + j] = N::sub(A[r * M + j], N::mul(f, A[col * M + j]));
+      b[r] = N::sub(b[r], N::mul(f, b[col]));
+    }
+  }
+  q[0] = N::one();
+  if (ok) {
+    for (int i = M - 1; i >= 0; --i) {
+      T acc = b[i];
+      for (int j = i + 1; j < M; ++j) acc = N::sub(acc, N::mul(A[i * M + j], q[j + 1]));
+      q[i + 1] = N::div(acc, A[i * M + i]);
+    }
+    for (int i = 0; i <= M; ++i) stn_at<N>(den, i, q[i]);
+    for (int i = 0; i <= L; ++i) {
+      T acc = N::zero();
+      for (int j = 0; j <= (i < M ? i : M); ++j) acc = N::add(acc, N::mul(q[j], ldn_at<N>(c, i - j)));
+      stn_at<N>(num, i, acc);
+    }
+    return L;
+  }
+  stn_at<N>(den, 0, N::one());
+  for (int i = 0; i <= K; ++i) stn_at<N>(num, i, ldn_at<N>(c, i));
+  return K;
+}
+
+template <class N>
+__device__ typename N::T horner(const double *a, int deg, const typename N::T &z) {
+  typename N::T acc = ldn_at<N>(a, deg);
+  for (int i = deg - 1; i >= 0; --i) acc = N::add(N::mul(acc, z), ldn_at<N>(a, i));
+  return acc;
+}
+
+// Track the paths of one CTA.  PN: predictor numbers, CN: corrector
+// (double-double), RN: refinement.  Output per path: xend (maxdim complex
+// quad-doubles), info (status, steps, rejected), dinfo (t, residual).
+template <class PN, class CN, class RN>
+__global__ void __launch_bounds__(kTrackThreads)
+    k_track(TrackDev S, TrackParDev P, int npaths, int path_begin, const int *__restrict__ path_sys,
+            const double *__restrict__ x0, int *queue, const float *__restrict__ model, double *__restrict__ xend,
+            int *__restrict__ info, double *__restrict__ dinfo, float *__restrict__ log, int log_cap,
+            int *__restrict__ log_count) {
+  extern __shared__ __align__(16) double sm[];
+  __shared__ int cur;
+  const int K = P.deg;
+  const int Wp = PN::width, Wr = RN::width;
+  const int n_max = S.maxdim;
+  int nm_max = 0;
+  for (int s = 0; s < S.nsys; ++s) nm_max = max(nm_max, S.mono_off[s + 1] - S.mono_off[s]);
+  const TrackLayout L = track_layout(n_max, K, P.dendeg, nm_max, S.maxvar, Wp, Wr);
+  dense_smem D = carve<RN>(sm + L.dense, n_max, n_max);
+  int next_static = blockIdx.x;
+  for (;;) {
+    if (queue) {
+      if (threadIdx.x == 0) cur = atomicAdd(queue, 1);
+      __syncthreads();
+    } else {
+      if (threadIdx.x == 0) cur = next_static;
+      __syncthreads();
+      next_static += gridDim.x;
+    }
+    const int p = cur;
+    __syncthreads();
+    if (p >= npaths) break;
+    const int path = path_begin + p;
+    const int s = path_sys[path];
+    const int n = S.dim[s];
+    double *xc = sm + L.xc;
+    // start point, refined at t = 0
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      const double *z = x0 + ((long)path * n_max + i) * 2;
+      stn_at<CN>(xc, i, cnum<CN>(z[0], z[1]));
+    }
+    __syncthreads();
+    double t = 0.0, dxn;
+    point_newton<CN>(S, s, n, 0.0, xc, sm + L.dxc, sm + L.hc, sm + L.Jc, sm + L.Qc, sm + L.Rc, sm + L.Ric, sm + L.Vc,
+                     sm + L.Gc, sm + L.wv, D, P.corsteps, P.tolres, 1, &dxn);
+    int status = 2, nsteps = 0, nrej = 0;
+    bool failed = false;
+    for (int step_it = 0; step_it < P.maxsteps; ++step_it) {
+      // ---------------- predictor: Newton on power series in PN
+      double *xs = sm + L.xs;
+      for (int t2 = threadIdx.x; t2 < n * (K + 1); t2 += blockDim.x) {
+        const int i = t2 / (K + 1), k = t2 % (K + 1);
+        typename PN::T v = PN::zero();
+        if (k == 0) v = conv_num<CN, PN>::go(ldn_at<CN>(xc, i));
+        stn_at<PN>(xs, t2, v);
+      }
+      __syncthreads();
+      for (int it = 0; it < P.nit; ++it) {
+        int w = (2 << it) - 1;
+        if (w > K) w = K;
+        hom_eval_cta<PN>(S, s, w, t, xs, K + 1, sm + L.V, sm + L.G, sm + L.hs, sm + L.J);
+        // QR of J_0 (copied: small_qr overwrites its argument with R)
+        for (int q = threadIdx.x; q < n * n; q += blockDim.x) stn_at<PN>(sm + L.R, q, ldn_at<PN>(sm + L.J, q));
+        __syncthreads();
+        small_qr<PN>(n, sm + L.Q, sm + L.R, sm + L.Ri, D);
+        // M = R^{-1} Q^H
+        for (int q = threadIdx.x; q < n * n; q += blockDim.x) {
+          const int i = q / n, j = q % n;
+          typename PN::T acc = PN::zero();
+          for (int l = i; l < n; ++l)
+            acc = PN::add(acc, PN::mul(ldn_at<PN>(sm + L.Ri, (long)i * n + l), PN::conj(ldn_at<PN>(sm + L.Q, (long)j * n + l))));
+          stn_at<PN>(sm + L.M, q, acc);
+        }
+        __syncthreads();
+        for (int k = 0; k <= w; ++k) {
+          for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            typename PN::T acc = PN::neg(ldn_at<PN>(sm + L.hs, (long)i * (w + 1) + k));
+            for (int j = 1; j <= k; ++j)
+              for (int l = 0; l < n; ++l)
+                acc = PN::sub(acc, PN::mul(ldn_at<PN>(sm + L.J, ((long)j * n + i) * n + l),
+                                           ldn_at<PN>(sm + L.dx, (long)(k - j) * n + l)));
+            stn_at<PN>(sm + L.rhs, i, acc);
+          }
+          __syncthreads();
+          cta_matvec<PN>(n, sm + L.M, sm + L.rhs, sm + L.dx + (long)k * n * Wp);
+        }
+        for (int t2 = threadIdx.x; t2 < n * (w + 1); t2 += blockDim.x) {
+          const int i = t2 / (w + 1), k = t2 % (w + 1);
+          const long o = (long)i * (K + 1) + k;
+          stn_at<PN>(xs, o, PN::add(ldn_at<PN>(xs, o), ldn_at<PN>(sm + L.dx, (long)k * n + i)));
+        }
+        __syncthreads();
+      }
+      // ---------------- Pade and the pole step
+      int pdeg_i = 0, qdeg_i = 0;
+      double rmin = 1e300;
+      double *num = sm + L.num, *den = sm + L.den;
+      for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const double *ci = xs + (long)i * (K + 1) * Wp;
+        pdeg_i = pade_one<PN>(P.numdeg, P.dendeg, K, ci, num + (long)i * (K + 1) * Wp, den + (long)i * (P.dendeg + 1) * Wp);
+        qdeg_i = (pdeg_i == P.numdeg) ? P.dendeg : 0;
+        const double cd = PN::mag(ldn_at<PN>(ci, K - 2));
+        if (cd != 0.0) rmin = fmin(rmin, PN::mag(ldn_at<PN>(ci, K - 3)) / cd);
+        double *mg = sm + L.mag + (long)i * (K + 1);
+        for (int k = 0; k <= K; ++k) mg[k] = PN::mag(ldn_at<PN>(ci, k));
+      }
+      // per-component Pade degrees go to shared memory for the evaluations
+      int *degs = reinterpret_cast<int *>(sm + L.degs);
+      if (threadIdx.x < n) {
+        degs[2 * threadIdx.x] = pdeg_i;
+        degs[2 * threadIdx.x + 1] = qdeg_i;
+      }
+      const double r = -block_max(-rmin, D.red);
+      const bool rfail = !(r < 1e299);
+      double pole_step = rfail ? P.maxsize : P.pbeta * r;
+      if (pole_step > P.maxsize) pole_step = P.maxsize;
+      double step = pole_step;
+      bool learned = false;
+      float *feat = reinterpret_cast<float *>(sm + L.feat);
+      if ((P.step_mode == 1 && model != nullptr) || log != nullptr) {
+        if (threadIdx.x == 0) track_features(n, K, t, pole_step, sm + L.mag, feat);
+        __syncthreads();
+      }
+      if (P.step_mode == 1 && model != nullptr) {
+        const float lr = mlp_forward_cta(model, feat, reinterpret_cast<float *>(sm + L.hbuf));
+        const double prop = pole_step * exp((double)lr) * P.learn_scale;
+        if (prop > P.minsize && prop == prop) {
+          step = fmin(prop, P.maxsize);
+          learned = true;
+        }
+      }
+      const double step0 = step;
+      bool accepted = false;
+      for (int attempt = 0; attempt < 2 && !accepted; ++attempt) {
+        if (attempt == 1) {
+          // the learned proposal was rejected: redo the step with the plain one
+          if (!learned) break;
+          learned = false;
+          step = pole_step;
+        }
+        if (t + step > 1.0) step = 1.0 - t;
+        // predictor feedback on the mixed residual
+        double *xp = sm + L.xp;
+        bool ok = false;
+        for (int h = 0; h < 64; ++h) {
+          for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            const typename PN::T z = PN::from(step);
+            const int pd = degs[2 * i], qd = degs[2 * i + 1];
+            const typename PN::T nv = horner<PN>(num + (long)i * (K + 1) * Wp, pd, z);
+            const typename PN::T dv = horner<PN>(den + (long)i * (P.dendeg + 1) * Wp, qd, z);
+            stn_at<PN>(xp, i, PN::div(nv, dv));
+          }
+          __syncthreads();
+          hom_eval_cta<PN>(S, s, 0, t + step, xp, 1, sm + L.V, sm + L.G, sm + L.hs, nullptr);
+          // |coefficients(t)| at |x|, one thread per equation
+          double part = 0.0;
+          for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            double ab = 0.0;
+            const int eq = S.eq_off[s] + i;
+            for (int tr = S.term_off[eq]; tr < S.term_off[eq + 1]; ++tr) {
+              const int gm = S.term_mono[tr];
+              double v = hypot(fma(S.term_b[2 * tr], t + step, S.term_a[2 * tr]),
+                               fma(S.term_b[2 * tr + 1], t + step, S.term_a[2 * tr + 1]));
+              for (int u = 0; u < S.mono_nvr[gm]; ++u) {
+                const double xa = PN::mag(ldn_at<PN>(xp, S.mono_idx[(long)gm * S.maxvar + u]));
+                for (int e = 0; e < S.mono_exp[(long)gm * S.maxvar + u]; ++e) v *= xa;
+              }
+              ab += v;
+            }
+            part += PN::mag(ldn_at<PN>(sm + L.hs, i)) / (ab + 1.0);
+          }
+          const double mixres = block_sum<md::num<double, false> >(part, D.red) / n;
+          if (mixres < P.alpha) { ok = true; break; }
+          step *= 0.5;
+          ++nrej;
+          if (step < P.minsize) break;
+        }
+        if (!ok) {
+          if (learned) continue;  // the plain step gets its own feedback
+          failed = true;
+          break;
+        }
+        // corrector with step halving
+        bool cok = false;
+        for (int h = 0; h < 64; ++h) {
+          for (int i = threadIdx.x; i < n; i += blockDim.x)
+            stn_at<CN>(xc, i, conv_num<PN, CN>::go(ldn_at<PN>(xp, i)));
+          __syncthreads();
+          if (point_newton<CN>(S, s, n, t + step, xc, sm + L.dxc, sm + L.hc, sm + L.Jc, sm + L.Qc, sm + L.Rc,
+                               sm + L.Ric, sm + L.Vc, sm + L.Gc, sm + L.wv, D, P.corsteps, P.tolres, 1, &dxn)) {
+            cok = true;
+            break;
+          }
+          ++nrej;
+          if (learned) break;  // rejected proposal: retry with the plain step
+          step *= 0.5;
+          if (step < P.minsize) break;
+          for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            const typename PN::T z = PN::from(step);
+            const int pd = degs[2 * i], qd = degs[2 * i + 1];
+            stn_at<PN>(xp, i, PN::div(horner<PN>(num + (long)i * (K + 1) * Wp, pd, z),
+                                      horner<PN>(den + (long)i * (P.dendeg + 1) * Wp, qd, z)));
+          }
+          __syncthreads();
+        }
+        if (cok) { accepted = true; break; }
+        if (learned) continue;  // rejected proposal: redo with the plain step
+        failed = true;
+        break;
+      }
+      if (failed || !accepted) { failed = true; break; }
+      // training log of (features, accepted step, proposal)
+      if (log != nullptr && threadIdx.x == 0) {
+        const int slot = atomicAdd(log_count, 1);
+        if (slot < log_cap) {
+          float *f = log + (long)slot * 32;
+          for (int q = 0; q < 24; ++q) f[q] = feat[q];
+          f[24] = (float)step;
+          f[25] = (float)pole_step;
+          f[26] = (float)step0;
+          f[27] = (float)t;
+        }
+      }
+      t += step;
+      ++nsteps;
+      if (fabs(1.0 - t) < P.epsilon) { status = 0; break; }
+    }
+    // ---------------- refinement and classification
+    double *xr = sm + L.xc;  // reuse the corrector slots at the refinement width
+    // xc holds CN numbers: widen in place from the top (RN width >= CN width)
+    if (RN::width != CN::width) {  // n <= blockDim.x: one number per thread
+      typename CN::T v = CN::zero();
+      if (threadIdx.x < n) v = ldn_at<CN>(xc, threadIdx.x);
+      __syncthreads();
+      if (threadIdx.x < n) stn_at<RN>(xr, threadIdx.x, conv_num<CN, RN>::go(v));
+      __syncthreads();
+    }
+    double res;
+    if (!failed && status == 0) {
+      point_newton<RN>(S, s, n, 1.0, xr, sm + L.dxc, sm + L.hc, sm + L.Jc, sm + L.Qc, sm + L.Rc, sm + L.Ric,
+                       sm + L.Vc, sm + L.Gc, sm + L.wv, D, P.refine_steps, 0.0, 0, &dxn);
+      res = point_residual<RN>(S, s, n, 1.0, xr, sm + L.hc, sm + L.Vc, sm + L.Gc, D);
+      status = (res <= P.restol) ? 0 : 3;
+    } else {
+      res = point_residual<RN>(S, s, n, t, xr, sm + L.hc, sm + L.Vc, sm + L.Gc, D);
+      status = failed ? 1 : 2;
+    }
+    for (int q = threadIdx.x; q < n_max * 8; q += blockDim.x) {
+      const int i = q / 8, c = q % 8;
+      double v = 0.0;
+      if (i < n) {
+        const int lim = RN::tr::limbs;
+        const int part = c / 4, limb = c % 4;
+        if (limb < lim) v = xr[(long)i * RN::width + part * lim + limb];
+      }
+      xend[((long)path * n_max) * 8 + q] = v;
+    }
+    if (threadIdx.x == 0) {
+      info[3 * path] = status;
+      info[3 * path + 1] = nsteps;
+      info[3 * path + 2] = nrej;
+      dinfo[2 * path] = t;
+      dinfo[2 * path + 1] = res;
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace phc
+
+namespace phc {
+
+long track_smem_bytes(int maxdim, int K, int M, int nmono_max, int maxvar, int pmode, int rmode) {
+  const int Wp = 2 * pmode, Wr = 2 * rmode;
+  return track_layout(maxdim, K, M, nmono_max, maxvar, Wp, Wr).total * (long)sizeof(double);
+}
+
+template <class PN, class CN, class RN>
+static int track_launch(const TrackDev &S, const TrackParDev &P, int nmono_max, int npaths, const int *path_sys,
+                        const double *x0, const void *model, double *xend, int *info, double *dinfo, float *log,
+                        int log_cap, int *log_count, int *queue, int one_per_launch, cudaStream_t st) {
+  const long smem = track_smem_bytes(S.maxdim, P.deg, P.dendeg, nmono_max, S.maxvar, PN::tr::limbs, RN::tr::limbs);
+  if (smem > 227 * 1024) {
+    set_error("track: %ld bytes of shared memory needed (dim %d, degree %d, %d monomials)", smem, S.maxdim, P.deg,
+              nmono_max);
+    return PHC_ERR_LIMIT;
+  }
+  auto kern = k_track<PN, CN, RN>;
+  PHC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const float *mdl = reinterpret_cast<const float *>(model);
+  if (one_per_launch) {
+    // the plain arrangement: one launch (one CTA) per path, back to back
+    for (int p = 0; p < npaths; ++p) {
+      kern<<<1, kTrackThreads, smem, st>>>(S, P, 1, p, path_sys, x0, nullptr, mdl, xend, info, dinfo, log, log_cap,
+                                           log_count);
+      PHC_CHECK_LAUNCH();
+    }
+    return PHC_OK;
+  }
+  int dev = 0, nsm = 148, per = 1;
+  PHC_CUDA(cudaGetDevice(&dev));
+  PHC_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  PHC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, kTrackThreads, smem));
+  if (per < 1) per = 1;
+  long grid = (long)nsm * per;
+  if (grid > npaths) grid = npaths;
+  if (grid < 1) return PHC_OK;
+  PHC_CUDA(cudaMemsetAsync(queue, 0, sizeof(int), st));
+  kern<<<(unsigned)grid, kTrackThreads, smem, st>>>(S, P, npaths, 0, path_sys, x0, queue, mdl, xend, info, dinfo, log,
+                                                     log_cap, log_count);
+  PHC_CHECK_LAUNCH();
+  return PHC_OK;
+}
+
+int track(const TrackDev &S, const TrackParDev &P, int nmono_max, int npaths, const int *path_sys, const double *x0,
+          int pmode, int rmode, const void *model, double *xend, int *info, double *dinfo, float *log, int log_cap,
+          int *log_count, int *queue, int one_per_launch, cudaStream_t st) {
+  PHC_REQUIRE(pmode == 1 || pmode == 2, "track: predictor precision %d not in {1,2}", pmode);
+  PHC_REQUIRE(rmode == 2 || rmode == 4, "track: refinement precision %d not in {2,4}", rmode);
+  PHC_REQUIRE(S.maxdim >= 1 && S.maxdim <= 32, "track: dimension %d not in [1,32]", S.maxdim);
+  PHC_REQUIRE(P.deg >= 3 && P.deg <= kTrackKmax && P.numdeg + P.dendeg == P.deg && P.dendeg <= 8 && P.nit >= 1,
+              "track: need 3 <= deg = numdeg + dendeg <= %d, dendeg <= 8", kTrackKmax);
+  PHC_REQUIRE(queue != nullptr || one_per_launch, "track: the batched launch needs a queue counter");
+  if (npaths == 0) return PHC_OK;
+  typedef md::num<double, true> Z1;
+  typedef md::num<md::dd, true> Z2;
+  typedef md::num<md::qd, true> Z4;
+  if (pmode == 1 && rmode == 2)
+    return track_launch<Z1, Z2, Z2>(S, P, nmono_max, npaths, path_sys, x0, model, xend, info, dinfo, log, log_cap,
+                                    log_count, queue, one_per_launch, st);
+  if (pmode == 1)
+    return track_launch<Z1, Z2, Z4>(S, P, nmono_max, npaths, path_sys, x0, model, xend, info, dinfo, log, log_cap,
+                                    log_count, queue, one_per_launch, st);
+  if (rmode == 2)
+    return track_launch<Z2, Z2, Z2>(S, P, nmono_max, npaths, path_sys, x0, model, xend, info, dinfo, log, log_cap,
+                                    log_count, queue, one_per_launch, st);
+  return track_launch<Z2, Z2, Z4>(S, P, nmono_max, npaths, path_sys, x0, model, xend, info, dinfo, log, log_cap,
+                                  log_count, queue, one_per_launch, st);
+}
+
+}  // namespace phc

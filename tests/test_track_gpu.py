@@ -1,0 +1,92 @@
+"""GPU path tracker against the CPU tracker restatement (oracle).
+
+Criteria: identical endpoint classification per path; endpoints of
+successful paths agree to 1e-26 absolute per component (both are refined in
+double-double at t = 1; quad-double refinement: 1e-50); endpoint residuals
+<= 1e-24; the one-path-per-launch arrangement gives bitwise the same
+results as the batched persistent kernel (same code per path)."""
+import numpy as np
+import pytest
+
+from oracle import pyoracle
+from phcpack_b200 import homotopy as hm
+
+pytestmark = pytest.mark.gpu
+ORC = pyoracle.oracle()
+
+
+def endpoint_diff(pb, xa, xb, limbs):
+    a = xa.reshape(-1, pb.maxdim, 8)
+    b = xb.reshape(-1, pb.maxdim, 8)
+    d = np.zeros(a.shape[:2])
+    for part in (0, 4):
+        acc = np.zeros(a.shape[:2])
+        for l in range(limbs - 1, -1, -1):
+            acc = acc + (a[..., part + l] - b[..., part + l])
+        d = np.maximum(d, np.abs(acc))
+    return d.max(axis=1)
+
+
+@pytest.mark.parametrize("pmode", [1, 2])
+def test_track_config4_sample_vs_oracle(pmode):
+    pb = hm.subset(hm.config4(), np.arange(0, 1024, 16))
+    ipar, dpar = hm.params()
+    g = hm.track_host(pb, pmode=pmode, rmode=2)
+    xo, io, do = pyoracle.track(ORC, pb, ipar, dpar, pmode=pmode, rmode=2, nthreads=8)
+    io = io.reshape(-1, 3)
+    assert np.array_equal(g.status, io[:, 0])
+    ok = g.status == 0
+    assert ok.mean() > 0.9
+    assert (g.residual[ok] <= 1e-24).all()
+    assert (endpoint_diff(pb, g.xend, xo, 2)[ok] <= 1e-26).all()
+    # step counts follow the same rules; rounding may move a few decisions
+    assert np.abs(g.steps - io[:, 1]).max() <= 3
+
+
+def test_track_quad_double_refinement():
+    pb = hm.subset(hm.config4(), [1, 77, 300, 901])
+    ipar, dpar = hm.params(restol=1e-50)
+    g = hm.track_host(pb, pmode=1, rmode=4, restol=1e-50)
+    xo, io, _ = pyoracle.track(ORC, pb, ipar, dpar, pmode=1, rmode=4)
+    assert np.array_equal(g.status, io.reshape(-1, 3)[:, 0])
+    ok = g.status == 0
+    assert ok.all()
+    assert (endpoint_diff(pb, g.xend, xo, 4)[ok] <= 1e-50).all()
+
+
+def test_one_path_per_launch_matches_batched():
+    import torch
+    pb = hm.subset(hm.config4(), np.arange(0, 1024, 64))
+    dt = hm.DeviceTracker(pb)
+    dt.run(pmode=2, rmode=2)
+    torch.cuda.synchronize()
+    a = dt.result()
+    dt.run(pmode=2, rmode=2, one_per_launch=True)
+    torch.cuda.synchronize()
+    b = dt.result()
+    assert np.array_equal(a.xend, b.xend) and np.array_equal(a.status, b.status)
+    assert np.array_equal(a.steps, b.steps)
+
+
+def test_track_mixed_sizes_vs_oracle():
+    # the 64-system mixed-size workload, a few paths of several systems
+    pb5 = hm.config5()
+    pick = np.concatenate([np.nonzero(pb5.path_sys == s)[0][:3] for s in range(0, 64, 8)])
+    pb = hm.subset(pb5, pick)
+    ipar, dpar = hm.params()
+    g = hm.track_host(pb, pmode=1, rmode=2)
+    xo, io, do = pyoracle.track(ORC, pb, ipar, dpar, pmode=1, rmode=2, nthreads=8)
+    assert np.array_equal(g.status, io.reshape(-1, 3)[:, 0])
+    ok = g.status == 0
+    assert (endpoint_diff(pb, g.xend, xo, 2)[ok] <= 1e-26 * np.maximum(1, np.abs(g.endpoints(pb.maxdim)).max(axis=1)[ok])).all()
+
+
+def test_track_device_entry_matches_host_entry():
+    import torch
+    pb = hm.subset(hm.config4(), [5, 6, 7, 8])
+    h = hm.track_host(pb, pmode=1, rmode=2)
+    dt = hm.DeviceTracker(pb)
+    dt.run(pmode=1, rmode=2)
+    torch.cuda.synchronize()
+    d = dt.result()
+    assert np.array_equal(h.xend, d.xend) and np.array_equal(h.status, d.status)
