@@ -65,6 +65,20 @@ __device__ __forceinline__ double block_max(double a, double *red) {
   return s;
 }
 
+// Block-wide minimum of one double per thread (any sign).
+__device__ __forceinline__ double block_min(double a, double *red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) a = fmin(a, __shfl_xor_sync(0xffffffffu, a, o));
+  __syncthreads();
+  if (lane == 0) red[warp] = a;
+  __syncthreads();
+  double s = red[0];
+  for (int w = 1; w < nw; ++w) s = fmin(s, red[w]);
+  __syncthreads();
+  return s;
+}
+
 // max_i |leading limb| of v (complex: |re| + |im|): the "1-norm" of the
 // reference's skip rules, Newton/dbl_onenorms_host.cpp:9,20
 template <class N>

@@ -88,7 +88,7 @@ __device__ double cta_maxmag(int n, const double *v, double *red) {
   double a = 0.0;
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
     const double m = N::mag(ldn_at<N>(v, i));
-    a = (m > a || m != m) ? m : a;  // NaN propagates
+    a = (m != m) ? INFINITY : fmax(a, m);  // a NaN reads as infinity
   }
   return block_max(a, red);
 }
@@ -306,7 +306,7 @@ __global__ void __launch_bounds__(kTrackThreads)
         degs[2 * threadIdx.x] = pdeg_i;
         degs[2 * threadIdx.x + 1] = qdeg_i;
       }
-      const double r = -block_max(-rmin, D.red);
+      const double r = block_min(rmin, D.red);
       const bool rfail = !(r < 1e299);
       double pole_step = rfail ? P.maxsize : P.pbeta * r;
       if (pole_step > P.maxsize) pole_step = P.maxsize;
