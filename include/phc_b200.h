@@ -101,6 +101,21 @@ int phc_bals_solve(int prec, int cplx, int ninst, int dim, int degp1, int szt, i
 int phc_bals_solve_host(int prec, int cplx, int ninst, int dim, int degp1, int szt, int tailidx, const double *mat,
                         double *rhs, double *sol, double *Q, double *R, int *flags, void *stream);
 
+/* phc_bals_solve without any allocation.  No counterpart in the reference:
+ * this entry point is for callers that cannot let a library call cudaMalloc
+ * or cudaFree (work recorded into a CUDA graph under stream capture,
+ * latency-critical callers that cannot afford cudaFree's device-wide
+ * synchronisation, frameworks whose own allocator owns all device memory).
+ * Same arguments and results as phc_bals_solve minus the workspace, which
+ * is a static device array of phc_bals_solve_static_capacity_bytes() bytes
+ * (8 MiB, held by every GPU that loads the library until exit); larger
+ * requests fail with -3.  All calls share that array: calls that overlap on
+ * the GPU race and must be serialised.  The first call on a device looks up
+ * the array's address and should come before any stream capture. */
+long long phc_bals_solve_static_capacity_bytes(void);
+int phc_bals_solve_static(int prec, int cplx, int ninst, int dim, int degp1, int szt, int tailidx, const double *mat,
+                          double *rhs, double *sol, double *Q, double *R, int *flags, void *stream);
+
 /* One Newton step on power series for nsys systems (row form) at working
  * degree deg <= maxdeg: evaluate and differentiate (phc_system_evaldiff),
  * linearise (matrix series -> series of matrices, rhs = -f), solve
