@@ -41,7 +41,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default=os.environ.get("PHC_BENCH_WORKLOAD", "eval"),
+    ap.add_argument("--workload", default=os.environ.get("PHC_BENCH_WORKLOAD", "track"),
                     choices=["track", "eval", "qr"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="budget of the CPU baseline sample")
     return ap.parse_args()
@@ -195,6 +195,8 @@ def main():
         dist.all_reduce(ts, op=dist.ReduceOp.MAX)
     total_s = float(ts.item())
 
+    if hasattr(work, "finish"):
+        work.finish()
     # end to end through the host entry point (pinned host buffers in, results out)
     e2e = work.e2e(stream, reps=max(1, min(3, args.steps)))
     check = work.check()

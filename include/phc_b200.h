@@ -196,8 +196,25 @@ int phc_track_host(int nsys, const int *dim, int maxvar, const int *mono_off, co
                    const int *term_mono, const double *term_a, const double *term_b, int npaths,
                    const int *path_sys, const double *x0, const int *ipar, const double *dpar, int pmode, int rmode,
                    int step_mode, const void *model, double *xend, int *info, double *dinfo, void *stream);
-/* Size in bytes of a learned step model (24 -> 128 -> 128 -> 1, BF16). */
+/* ------------------------------------------------------- learned step size
+ * No counterpart in the reference (its trackers use the ratio / Pade pole
+ * and curvature steps only).  A 24 -> 128 -> 128 -> 1 ReLU network predicts
+ * log(accepted step / pole step) from 24 features of the predictor's series
+ * (phcpack_b200/csrc/mlp.cuh).  Model buffer: FP32 normalisation and biases,
+ * BF16 weights, phc_mlp_model_bytes() bytes.  Training keeps FP32 master
+ * parameters (phc_mlp_param_count() floats: W1[128][24], b1[128],
+ * W2[128][128], b2[128], W3[128], b3) and Adam moments of the same size. */
 long long phc_mlp_model_bytes(void);
+long long phc_mlp_param_count(void);
+/* params + normalisation (24 means, 24 inverse deviations) -> model buffer */
+int phc_mlp_pack(const float *params, const float *mean, const float *inv_std, void *model, void *stream);
+/* out[b] = network(X[b]) for nb samples of 24 floats */
+int phc_mlp_forward(const void *model, int nb, const float *X, float *out, void *stream);
+/* grad += d/dparams of the mean squared error over (X, y); loss += that error */
+int phc_mlp_grad(const void *model, int nb, const float *X, const float *y, float *grad, float *loss, void *stream);
+/* one Adam step (t >= 1) on params from grad, which is cleared */
+int phc_mlp_adam(float *params, float *grad, float *m, float *v, float lr, float beta1, float beta2, float eps,
+                 int t, void *stream);
 
 #ifdef __cplusplus
 }

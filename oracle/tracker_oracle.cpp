@@ -16,7 +16,8 @@
 // restated and what is left out:
 //  * predictor: Newton on power series in s = t - t0 to degree K (working
 //    degree doubling 1, 3, 7, ... K), each step a block-Toeplitz solve with
-//    the QR of J_0; [L/M] Pade approximant per component; pole step
+//    the QR of J_0 (factored once per step and reused, as the reference's
+//    noqr rule does); [L/M] Pade approximant per component; pole step
 //    pbeta * r with r the smallest Fabry radius |c_{K-3}/c_{K-2}| (offset 2
 //    as in Newton_Fabry); step = min(pole step, maxsize), cut at t = 1;
 //  * the Hessian curvature step (Hesse_Pade, singular values of Hessians)
@@ -193,8 +194,10 @@ static void series_newton(const TrackSys &S, int s, const TrackPar &P, double t0
     for (int i = 0; i < n; ++i)
       for (int k = 0; k <= w; ++k) xw[i][k] = x[i][k];
     hom_eval(S, s, w, t0, xw, h, &jac);
-    for (int l = 0; l < n * n; ++l) A[l] = jac[l];
-    qr.factor(n, A);
+    if (it == 0) {  // J_0 factored once per step, reused by later iterations
+      for (int l = 0; l < n * n; ++l) A[l] = jac[l];
+      qr.factor(n, A);
+    }
     for (int k = 0; k <= w; ++k) {
       for (int i = 0; i < n; ++i) {
         T acc = -h[i][k];

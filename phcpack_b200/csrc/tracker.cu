@@ -8,7 +8,7 @@
 //   predictor, in PN precision (double or double-double):
 //     Newton on power series in s = t - t0 to degree K, working degree
 //     1, 3, 7, ..., K, each step a block-Toeplitz solve with the QR of J_0
-//     (R^{-1} Q^H formed once per step);
+//     (factored and R^{-1} Q^H formed once per predictor step);
 //     [L/M] Pade approximant per component; pole step pbeta * r, r the
 //     smallest Fabry radius |c_{K-3}/c_{K-2}|; step <= maxsize, cut at t = 1;
 //     predictor feedback: halve until the mixed residual < alpha;
@@ -195,6 +195,43 @@ __device__ typename N::T horner(const double *a, int deg, const typename N::T &z
   return acc;
 }
 
+// Evaluate the Pade approximants at step st into xp, and return the mixed
+// residual (1/n) sum_i |h_i(xp, t+st)| / (|h|_i(|xp|, t+st) + 1) of
+// Solutions/standard_mixed_residuals.adb:472, where |h| has the moduli of
+// the coefficients at t+st.  Predictor_Feedback,
+// Curves/standard_predictor_convolutions.adb:958-993.
+template <class PN>
+__device__ double pade_mixres(const TrackDev &S, int s, int n, int K, int dendeg, double t, double st,
+                              const double *num, const double *den, const int *degs, double *xp, double *V,
+                              double *G, double *hs, dense_smem &D) {
+  const int Wp = PN::width;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const typename PN::T z = PN::from(st);
+    const typename PN::T nv = horner<PN>(num + (long)i * (K + 1) * Wp, degs[2 * i], z);
+    const typename PN::T dv = horner<PN>(den + (long)i * (dendeg + 1) * Wp, degs[2 * i + 1], z);
+    stn_at<PN>(xp, i, PN::div(nv, dv));
+  }
+  __syncthreads();
+  hom_eval_cta<PN>(S, s, 0, t + st, xp, 1, V, G, hs, nullptr);
+  double part = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    double ab = 0.0;
+    const int eq = S.eq_off[s] + i;
+    for (int tr = S.term_off[eq]; tr < S.term_off[eq + 1]; ++tr) {
+      const int gm = S.term_mono[tr];
+      double v = hypot(fma(S.term_b[2 * tr], t + st, S.term_a[2 * tr]),
+                       fma(S.term_b[2 * tr + 1], t + st, S.term_a[2 * tr + 1]));
+      for (int u = 0; u < S.mono_nvr[gm]; ++u) {
+        const double xa = PN::mag(ldn_at<PN>(xp, S.mono_idx[(long)gm * S.maxvar + u]));
+        for (int e = 0; e < S.mono_exp[(long)gm * S.maxvar + u]; ++e) v *= xa;
+      }
+      ab += v;
+    }
+    part += PN::mag(ldn_at<PN>(hs, i)) / (ab + 1.0);
+  }
+  return block_sum<md::num<double, false> >(part, D.red) / n;
+}
+
 // Track the paths of one CTA.  PN: predictor numbers, CN: corrector
 // (double-double), RN: refinement.  Output per path: xend (maxdim complex
 // quad-doubles), info (status, steps, rejected), dinfo (t, residual).
@@ -255,19 +292,26 @@ __global__ void __launch_bounds__(kTrackThreads)
         int w = (2 << it) - 1;
         if (w > K) w = K;
         hom_eval_cta<PN>(S, s, w, t, xs, K + 1, sm + L.V, sm + L.G, sm + L.hs, sm + L.J);
-        // QR of J_0 (copied: small_qr overwrites its argument with R)
-        for (int q = threadIdx.x; q < n * n; q += blockDim.x) stn_at<PN>(sm + L.R, q, ldn_at<PN>(sm + L.J, q));
-        __syncthreads();
-        small_qr<PN>(n, sm + L.Q, sm + L.R, sm + L.Ri, D);
-        // M = R^{-1} Q^H
-        for (int q = threadIdx.x; q < n * n; q += blockDim.x) {
-          const int i = q / n, j = q % n;
-          typename PN::T acc = PN::zero();
-          for (int l = i; l < n; ++l)
-            acc = PN::add(acc, PN::mul(ldn_at<PN>(sm + L.Ri, (long)i * n + l), PN::conj(ldn_at<PN>(sm + L.Q, (long)j * n + l))));
-          stn_at<PN>(sm + L.M, q, acc);
+        if (it == 0) {
+          // QR of J_0 once per step: the corrected point changes the
+          // constant term only at roundoff level in later iterations (the
+          // reuse the reference makes with its noqr rule,
+          // Newton/dbl2_bals_host.cpp:43-60).  small_qr overwrites its
+          // argument with R, so J_0 is copied first.
+          for (int q = threadIdx.x; q < n * n; q += blockDim.x) stn_at<PN>(sm + L.R, q, ldn_at<PN>(sm + L.J, q));
+          __syncthreads();
+          small_qr<PN>(n, sm + L.Q, sm + L.R, sm + L.Ri, D);
+          // M = R^{-1} Q^H
+          for (int q = threadIdx.x; q < n * n; q += blockDim.x) {
+            const int i = q / n, j = q % n;
+            typename PN::T acc = PN::zero();
+            for (int l = i; l < n; ++l)
+              acc = PN::add(acc, PN::mul(ldn_at<PN>(sm + L.Ri, (long)i * n + l),
+                                         PN::conj(ldn_at<PN>(sm + L.Q, (long)j * n + l))));
+            stn_at<PN>(sm + L.M, q, acc);
+          }
+          __syncthreads();
         }
-        __syncthreads();
         for (int k = 0; k <= w; ++k) {
           for (int i = threadIdx.x; i < n; i += blockDim.x) {
             typename PN::T acc = PN::neg(ldn_at<PN>(sm + L.hs, (long)i * (w + 1) + k));
@@ -339,33 +383,8 @@ __global__ void __launch_bounds__(kTrackThreads)
         double *xp = sm + L.xp;
         bool ok = false;
         for (int h = 0; h < 64; ++h) {
-          for (int i = threadIdx.x; i < n; i += blockDim.x) {
-            const typename PN::T z = PN::from(step);
-            const int pd = degs[2 * i], qd = degs[2 * i + 1];
-            const typename PN::T nv = horner<PN>(num + (long)i * (K + 1) * Wp, pd, z);
-            const typename PN::T dv = horner<PN>(den + (long)i * (P.dendeg + 1) * Wp, qd, z);
-            stn_at<PN>(xp, i, PN::div(nv, dv));
-          }
-          __syncthreads();
-          hom_eval_cta<PN>(S, s, 0, t + step, xp, 1, sm + L.V, sm + L.G, sm + L.hs, nullptr);
-          // |coefficients(t)| at |x|, one thread per equation
-          double part = 0.0;
-          for (int i = threadIdx.x; i < n; i += blockDim.x) {
-            double ab = 0.0;
-            const int eq = S.eq_off[s] + i;
-            for (int tr = S.term_off[eq]; tr < S.term_off[eq + 1]; ++tr) {
-              const int gm = S.term_mono[tr];
-              double v = hypot(fma(S.term_b[2 * tr], t + step, S.term_a[2 * tr]),
-                               fma(S.term_b[2 * tr + 1], t + step, S.term_a[2 * tr + 1]));
-              for (int u = 0; u < S.mono_nvr[gm]; ++u) {
-                const double xa = PN::mag(ldn_at<PN>(xp, S.mono_idx[(long)gm * S.maxvar + u]));
-                for (int e = 0; e < S.mono_exp[(long)gm * S.maxvar + u]; ++e) v *= xa;
-              }
-              ab += v;
-            }
-            part += PN::mag(ldn_at<PN>(sm + L.hs, i)) / (ab + 1.0);
-          }
-          const double mixres = block_sum<md::num<double, false> >(part, D.red) / n;
+          const double mixres = pade_mixres<PN>(S, s, n, K, P.dendeg, t, step, num, den, degs, xp, sm + L.V,
+                                                sm + L.G, sm + L.hs, D);
           if (mixres < P.alpha) { ok = true; break; }
           step *= 0.5;
           ++nrej;
@@ -405,16 +424,32 @@ __global__ void __launch_bounds__(kTrackThreads)
         break;
       }
       if (failed || !accepted) { failed = true; break; }
-      // training log of (features, accepted step, proposal)
-      if (log != nullptr && threadIdx.x == 0) {
-        const int slot = atomicAdd(log_count, 1);
-        if (slot < log_cap) {
-          float *f = log + (long)slot * 32;
-          for (int q = 0; q < 24; ++q) f[q] = feat[q];
-          f[24] = (float)step;
-          f[25] = (float)pole_step;
-          f[26] = (float)step0;
-          f[27] = (float)t;
+      // training log: features, accepted step, plain step, proposal, t and
+      // the largest probed step (pole step times 1.5, 2, 3, 4, 6, at most
+      // maxsize and 1 - t) whose Pade prediction still passes the feedback
+      if (log != nullptr) {
+        double best = step;
+        const double mults[5] = {1.5, 2.0, 3.0, 4.0, 6.0};
+        for (int q = 0; q < 5; ++q) {
+          double sp = fmin(pole_step * mults[q], P.maxsize);
+          if (t + sp > 1.0) sp = 1.0 - t;
+          if (sp <= best) continue;
+          const double mr = pade_mixres<PN>(S, s, n, K, P.dendeg, t, sp, num, den, degs, sm + L.xp, sm + L.V,
+                                            sm + L.G, sm + L.hs, D);
+          if (mr < P.alpha) best = sp;
+        }
+        if (threadIdx.x == 0) {
+          const int slot = atomicAdd(log_count, 1);
+          if (slot < log_cap) {
+            float *f = log + (long)slot * 32;
+            for (int q = 0; q < 24; ++q) f[q] = feat[q];
+            f[24] = (float)step;
+            f[25] = (float)pole_step;
+            f[26] = (float)step0;
+            f[27] = (float)t;
+            f[28] = (float)best;
+            for (int q = 29; q < 32; ++q) f[q] = 0.0f;
+          }
         }
       }
       t += step;

@@ -245,8 +245,10 @@ def _result(xend, info, dinfo):
                        dinfo[:, 1].copy())
 
 
-def track_host(pb: TrackProblem, pmode=1, rmode=2, step_mode=0, model=None, **kw) -> TrackResult:
-    """Track every path of pb on the GPU (host arrays in and out)."""
+def track_host(pb: TrackProblem, pmode=1, rmode=2, step_mode=0, model=None, stream_ptr=0, **kw) -> TrackResult:
+    """Track every path of pb on the GPU (host arrays in and out), the shape
+    of gpumanypaths_dd: start solutions in, end points and per-path status
+    out.  stream_ptr: a cudaStream_t as an int (0 = default stream)."""
     ipar, dpar = params(**kw)
     xend = np.zeros(pb.npaths * pb.maxdim * 8)
     info = np.zeros(pb.npaths * 3, np.int32)
@@ -256,7 +258,7 @@ def track_host(pb: TrackProblem, pmode=1, rmode=2, step_mode=0, model=None, **kw
               _lib.ptr(pb.mono_idx), _lib.ptr(pb.mono_exp), _lib.ptr(pb.eq_off), _lib.ptr(pb.term_off),
               _lib.ptr(pb.term_mono), _lib.ptr(pb.term_a), _lib.ptr(pb.term_b), pb.npaths, _lib.ptr(pb.path_sys),
               _lib.ptr(pb.x0), _lib.ptr(ipar), _lib.ptr(dpar), pmode, rmode, step_mode, _lib.ptr(m),
-              _lib.ptr(xend), _lib.ptr(info), _lib.ptr(dinfo), _lib.c_void_p(0))
+              _lib.ptr(xend), _lib.ptr(info), _lib.ptr(dinfo), _lib.c_void_p(stream_ptr))
     return _result(xend, info, dinfo)
 
 

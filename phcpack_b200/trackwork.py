@@ -1,0 +1,188 @@
+"""bench.py workload 'track': path tracking on the 1024-path dense quadratic
+homotopy (n = 10, unit-circle coefficients, total-degree start system,
+random complex gamma), degree-8 series, [4/4] Pade, 3 double-double
+corrector steps, endpoints refined in double-double.
+
+The measured arm is the batched persistent tracker with the FP64 predictor
+and the double-double corrector, using the learned step proposer when a
+trained model is available (phcpack_b200/models/step_mlp.npz).  Next to it
+the same run is timed as the plain arrangement: all double-double, one path
+per launch.
+"""
+from __future__ import annotations
+
+import os
+import time
+
+import numpy as np
+
+from . import _lib
+from . import homotopy as hm
+from .benchwork import MD_ADD, MD_MUL, _threads_run, cpu_info
+
+MODEL_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "models", "step_mlp.npz")
+
+
+def load_model_bytes():
+    if not os.path.exists(MODEL_PATH):
+        return None
+    with np.load(MODEL_PATH) as z:
+        return np.ascontiguousarray(z["model"])
+
+
+def track_flops(pb: hm.TrackProblem, steps, rejected, pmode=1):
+    """Algorithmic work of the tracked paths, a count of complex
+    multiply-adds per phase weighted with the reference's convention
+    (double-double add 20, mul 23; double 1 and 1; complex product = 4
+    multiplications + 2 additions, accumulation 2 additions):
+      series Newton (4 steps at working degrees 1, 3, 7, 8): per step one
+        evaluation (a series product per distinct monomial, the coefficient
+        gathers), the QR of J_0 with explicit Q, R^{-1} and R^{-1} Q^H
+        (about 4 n^3), the block-Toeplitz solve ((w+1)(w+2)/2 n^2);
+      predictor feedback: one point evaluation;
+      corrector: 2 double-double Newton iterations (point evaluation, 4 n^3);
+      a rejected step costs one feedback and one corrector.
+    Returns (flops, the cost weights used)."""
+    n = pb.maxdim
+    nmono = pb.nmono_max
+    nterm = int(np.diff(pb.term_off).mean())
+    njg = 2 * nterm  # Jacobian gather entries per equation (quadratic monomials)
+
+    def cma(prec):  # flops of one complex multiply-add in precision prec
+        return 4 * MD_MUL[prec] + 4 * MD_ADD[prec]
+
+    def series_eval(w):
+        conv = (w + 1) * (w + 2) // 2
+        return nmono * conv + 2 * (n * (w + 1) * nterm + n * (w + 1) * njg)
+
+    def newton_step(w):
+        return series_eval(w) + 4 * n ** 3 + (w + 1) * (w + 2) // 2 * n * n
+
+    pred = sum(newton_step(w) for w in (1, 3, 7, 8)) * cma(pmode)
+    feed = series_eval(0) * cma(pmode)
+    corr = 2 * (series_eval(0) + 4 * n ** 3 + n * n) * cma(2)
+    steps = np.asarray(steps, dtype=np.float64)
+    rej = np.asarray(rejected, dtype=np.float64)
+    total = float((steps * (pred + feed + corr) + rej * (feed + corr)).sum())
+    return total
+
+
+class TrackWork:
+    metric = ("paths/s at endpoint residual <= 1e-24 (double-double), batched + precision-split"
+              " + learned-step tracker, 1024-path dense quadratic homotopy")
+    unit = "paths/s"
+    dtype = "f64 predictor + double-double corrector (complex)"
+    kernel_tag = "k_track_config4"
+    dominant_launches_per_step = 1
+
+    def __init__(self, torch, dev, rank, npaths=1024):
+        self.torch = torch
+        pb = hm.config4(seed=4 + rank)
+        if npaths < pb.npaths:
+            pb = hm.subset(pb, np.arange(npaths))
+        self.pb = pb
+        self.dt = hm.DeviceTracker(pb, device=dev)
+        self.model = load_model_bytes()
+        self.step_mode = 1 if self.model is not None else 0
+        if self.model is not None:
+            self.dt.set_model(self.model)
+        self.units_per_step = pb.npaths
+        self.l2_note = "working set (systems, paths, endpoints) < L2; the step is latency bound, not memory bound"
+        self.config = {"workload": "path tracking: dense quadratic n=10, 1024 total-degree paths, degree-8 series, "
+                                   "[4/4] Pade, 3 dd corrector steps, dd endpoint refinement",
+                       "paths": pb.npaths, "dim": pb.maxdim, "predictor": "fp64", "corrector": "double-double",
+                       "step": "learned (MLP) with plain fallback" if self.step_mode else "plain pole step",
+                       "system": pb.note}
+        self.flops_note = None
+        self.dominant_flops_per_launch = 0.0
+        self.dominant_bytes_per_launch = float(pb.npaths * pb.maxdim * (16 + 64))
+
+    def step(self, stream):
+        self.dt.run(pmode=1, rmode=2, step_mode=self.step_mode, stream=stream)
+        return 1
+
+    def finish(self):
+        """After the timed steps: per-path counters of the last run give the
+        algorithmic flops per launch."""
+        r = self.dt.result()
+        self.last = r
+        self.dominant_flops_per_launch = track_flops(self.pb, r.steps, r.rejected, pmode=1)
+        self.flops_note = ("modelled complex multiply-adds per phase (trackwork.track_flops), reference weights "
+                           "dd add 20 mul 23, double 1; from the launch's own step and rejection counts")
+        return r
+
+    def e2e(self, stream, reps=2):
+        torch = self.torch
+        times = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            r = hm.track_host(self.pb, pmode=1, rmode=2, step_mode=self.step_mode, model=self.model,
+                              stream_ptr=stream.cuda_stream)
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1) / 1e3)
+        t = float(np.median(times))
+        pb = self.pb
+        h2d = (pb.dim.nbytes + pb.mono_off.nbytes + pb.mono_nvr.nbytes + pb.mono_idx.nbytes + pb.mono_exp.nbytes
+               + pb.eq_off.nbytes + pb.term_off.nbytes + pb.term_mono.nbytes + pb.term_a.nbytes + pb.term_b.nbytes
+               + pb.path_sys.nbytes + pb.x0.nbytes)
+        d2h = pb.npaths * (pb.maxdim * 64 + 12 + 16)
+        return {"value": pb.npaths / t, "unit": self.unit, "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h), "path": "phc_track_host",
+                "success": int((r.status == 0).sum())}
+
+    def plain(self, stream):
+        """The plain arrangement: all double-double, plain pole step, one
+        path per launch."""
+        torch = self.torch
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        self.dt.run(pmode=2, rmode=2, step_mode=0, one_per_launch=True, stream=stream)  # warm
+        torch.cuda.synchronize()
+        e0.record(stream)
+        self.dt.run(pmode=2, rmode=2, step_mode=0, one_per_launch=True, stream=stream)
+        e1.record(stream)
+        e1.synchronize()
+        t = e0.elapsed_time(e1) / 1e3
+        r = self.dt.result()
+        return t, r
+
+    def check(self):
+        torch = self.torch
+        out = {}
+        r = getattr(self, "last", None) or self.dt.result()
+        ok = r.status == 0
+        out["success"] = int(ok.sum())
+        out["max_residual_success"] = float(r.residual[ok].max()) if ok.any() else None
+        out["mean_steps"] = float(r.steps.mean())
+        out["rejected"] = int(r.rejected.sum())
+        s = torch.cuda.Stream(device=self.dt.xend.device)
+        tp, rp = self.plain(s)
+        out["plain_one_path_per_launch"] = {"paths_per_s": self.pb.npaths / tp, "seconds": tp,
+                                            "success": int((rp.status == 0).sum()),
+                                            "mean_steps": float(rp.steps.mean()),
+                                            "same_classification": bool(np.array_equal(rp.status == 0, ok))}
+        return out
+
+
+def cpu_sample(seconds):
+    """The CPU tracker (oracle restatement of the Ada series-Pade tracker) on
+    a sample of the 1024 paths, all host cores."""
+    from oracle import pyoracle
+    model, cores = cpu_info()
+    pb = hm.config4()
+    ipar, dpar = hm.params()
+    lib = pyoracle.oracle()
+    t = time.perf_counter()
+    one = hm.subset(pb, [0])
+    pyoracle.track(lib, one, ipar, dpar, pmode=1, rmode=2, nthreads=1)
+    t1 = time.perf_counter() - t
+    n = int(min(pb.npaths, max(cores, seconds / max(t1, 1e-6) * cores * 0.8)))
+    sub = hm.subset(pb, np.arange(n))
+    t = time.perf_counter()
+    _, info, _ = pyoracle.track(lib, sub, ipar, dpar, pmode=1, rmode=2, nthreads=cores)
+    el = time.perf_counter() - t
+    ok = int((info.reshape(-1, 3)[:, 0] == 0).sum())
+    return {"value": n / el, "unit": "paths/s", "cores": cores, "kind": "port",
+            "sample": f"{n} of the 1024 paths, {ok} successful, {cores} threads (std::thread), CPU: {model}; the "
+                      "reference's tracker is Ada (no GNAT here), so this is the C++ restatement"}
