@@ -102,6 +102,10 @@ def config2_device(torch, dev, nsys=4096, dim=32, deg=31, nmon=32, maxvar=4, exp
                 exps=exps, cst=cst, cff=cff, input=inp)
 
 
+EVAL_WORKLOAD = ("eval/diff: 4096 systems, n=32, 32 monomials/polynomial over <=4 variables, exponents {1,2,3}, "
+                 "unit-circle coefficients, degree 31, complex dd")
+
+
 class EvalWork:
     metric = "systems/s, batched eval/diff of polynomial systems at power series (complex double-double)"
     unit = "systems/s"
@@ -124,9 +128,7 @@ class EvalWork:
         self.dominant_bytes_per_launch = float(in_bytes + self.out.numel() * 8)
         self.flops_note = ("reference op weights: dd add 20, mul 23, complex x4 per convolution; "
                            f"{nconv} convolutions of degree {d['deg']} per step")
-        self.config = {"workload": "eval/diff: 4096 systems, n=32, 32 monomials/polynomial over <=4 variables, "
-                                   "exponents {1,2,3}, unit-circle coefficients, degree 31, complex dd",
-                       "systems": d["nsys"], "dim": d["dim"], "degree": d["deg"]}
+        self.config = {"workload": EVAL_WORKLOAD, "systems": d["nsys"], "dim": d["dim"], "degree": d["deg"]}
         self.host = None
 
     def _args(self, stream_ptr, out_ptr, host=None):
@@ -265,10 +267,16 @@ def reference_arm(args):
         if k >= args.warmup and res and res.get("value"):
             vals.append(res["value"])
     v = float(np.median(vals)) if vals else None
-    names = {"eval": EvalWork.metric, "track": "paths/s", "qr": "instances/s"}
-    unit = res.get("unit") if res else None
-    return {"impl": "reference", "metric": names.get(args.workload), "value": v, "unit": unit,
+    if args.workload == "track":
+        from . import trackwork
+        metric, unit, config = trackwork.TrackWork.metric, "paths/s", trackwork.static_config()
+    elif args.workload == "qr":
+        from . import qrwork
+        metric, unit, config = qrwork.QRWork.metric, qrwork.QRWork.unit, qrwork.static_config()
+    else:
+        metric, unit, config = EvalWork.metric, EvalWork.unit, {"workload": EVAL_WORKLOAD}
+    return {"impl": "reference", "metric": metric, "value": v, "unit": unit,
             "n_gpus": 0, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
             "cpu_baseline": dict(res or {}, value=v),
             "e2e": {"value": v, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "config": {"workload": args.workload}}
+            "config": config}

@@ -67,6 +67,18 @@ def track_flops(pb: hm.TrackProblem, steps, rejected, pmode=1):
     return total
 
 
+def static_config(npaths=1024, learned=None, note=None):
+    """The benchmark configuration, shared by the GPU and the reference arm."""
+    if learned is None:
+        learned = os.path.exists(MODEL_PATH)
+    if note is None:
+        note = hm.config4().note
+    return {"workload": "path tracking: dense quadratic n=10, 1024 total-degree paths, degree-8 series, "
+                        "[4/4] Pade, 3 dd corrector steps, dd endpoint refinement",
+            "paths": npaths, "dim": 10, "predictor": "fp64", "corrector": "double-double",
+            "step": "learned (MLP) with plain fallback" if learned else "plain pole step", "system": note}
+
+
 class TrackWork:
     metric = ("paths/s at endpoint residual <= 1e-24 (double-double), batched + precision-split"
               " + learned-step tracker, 1024-path dense quadratic homotopy")
@@ -88,11 +100,7 @@ class TrackWork:
             self.dt.set_model(self.model)
         self.units_per_step = pb.npaths
         self.l2_note = "working set (systems, paths, endpoints) < L2; the step is latency bound, not memory bound"
-        self.config = {"workload": "path tracking: dense quadratic n=10, 1024 total-degree paths, degree-8 series, "
-                                   "[4/4] Pade, 3 dd corrector steps, dd endpoint refinement",
-                       "paths": pb.npaths, "dim": pb.maxdim, "predictor": "fp64", "corrector": "double-double",
-                       "step": "learned (MLP) with plain fallback" if self.step_mode else "plain pole step",
-                       "system": pb.note}
+        self.config = static_config(pb.npaths, learned=bool(self.step_mode), note=pb.note)
         self.flops_note = None
         self.dominant_flops_per_launch = 0.0
         self.dominant_bytes_per_launch = float(pb.npaths * pb.maxdim * (16 + 64))
