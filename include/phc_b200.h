@@ -101,6 +101,23 @@ int phc_bals_solve(int prec, int cplx, int ninst, int dim, int degp1, int szt, i
 int phc_bals_solve_host(int prec, int cplx, int ninst, int dim, int degp1, int szt, int tailidx, const double *mat,
                         double *rhs, double *sol, double *Q, double *R, int *flags, void *stream);
 
+/* The same QR and least-squares solve with a choice of how the four WY
+ * trailing products of each tile (R += Y (W^T C), Q += (Q W^T) Y) run:
+ * wy = 0 on the CUDA cores in multiple-double arithmetic (as above), wy = 1
+ * as Ozaki-split products on the FP64 tensor cores (mma.sync m8n8k4 f64):
+ * each operand cut into 21-bit slices on per-row / per-column exponent
+ * grids so that every slice product and every inner sum is exact, the sums
+ * of equal order added into the multiple-double result.  wy = 1 applies to
+ * real numbers with dim <= 64 (complex numbers keep the CUDA-core products).
+ * The products of Matrices/dbl2_baqr_kernels.cu:2872-3444 (dbl2_small_WYT,
+ * _QWYT, _Qupdate, _YWTC, _R_add_YWTC) in the reference run one thread per
+ * entry on CUDA cores.  Workspace: ninst * phc_dense_workspace_bytes_wy(...). */
+long long phc_dense_workspace_bytes_wy(int prec, int cplx, int n, int szt, int wy);
+int phc_blocked_houseqr_wy(int prec, int cplx, int ninst, int nrows, int ncols, int szt, const double *A, double *Q,
+                           double *R, double *work, int wy, void *stream);
+int phc_bals_solve_wy(int prec, int cplx, int ninst, int dim, int degp1, int szt, int tailidx, const double *mat,
+                      double *rhs, double *sol, double *Q, double *R, int *flags, double *work, int wy, void *stream);
+
 /* phc_bals_solve without any allocation.  No counterpart in the reference:
  * this entry point is for callers that cannot let a library call cudaMalloc
  * or cudaFree (work recorded into a CUDA graph under stream capture,

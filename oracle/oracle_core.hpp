@@ -138,7 +138,7 @@ static void house(int n, const T *x, T *v, typename real_of<T>::type *beta) {
     *beta = R(0.0);
     return;
   }
-  T v0;
+  T v0 = T();
   if constexpr (is_cx<T>::v) {
     R sq0 = norm2(x[0]);
     R rad0 = sqrt(sq0);
@@ -174,7 +174,7 @@ static void left_update(int nrows, int ncols, int k, T *Rm, int ldr, const T *v,
                         const typename real_of<T>::type &beta) {
   std::vector<T> w(ncols - k);
   for (int j = k; j < ncols; ++j) {
-    T acc;
+    T acc = T();
     for (int i = k; i < nrows; ++i) acc = acc + conj(Rm[(long)i * ldr + j]) * v[i - k];
     w[j - k] = T(acc) * T(beta);
   }
@@ -220,12 +220,12 @@ static void blocked_houseqr(int nrows, int ncols, int szt, int nbt, const T *A, 
     std::vector<T> p(szt);
     for (int j = 1; j < szt; ++j) {
       for (int kk = 0; kk < j; ++kk) {
-        T acc;
+        T acc = T();
         for (int i = 0; i < rowdim; ++i) acc = acc + conj(Y[kk][i]) * Y[j][i];
         p[kk] = acc;
       }
       for (int i = 0; i < rowdim; ++i) {
-        T z;
+        T z = T();
         for (int kk = 0; kk < j; ++kk) z = z + W[kk][i] * p[kk];
         z = z + Y[j][i];
         W[j][i] = -(T(B[j]) * z);
@@ -237,13 +237,13 @@ static void blocked_houseqr(int nrows, int ncols, int szt, int nbt, const T *A, 
       std::vector<T> YWH((long)rowdim * rowdim), prd((long)rowdim * coldim);
       for (int i = 0; i < rowdim; ++i)
         for (int j = 0; j < rowdim; ++j) {
-          T acc;
+          T acc = T();
           for (int kk = 0; kk < szt; ++kk) acc = acc + Y[kk][i] * conj(W[kk][j]);
           YWH[(long)i * rowdim + j] = acc;
         }
       for (int i = 0; i < rowdim; ++i)
         for (int j = 0; j < coldim; ++j) {
-          T acc;
+          T acc = T();
           for (int kk = 0; kk < rowdim; ++kk) acc = acc + YWH[(long)i * rowdim + kk] * Rm[(long)(rowoff + kk) * ncols + coloff + j];
           prd[(long)i * coldim + j] = acc;
         }
@@ -255,13 +255,13 @@ static void blocked_houseqr(int nrows, int ncols, int szt, int nbt, const T *A, 
       std::vector<T> WYH((long)rowdim * rowdim), prd((long)nrows * rowdim);
       for (int i = 0; i < rowdim; ++i)
         for (int j = 0; j < rowdim; ++j) {
-          T acc;
+          T acc = T();
           for (int kk = 0; kk < szt; ++kk) acc = acc + W[kk][i] * conj(Y[kk][j]);
           WYH[(long)i * rowdim + j] = acc;
         }
       for (int i = 0; i < nrows; ++i)
         for (int j = 0; j < rowdim; ++j) {
-          T acc;
+          T acc = T();
           for (int kk = 0; kk < rowdim; ++kk) acc = acc + Q[(long)i * nrows + rowoff + kk] * WYH[(long)kk * rowdim + j];
           prd[(long)i * rowdim + j] = acc;
         }
@@ -291,7 +291,7 @@ static void houseqr(int nrows, int ncols, const T *A, T *Q, T *Rm) {
     left_update(nrows, ncols, k, Rm, ncols, v.data(), beta);
     // Q <- Q (I - beta v v^H), dbl2_factorizations.cpp:629/:662
     for (int i = 0; i < nrows; ++i) {
-      T acc;
+      T acc = T();
       for (int j = k; j < nrows; ++j) acc = acc + Q[(long)i * nrows + j] * v[j - k];
       w[i] = acc * T(beta);
     }
@@ -331,7 +331,7 @@ template <class T> static void upper_tiled_solver(int dim, int szt, int nbt, T *
   int idx = (nbt - 1) * szt;
   invert_tile(idx);
   for (int i = 0; i < szt; ++i) {
-    T acc;
+    T acc = T();
     for (int j = 0; j < szt; ++j) acc = acc + inv[(long)i * szt + j] * b[idx + j];
     x[idx + i] = acc;
   }
@@ -341,13 +341,13 @@ template <class T> static void upper_tiled_solver(int dim, int szt, int nbt, T *
     for (int L = 0; L < k; ++L) {
       const int r = L * szt;
       for (int i = 0; i < szt; ++i) {
-        T acc;
+        T acc = T();
         for (int j = 0; j < szt; ++j) acc = acc + U[(long)(r + i) * dim + idx + szt + j] * x[idx + szt + j];
         b[r + i] = b[r + i] - acc;
       }
     }
     for (int i = 0; i < szt; ++i) {
-      T acc;
+      T acc = T();
       for (int j = 0; j < szt; ++j) acc = acc + inv[(long)i * szt + j] * b[idx + j];
       wb[i] = acc;
     }
@@ -369,7 +369,7 @@ template <class T> static double maxnorm(int dim, const T *v) {
 // x = R^{-1} Q^H b, Matrices/dbl2_factorizations.cpp:823 (factors_qrbs)
 template <class T> static void qrbs(int n, const T *Q, const T *Rm, const T *b, T *x, T *w) {
   for (int i = 0; i < n; ++i) {
-    T acc;
+    T acc = T();
     for (int j = 0; j < n; ++j) acc = acc + conj(Q[(long)j * n + i]) * b[j];
     w[i] = acc;
   }

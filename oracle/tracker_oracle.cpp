@@ -264,7 +264,7 @@ static bool pade(int L, int M, const std::vector<T> &c, std::vector<T> &p, std::
     return false;
   }
   for (int i = 0; i <= L; ++i) {
-    T acc;
+    T acc = T();
     for (int j = 0; j <= std::min(i, M); ++j) acc = acc + q[j] * c[i - j];
     p[i] = acc;
   }

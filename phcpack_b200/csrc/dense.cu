@@ -8,7 +8,13 @@ namespace phc {
 
 static const int kDenseThreads = 256;
 
-template <class N>
+// per-instance workspace (doubles); the split tensor-core products need
+// ozaki_work_doubles more
+__host__ __device__ inline long dense_stride(int n, int szt, int W, bool oz) {
+  return dense_work_numbers(n, szt) * W + (oz ? ozaki_work_doubles(n, ozaki_slices<md::qd>::s) : 0);
+}
+
+template <class N, bool OZ>
 __global__ void __launch_bounds__(kDenseThreads)
     k_blocked_houseqr(int n, int ncols, int szt, const double *__restrict__ A, double *__restrict__ Q,
                       double *__restrict__ Rm, double *__restrict__ work) {
@@ -21,7 +27,7 @@ __global__ void __launch_bounds__(kDenseThreads)
   double *r = Rm + inst * n * ncols * W;
   for (long t = threadIdx.x; t < (long)n * ncols * W; t += blockDim.x) r[t] = a[t];
   __syncthreads();
-  block_houseqr<N>(n, ncols, szt, q, r, work + inst * dense_work_numbers(n, szt) * W, S);
+  block_houseqr<N, OZ>(n, ncols, szt, q, r, work + inst * dense_stride(n, szt, W, OZ), S);
 }
 
 // Like Matrices/dbl2_tabs_kernels.cu:952 (GPU_dbl2_upper_tiled_solver): b is
@@ -54,7 +60,7 @@ __global__ void __launch_bounds__(kDenseThreads)
 // right hand side below 1e-28; 1e-15 and 1e-56 in double and quad-double).
 // flags per instance: zeroQ, noqr, upidx, bsidx, newtail; with tailidx < 0
 // the tail starts at the instance's flags[4].
-template <class N>
+template <class N, bool OZ>
 __global__ void __launch_bounds__(kDenseThreads)
     k_bals_solve(int n, int degp1, int szt, int tailidx, const double *__restrict__ mat, double *__restrict__ rhs,
                  double *__restrict__ sol, double *__restrict__ Q, double *__restrict__ Rm, int *__restrict__ flags,
@@ -71,7 +77,7 @@ __global__ void __launch_bounds__(kDenseThreads)
   double *q = Q + inst * nn * W;
   double *r = Rm + inst * nn * W;
   int *fl = flags + inst * 5;
-  double *wk = work + inst * dense_work_numbers(n, szt) * W;
+  double *wk = work + inst * dense_stride(n, szt, W, OZ);
   double *tinv = wk + 4L * n * szt * W;
   int zeroQ = fl[0], noqr = fl[1];
   const int tail0 = max(1, tailidx >= 0 ? tailidx : fl[4]);
@@ -86,7 +92,7 @@ __global__ void __launch_bounds__(kDenseThreads)
     if (!noqr) {
       for (long t = threadIdx.x; t < nn * W; t += blockDim.x) r[t] = A[t];
       __syncthreads();
-      block_houseqr<N>(n, n, szt, q, r, wk, S);
+      block_houseqr<N, OZ>(n, n, szt, q, r, wk, S);
       zeroQ = 0;
       block_invert_tiles<N>(n, szt, r, n, tinv);
       tinv_ok = true;
@@ -143,10 +149,11 @@ __global__ void __launch_bounds__(kDenseThreads)
 
 template <class N>
 static int qr_launch(int ninst, int n, int ncols, int szt, const double *A, double *Q, double *R, double *work,
-                     cudaStream_t st) {
+                     cudaStream_t st, bool oz) {
   const long smem = dense_smem_doubles(n, szt, N::width) * sizeof(double);
-  PHC_CUDA(cudaFuncSetAttribute(k_blocked_houseqr<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k_blocked_houseqr<N><<<ninst, kDenseThreads, smem, st>>>(n, ncols, szt, A, Q, R, work);
+  auto kern = oz ? k_blocked_houseqr<N, true> : k_blocked_houseqr<N, false>;
+  PHC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  kern<<<ninst, kDenseThreads, smem, st>>>(n, ncols, szt, A, Q, R, work);
   PHC_CHECK_LAUNCH();
   return PHC_OK;
 }
@@ -160,10 +167,11 @@ static int tabs_launch(int ninst, int dim, int szt, double *U, double *b, double
 
 template <class N>
 static int bals_launch(int ninst, int n, int degp1, int szt, int tailidx, const double *mat, double *rhs, double *sol,
-                       double *Q, double *R, int *flags, double *work, cudaStream_t st) {
+                       double *Q, double *R, int *flags, double *work, cudaStream_t st, bool oz) {
   const long smem = dense_smem_doubles(n, szt, N::width) * sizeof(double);
-  PHC_CUDA(cudaFuncSetAttribute(k_bals_solve<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k_bals_solve<N><<<ninst, kDenseThreads, smem, st>>>(n, degp1, szt, tailidx, mat, rhs, sol, Q, R, flags, work);
+  auto kern = oz ? k_bals_solve<N, true> : k_bals_solve<N, false>;
+  PHC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  kern<<<ninst, kDenseThreads, smem, st>>>(n, degp1, szt, tailidx, mat, rhs, sol, Q, R, flags, work);
   PHC_CHECK_LAUNCH();
   return PHC_OK;
 }
@@ -190,7 +198,20 @@ int blocked_houseqr(int prec, int cplx, int ninst, int n, int ncols, int szt, co
   PHC_REQUIRE(prec_ok(prec), "blocked_houseqr: precision %d", prec);
   PHC_REQUIRE(n >= 1 && szt >= 1 && ncols % szt == 0 && ncols <= n && ncols >= 1, "blocked_houseqr: need ncols = szt*nbt <= n");
   if (ninst == 0) return PHC_OK;
-  PHC_DISPATCH(prec, cplx, qr_launch<N>(ninst, n, ncols, szt, A, Q, R, work, st));
+  PHC_DISPATCH(prec, cplx, qr_launch<N>(ninst, n, ncols, szt, A, Q, R, work, st, false));
+}
+
+long dense_work_doubles_wy(int prec, int cplx, int n, int szt, int wy) {
+  return dense_stride(n, szt, width_of(prec, cplx), wy != 0 && !cplx);
+}
+
+int blocked_houseqr_wy(int prec, int cplx, int ninst, int n, int ncols, int szt, const double *A, double *Q,
+                       double *R, double *work, int wy, cudaStream_t st) {
+  PHC_REQUIRE(prec_ok(prec), "blocked_houseqr: precision %d", prec);
+  PHC_REQUIRE(n >= 1 && n <= 64 && szt >= 1 && ncols % szt == 0 && ncols <= n && ncols >= 1,
+              "blocked_houseqr: need ncols = szt*nbt <= n <= 64 with the tensor-core products");
+  if (ninst == 0) return PHC_OK;
+  PHC_DISPATCH(prec, cplx, qr_launch<N>(ninst, n, ncols, szt, A, Q, R, work, st, wy != 0 && !cplx));
 }
 
 int upper_tiled_solver(int prec, int cplx, int ninst, int dim, int szt, double *U, double *b, double *x, double *work,
@@ -207,7 +228,18 @@ int bals_solve(int prec, int cplx, int ninst, int n, int degp1, int szt, int tai
   PHC_REQUIRE(n >= 1 && szt >= 1 && n % szt == 0 && degp1 >= 1, "bals_solve: need n = szt*nbt, degp1 >= 1");
   PHC_REQUIRE(tailidx != 0 && tailidx <= degp1, "bals_solve: tailidx %d not in [1, degp1=%d] (or < 0: per instance)", tailidx, degp1);
   if (ninst == 0) return PHC_OK;
-  PHC_DISPATCH(prec, cplx, bals_launch<N>(ninst, n, degp1, szt, tailidx, mat, rhs, sol, Q, R, flags, work, st));
+  PHC_DISPATCH(prec, cplx, bals_launch<N>(ninst, n, degp1, szt, tailidx, mat, rhs, sol, Q, R, flags, work, st, false));
+}
+
+int bals_solve_wy(int prec, int cplx, int ninst, int n, int degp1, int szt, int tailidx, const double *mat,
+                  double *rhs, double *sol, double *Q, double *R, int *flags, double *work, int wy, cudaStream_t st) {
+  PHC_REQUIRE(prec_ok(prec), "bals_solve: precision %d", prec);
+  PHC_REQUIRE(n >= 1 && n <= 64 && szt >= 1 && n % szt == 0 && degp1 >= 1,
+              "bals_solve: need n = szt*nbt <= 64 with the tensor-core products, degp1 >= 1");
+  PHC_REQUIRE(tailidx != 0 && tailidx <= degp1, "bals_solve: tailidx %d not in [1, degp1=%d] (or < 0: per instance)", tailidx, degp1);
+  if (ninst == 0) return PHC_OK;
+  PHC_DISPATCH(prec, cplx,
+               bals_launch<N>(ninst, n, degp1, szt, tailidx, mat, rhs, sol, Q, R, flags, work, st, wy != 0 && !cplx));
 }
 
 }  // namespace phc

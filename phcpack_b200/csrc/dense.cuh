@@ -11,6 +11,7 @@
 // across warps.
 #pragma once
 #include "md.cuh"
+#include "ozaki.cuh"
 
 namespace phc {
 
@@ -230,8 +231,11 @@ __device__ void block_apply_reflector(int n, int ncols, int c, int e, double *Rm
 // the szt reflectors are applied to the panel column by column, then
 // W = -B (I + W Y^H) Y column by column (:13), the trailing columns get
 // R <- R + Y (W^H R) and Q <- Q + (Q W) Y^H.  R must hold A on entry.
-// work: dense_work_numbers(n, szt) numbers of this instance.
-template <class N>
+// work: dense_work_numbers(n, szt) numbers of this instance; with OZ (real
+// numbers only) the four trailing products run as Ozaki-split products on
+// the FP64 tensor cores (ozaki.cuh) in ozaki_work_doubles more doubles
+// after that; complex numbers keep the CUDA-core products.
+template <class N, bool OZ = false>
 __device__ void block_houseqr(int n, int ncols, int szt, double *Q, double *Rm, double *work, dense_smem &S) {
   typedef typename N::T T;
   typedef typename N::real R;
@@ -285,6 +289,33 @@ __device__ void block_houseqr(int n, int ncols, int szt, double *Q, double *Rm, 
         }
         __syncthreads();
       }
+    }
+    if constexpr (OZ && !N::is_complex) {
+      double *oz = work + dense_work_numbers(n, szt) * W;
+      if (k < nbt - 1) {
+        const int nc = ncols - endcol;
+        // P = W^T C, then C += Y^T P
+        ozaki_gemm<R>(szt, nc, m, [&](int a, int b) { return ldn_at<N>(Wm, (long)a * m + b); },
+                      [&](int a, int b) { return ldn_at<N>(Rm, (long)(rowoff + a) * ncols + endcol + b); },
+                      [&](int a, int b, const R &v) { stn_at<N>(P, (long)a * nc + b, v); }, oz);
+        ozaki_gemm<R>(m, nc, szt, [&](int a, int b) { return ldn_at<N>(Y, (long)b * m + a); },
+                      [&](int a, int b) { return ldn_at<N>(P, (long)a * nc + b); },
+                      [&](int a, int b, const R &v) {
+                        const long o = (long)(rowoff + a) * ncols + endcol + b;
+                        stn_at<N>(Rm, o, N::add(ldn_at<N>(Rm, o), v));
+                      }, oz);
+      }
+      // T = Q[:, rowoff..] W^T, then Q[:, rowoff..] += T Y
+      ozaki_gemm<R>(n, szt, m, [&](int a, int b) { return ldn_at<N>(Q, (long)a * n + rowoff + b); },
+                    [&](int a, int b) { return ldn_at<N>(Wm, (long)b * m + a); },
+                    [&](int a, int b, const R &v) { stn_at<N>(Tm, (long)a * szt + b, v); }, oz);
+      ozaki_gemm<R>(n, m, szt, [&](int a, int b) { return ldn_at<N>(Tm, (long)a * szt + b); },
+                    [&](int a, int b) { return ldn_at<N>(Y, (long)a * m + b); },
+                    [&](int a, int b, const R &v) {
+                      const long o = (long)a * n + rowoff + b;
+                      stn_at<N>(Q, o, N::add(ldn_at<N>(Q, o), v));
+                    }, oz);
+      continue;
     }
     if (k < nbt - 1) {
       // R[rowoff.., endcol..] += Y (W^H C)

@@ -91,3 +91,47 @@ class DeviceBals:
         _lib.call("phc_bals_solve", self.prec, int(self.cplx), self.ninst, self.dim, self.degp1, self.szt, tailidx,
                   _lib.ptr(self.mat), _lib.ptr(self.rhs), _lib.ptr(self.sol), _lib.ptr(self.Q), _lib.ptr(self.R),
                   _lib.ptr(self.flags), _lib.ptr(self.work), _lib.c_void_p(s))
+
+
+def workspace_bytes_wy(prec, cplx, n, szt, wy):
+    f = _lib.lib().phc_dense_workspace_bytes_wy
+    f.restype = _lib.ctypes.c_longlong
+    return int(f(prec, int(cplx), n, szt, int(wy)))
+
+
+def _dev(a):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a)).to("cuda")
+
+
+def blocked_houseqr_wy(prec, cplx, A, ninst, nrows, ncols, szt, wy=1):
+    """Blocked QR with the WY trailing products on the FP64 tensor cores
+    (wy=1, Ozaki splitting) or on the CUDA cores (wy=0); device buffers
+    through torch, host arrays in and out."""
+    import torch
+    W = width(prec, cplx)
+    dA = _dev(np.asarray(A, np.float64))
+    dQ = torch.zeros(ninst * nrows * nrows * W, dtype=torch.float64, device="cuda")
+    dR = torch.zeros(ninst * nrows * ncols * W, dtype=torch.float64, device="cuda")
+    work = torch.zeros(ninst * workspace_bytes_wy(prec, cplx, nrows, szt, wy) // 8, dtype=torch.float64,
+                       device="cuda")
+    _lib.call("phc_blocked_houseqr_wy", prec, int(cplx), ninst, nrows, ncols, szt, _lib.ptr(dA), _lib.ptr(dQ),
+              _lib.ptr(dR), _lib.ptr(work), int(wy), _lib.c_void_p(0))
+    torch.cuda.synchronize()
+    return dQ.cpu().numpy(), dR.cpu().numpy()
+
+
+def bals_solve_wy(prec, cplx, mat, rhs, ninst, dim, degp1, szt, wy=1, tailidx=1):
+    import torch
+    W = width(prec, cplx)
+    dm, db = _dev(np.asarray(mat, np.float64)), _dev(np.asarray(rhs, np.float64))
+    f64 = dict(dtype=torch.float64, device="cuda")
+    dx = torch.zeros(ninst * degp1 * dim * W, **f64)
+    dQ = torch.zeros(ninst * dim * dim * W, **f64)
+    dR = torch.zeros(ninst * dim * dim * W, **f64)
+    fl = _dev(np.tile(np.array([1, 0, 0, 0, tailidx], np.int32), ninst))
+    work = torch.zeros(ninst * workspace_bytes_wy(prec, cplx, dim, szt, wy) // 8, **f64)
+    _lib.call("phc_bals_solve_wy", prec, int(cplx), ninst, dim, degp1, szt, tailidx, _lib.ptr(dm), _lib.ptr(db),
+              _lib.ptr(dx), _lib.ptr(dQ), _lib.ptr(dR), _lib.ptr(fl), _lib.ptr(work), int(wy), _lib.c_void_p(0))
+    torch.cuda.synchronize()
+    return dx.cpu().numpy(), fl.cpu().numpy()
