@@ -173,7 +173,12 @@ int phc_newton_host(int prec, int cplx, int nsys, int dim, int deg, int szt, int
  *   term_mono[r] (global id), a = term_a[2r] + i term_a[2r+1], b likewise.
  * Jacobian gather lists (from phc_track_prepare): for (equation e, variable
  *   j) the entries jg_off[e*maxdim+j] .. jg_off[e*maxdim+j+1]-1 of jg_term,
- *   jg_slot.
+ *   jg_slot.  A slot >= 0 is the variable's place in the term's monomial
+ *   (the partial is staged in shared memory); for monomials of total degree
+ *   <= 2 the partial is read in place: -1 the constant 1, -2 the series
+ *   2 x_j, -3-l the series x_l.  phc_track_prepare returns the number of
+ *   staged entries; pass it as gstaged to phc_track and phc_track_smem_bytes
+ *   (0 drops the staging buffer from shared memory).
  * Paths: path p belongs to system path_sys[p] and starts at x0 (maxdim complex
  *   doubles per path).
  * ipar: deg (series degree K), numdeg (L), dendeg (M), nit (series Newton
@@ -196,16 +201,17 @@ int phc_newton_host(int prec, int cplx, int nsys, int dim, int deg, int szt, int
 long long phc_track_gather_count(int nsys, const int *mono_off, const int *mono_nvr, const int *eq_off,
                                  const int *term_off, const int *term_mono);
 int phc_track_prepare(int nsys, const int *dim, int maxvar, const int *mono_off, const int *mono_nvr,
-                      const int *mono_idx, const int *eq_off, const int *term_off, const int *term_mono, int maxdim,
-                      int *jg_off, int *jg_term, int *jg_slot);
-long long phc_track_smem_bytes(int maxdim, int deg, int dendeg, int nmono_max, int maxvar, int pmode, int rmode);
+                      const int *mono_idx, const int *mono_exp, const int *eq_off, const int *term_off,
+                      const int *term_mono, int maxdim, int *jg_off, int *jg_term, int *jg_slot);
+long long phc_track_smem_bytes(int maxdim, int deg, int dendeg, int nmono_max, int maxvar, int pmode, int rmode,
+                               int gstaged);
 int phc_track(int nsys, const int *dim, int maxvar, int maxdim, int nmono_max, const int *mono_off,
               const int *mono_nvr, const int *mono_idx, const int *mono_exp, const int *eq_off, const int *term_off,
               const int *term_mono, const double *term_a, const double *term_b, const int *jg_off,
-              const int *jg_term, const int *jg_slot, int npaths, const int *path_sys, const double *x0,
-              const int *ipar, const double *dpar, int pmode, int rmode, int step_mode, const void *model,
-              double *xend, int *info, double *dinfo, float *log, int log_cap, int *log_count, int *queue,
-              int one_per_launch, void *stream);
+              const int *jg_term, const int *jg_slot, int gstaged, int npaths, const int *path_sys,
+              const double *x0, const int *ipar, const double *dpar, int pmode, int rmode, int step_mode,
+              const void *model, double *xend, int *info, double *dinfo, float *log, int log_cap, int *log_count,
+              int *queue, int one_per_launch, void *stream);
 /* Host arrays in and out; returns the number of paths not classified as
  * success (>= 0) or an error (< 0). */
 int phc_track_host(int nsys, const int *dim, int maxvar, const int *mono_off, const int *mono_nvr,

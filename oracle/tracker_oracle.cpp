@@ -16,15 +16,17 @@
 // restated and what is left out:
 //  * predictor: Newton on power series in s = t - t0 to degree K (working
 //    degree doubling 1, 3, 7, ... K), each step a block-Toeplitz solve with
-//    the QR of J_0 (factored once per step and reused, as the reference's
-//    noqr rule does); [L/M] Pade approximant per component; pole step
+//    the LU of J_0 (factored once per step and reused, as LU_Prediction
+//    does; applied as the explicit inverse); [L/M] Pade approximant per
+//    component; pole step
 //    pbeta * r with r the smallest Fabry radius |c_{K-3}/c_{K-2}| (offset 2
 //    as in Newton_Fabry); step = min(pole step, maxsize), cut at t = 1;
 //  * the Hessian curvature step (Hesse_Pade, singular values of Hessians)
 //    is left out: the predictor feedback and the corrector bound the step;
 //  * predictor feedback: halve the step until the mixed residual of the
 //    Pade prediction is below alpha (fail below minsize);
-//  * corrector: at most corsteps Newton steps at the new t, converged when
+//  * corrector: at most corsteps LU Newton steps at the new t (LU_Newton_Steps,
+//    Curves/corrector_convolutions.adb:1193-1224), converged when
 //    max |dx_i| <= tolres, followed by one extra step; on failure halve the
 //    step and re-evaluate the Pade approximant (fail below minsize);
 //  * stop when |1 - t| < epsilon; refine the endpoint at t = 1 and classify
@@ -164,18 +166,74 @@ static void hom_abs_eval(const TrackSys &S, int s, double t, const std::vector<d
 
 template <class R> static double cabs(const cx<R> &a) { return std::hypot(to_double(a.re), to_double(a.im)); }
 
-// Solve A x = b (n x n complex) by the Householder QR of this oracle
-template <class T> struct qr_solver {
-  int n;
-  std::vector<T> Q, Rm, w;
+// LU factorization with partial pivoting and its solves: lufac and lusolve
+// of Math_Lib/Reduction/standard_complex_linear_solvers.adb:123-178 and
+// :552-583 (LINPACK zgefa/zgesl).  The pivot of column k is the first row of
+// largest |re| + |im| (leading limbs); the multipliers -a_ik / a_kk are
+// stored below the diagonal.  Where lusolve divides by u_kk, the back
+// substitution here multiplies by dinv[k] = 1 / u_kk formed during the
+// factorization (NaN for a zero pivot), as the GPU tracker does.
+template <class T> struct lu_solver {
+  typedef typename real_of<T>::type R;
+  int n = 0, info = 0;
+  std::vector<T> a, dinv;
+  std::vector<int> ipvt;
   void factor(int n_, const std::vector<T> &A) {
     n = n_;
-    Q.assign((long)n * n, T());
-    Rm.assign((long)n * n, T());
-    w.assign(n, T());
-    houseqr(n, n, A.data(), Q.data(), Rm.data());
+    a.assign(A.begin(), A.begin() + (long)n * n);
+    dinv.assign(n, T());
+    ipvt.assign(n, 0);
+    info = 0;
+    for (int k = 0; k < n; ++k) {
+      int ell = k;
+      double smax = lead(a[(long)k * n + k]);
+      if (std::isnan(smax)) smax = INFINITY;
+      for (int i = k + 1; i < n; ++i) {
+        double v = lead(a[(long)i * n + k]);
+        if (std::isnan(v)) v = INFINITY;
+        if (v > smax) { smax = v; ell = i; }
+      }
+      ipvt[k] = ell;
+      if (smax == 0.0) {
+        if (info == 0) info = k + 1;
+        dinv[k] = T(R(NAN));
+        continue;
+      }
+      if (ell != k)
+        for (int j = k; j < n; ++j) std::swap(a[(long)ell * n + j], a[(long)k * n + j]);
+      const T inv = T(R(1.0)) / a[(long)k * n + k];
+      dinv[k] = inv;
+      const T temp = -inv;
+      for (int i = k + 1; i < n; ++i) a[(long)i * n + k] = temp * a[(long)i * n + k];
+      for (int i = k + 1; i < n; ++i)
+        for (int j = k + 1; j < n; ++j) a[(long)i * n + j] = a[(long)i * n + j] + a[(long)k * n + j] * a[(long)i * n + k];
+    }
   }
-  void solve(const T *b, T *x) { qrbs(n, Q.data(), Rm.data(), b, x, w.data()); }
+  // x = A^{-1} b (x may alias b)
+  void solve(const T *b, T *x) const {
+    if (x != b) for (int i = 0; i < n; ++i) x[i] = b[i];
+    for (int k = 0; k < n - 1; ++k) {
+      const int ell = ipvt[k];
+      const T t = x[ell];
+      if (ell != k) { x[ell] = x[k]; x[k] = t; }
+      for (int i = k + 1; i < n; ++i) x[i] = x[i] + t * a[(long)i * n + k];
+    }
+    for (int kb = n - 1; kb >= 0; --kb) {
+      x[kb] = x[kb] * dinv[kb];
+      const T t = x[kb];
+      for (int j = 0; j < kb; ++j) x[j] = x[j] - t * a[(long)j * n + kb];
+    }
+  }
+  // M = A^{-1}, row-major, column by column
+  void inverse(std::vector<T> &M) const {
+    M.assign((long)n * n, T());
+    std::vector<T> col(n);
+    for (int c = 0; c < n; ++c) {
+      for (int i = 0; i < n; ++i) col[i] = (i == c) ? T(R(1.0)) : T();
+      solve(col.data(), col.data());
+      for (int i = 0; i < n; ++i) M[(long)i * n + c] = col[i];
+    }
+  }
 };
 
 // Newton on power series (the predictor): x[i] series of degree K, on
@@ -185,8 +243,8 @@ static void series_newton(const TrackSys &S, int s, const TrackPar &P, double t0
   const int n = S.dim[s];
   const int K = P.deg;
   std::vector<std::vector<T> > h;
-  std::vector<T> jac, rhs(n), dx((long)(K + 1) * n), A((long)n * n);
-  qr_solver<T> qr;
+  std::vector<T> jac, rhs(n), dx((long)(K + 1) * n), M;
+  lu_solver<T> lu;
   for (int it = 0; it < P.nit; ++it) {
     int w = (2 << it) - 1;
     if (w > K) w = K;
@@ -194,9 +252,9 @@ static void series_newton(const TrackSys &S, int s, const TrackPar &P, double t0
     for (int i = 0; i < n; ++i)
       for (int k = 0; k <= w; ++k) xw[i][k] = x[i][k];
     hom_eval(S, s, w, t0, xw, h, &jac);
-    if (it == 0) {  // J_0 factored once per step, reused by later iterations
-      for (int l = 0; l < n * n; ++l) A[l] = jac[l];
-      qr.factor(n, A);
+    if (it == 0) {  // J_0 factored once per step (LU_Prediction), M = J_0^{-1}
+      lu.factor(n, jac);
+      lu.inverse(M);
     }
     for (int k = 0; k <= w; ++k) {
       for (int i = 0; i < n; ++i) {
@@ -205,7 +263,11 @@ static void series_newton(const TrackSys &S, int s, const TrackPar &P, double t0
           for (int l = 0; l < n; ++l) acc = acc - jac[((long)j * n + i) * n + l] * dx[(long)(k - j) * n + l];
         rhs[i] = acc;
       }
-      qr.solve(rhs.data(), dx.data() + (long)k * n);
+      for (int i = 0; i < n; ++i) {
+        T acc = T();
+        for (int j = 0; j < n; ++j) acc = acc + M[(long)i * n + j] * rhs[j];
+        dx[(long)k * n + i] = acc;
+      }
     }
     for (int i = 0; i < n; ++i)
       for (int k = 0; k <= w; ++k) x[i][k] = x[i][k] + dx[(long)k * n + i];
@@ -284,8 +346,8 @@ static bool point_newton(const TrackSys &S, int s, double t, std::vector<T> &x, 
                          double *lastdx) {
   const int n = S.dim[s];
   std::vector<std::vector<T> > xs(n, std::vector<T>(1)), h;
-  std::vector<T> jac, rhs(n), dx(n);
-  qr_solver<T> qr;
+  std::vector<T> jac, dx(n);
+  lu_solver<T> lu;
   bool conv = false;
   int extra_left = extra;
   *lastdx = 1e300;
@@ -293,9 +355,13 @@ static bool point_newton(const TrackSys &S, int s, double t, std::vector<T> &x, 
     if (it >= maxit && !conv) break;
     for (int i = 0; i < n; ++i) xs[i][0] = x[i];
     hom_eval(S, s, 0, t, xs, h, &jac);
-    qr.factor(n, jac);
-    for (int i = 0; i < n; ++i) rhs[i] = -h[i][0];
-    qr.solve(rhs.data(), dx.data());
+    lu.factor(n, jac);
+    for (int i = 0; i < n; ++i) dx[i] = -h[i][0];
+    lu.solve(dx.data(), dx.data());
+    if (lu.info != 0) {  // singular Jacobian: x unchanged, not converged
+      *lastdx = INFINITY;
+      return false;
+    }
     double m = 0.0;
     for (int i = 0; i < n; ++i) {
       x[i] = x[i] + dx[i];

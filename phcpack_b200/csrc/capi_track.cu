@@ -9,7 +9,7 @@ namespace phc {
 int track(const TrackDev &S, const TrackParDev &P, int nmono_max, int npaths, const int *path_sys, const double *x0,
           int pmode, int rmode, const void *model, double *xend, int *info, double *dinfo, float *log, int log_cap,
           int *log_count, int *queue, int one_per_launch, cudaStream_t st);
-long track_smem_bytes(int maxdim, int K, int M, int nmono_max, int maxvar, int pmode, int rmode);
+long track_smem_bytes(int maxdim, int K, int M, int nmono_max, int maxvar, int pmode, int rmode, int gst);
 }  // namespace phc
 
 using namespace phc;
@@ -47,8 +47,8 @@ long long phc_track_gather_count(int nsys, const int *mono_off, const int *mono_
 }
 
 int phc_track_prepare(int nsys, const int *dim, int maxvar, const int *mono_off, const int *mono_nvr,
-                      const int *mono_idx, const int *eq_off, const int *term_off, const int *term_mono, int maxdim,
-                      int *jg_off, int *jg_term, int *jg_slot) {
+                      const int *mono_idx, const int *mono_exp, const int *eq_off, const int *term_off,
+                      const int *term_mono, int maxdim, int *jg_off, int *jg_term, int *jg_slot) {
   PHC_REQUIRE(nsys >= 0 && maxvar >= 1 && maxdim >= 1, "track_prepare: bad sizes");
   const int neq = eq_off[nsys];
   std::vector<std::vector<std::pair<int, int> > > lists((size_t)neq * maxdim);
@@ -67,21 +67,29 @@ int phc_track_prepare(int nsys, const int *dim, int maxvar, const int *mono_off,
         }
       }
   }
-  int q = 0;
+  // slot codes: partials of monomials of total degree <= 2 are read in place
+  int q = 0, staged = 0;
   for (size_t g = 0; g < lists.size(); ++g) {
     jg_off[g] = q;
     for (auto &pr : lists[g]) {
+      const int m = term_mono[pr.first], v = pr.second;
+      const int *ix = mono_idx + (long)m * maxvar, *ex = mono_exp + (long)m * maxvar;
+      int code = v;
+      if (simple_monomial(mono_nvr[m], ex))
+        code = mono_nvr[m] == 1 ? (ex[0] == 1 ? -1 : -2) : -3 - ix[1 - v];
+      else
+        ++staged;
       jg_term[q] = pr.first;
-      jg_slot[q] = pr.second;
+      jg_slot[q] = code;
       ++q;
     }
   }
   jg_off[lists.size()] = q;
-  return PHC_OK;
+  return staged;
 }
 
-long long phc_track_smem_bytes(int maxdim, int deg, int dendeg, int nmono_max, int maxvar, int pmode, int rmode) {
-  return track_smem_bytes(maxdim, deg, dendeg, nmono_max, maxvar, pmode, rmode);
+long long phc_track_smem_bytes(int maxdim, int deg, int dendeg, int nmono_max, int maxvar, int pmode, int rmode, int gstaged) {
+  return track_smem_bytes(maxdim, deg, dendeg, nmono_max, maxvar, pmode, rmode, gstaged);
 }
 
 long long phc_mlp_model_bytes(void) { return mlp_model_bytes(); }
@@ -89,12 +97,12 @@ long long phc_mlp_model_bytes(void) { return mlp_model_bytes(); }
 int phc_track(int nsys, const int *dim, int maxvar, int maxdim, int nmono_max, const int *mono_off,
               const int *mono_nvr, const int *mono_idx, const int *mono_exp, const int *eq_off, const int *term_off,
               const int *term_mono, const double *term_a, const double *term_b, const int *jg_off,
-              const int *jg_term, const int *jg_slot, int npaths, const int *path_sys, const double *x0,
-              const int *ipar, const double *dpar, int pmode, int rmode, int step_mode, const void *model,
-              double *xend, int *info, double *dinfo, float *log, int log_cap, int *log_count, int *queue,
-              int one_per_launch, void *stream) {
-  TrackDev S{nsys, maxvar, maxdim, dim, mono_off, mono_nvr, mono_idx, mono_exp, eq_off, term_off, term_mono, term_a,
-             term_b, jg_off, jg_term, jg_slot};
+              const int *jg_term, const int *jg_slot, int gstaged, int npaths, const int *path_sys,
+              const double *x0, const int *ipar, const double *dpar, int pmode, int rmode, int step_mode,
+              const void *model, double *xend, int *info, double *dinfo, float *log, int log_cap, int *log_count,
+              int *queue, int one_per_launch, void *stream) {
+  TrackDev S{nsys,      maxvar, maxdim, dim,    mono_off, mono_nvr, mono_idx, mono_exp,    eq_off,
+             term_off,  term_mono, term_a, term_b, jg_off,  jg_term,  jg_slot,  gstaged != 0};
   return track(S, make_par(ipar, dpar, step_mode), nmono_max, npaths, path_sys, x0, pmode, rmode,
                step_mode ? model : nullptr, xend, info, dinfo, log, log_cap, log_count, queue, one_per_launch,
                (cudaStream_t)stream);
@@ -116,9 +124,9 @@ int phc_track_host(int nsys, const int *dim, int maxvar, const int *mono_off, co
   const int nmono = mono_off[nsys];
   const long long njg = phc_track_gather_count(nsys, mono_off, mono_nvr, eq_off, term_off, term_mono);
   std::vector<int> jg_off((size_t)neq * maxdim + 1), jg_term(njg > 0 ? njg : 1), jg_slot(njg > 0 ? njg : 1);
-  int rc = phc_track_prepare(nsys, dim, maxvar, mono_off, mono_nvr, mono_idx, eq_off, term_off, term_mono, maxdim,
-                             jg_off.data(), jg_term.data(), jg_slot.data());
-  if (rc) return rc;
+  const int staged = phc_track_prepare(nsys, dim, maxvar, mono_off, mono_nvr, mono_idx, mono_exp, eq_off, term_off,
+                                       term_mono, maxdim, jg_off.data(), jg_term.data(), jg_slot.data());
+  if (staged < 0) return staged;
   // one device buffer for everything
   std::vector<std::pair<const void *, size_t> > ins = {
       {dim, nsys * 4ul}, {mono_off, (nsys + 1) * 4ul}, {mono_nvr, nmono * 4ul},
@@ -158,7 +166,7 @@ int phc_track_host(int nsys, const int *dim, int maxvar, const int *mono_off, co
     auto I = [&](int i) { return (const int *)(b + off[i]); };
     auto Dp = [&](int i) { return (const double *)(b + off[i]); };
     out = phc_track(nsys, I(0), maxvar, maxdim, nmono_max, I(1), I(2), I(3), I(4), I(5), I(6), I(7), Dp(8), Dp(9),
-                    I(10), I(11), I(12), npaths, I(13), Dp(14), ipar, dpar, pmode, rmode, step_mode,
+                    I(10), I(11), I(12), staged, npaths, I(13), Dp(14), ipar, dpar, pmode, rmode, step_mode,
                     step_mode && model ? (const void *)(b + off[15]) : nullptr, (double *)(b + o_xend),
                     (int *)(b + o_info), (double *)(b + o_dinfo), nullptr, 0, nullptr, (int *)(b + o_q), 0, st);
   }

@@ -7,12 +7,12 @@
 // :37-85, restated):
 //   predictor, in PN precision (double or double-double):
 //     Newton on power series in s = t - t0 to degree K, working degree
-//     1, 3, 7, ..., K, each step a block-Toeplitz solve with the QR of J_0
-//     (factored and R^{-1} Q^H formed once per predictor step);
+//     1, 3, 7, ..., K, each step a block-Toeplitz solve with the LU of J_0
+//     (factored and J_0^{-1} formed once per predictor step);
 //     [L/M] Pade approximant per component; pole step pbeta * r, r the
 //     smallest Fabry radius |c_{K-3}/c_{K-2}|; step <= maxsize, cut at t = 1;
 //     predictor feedback: halve until the mixed residual < alpha;
-//   corrector, in double-double: at most corsteps Newton steps, converged
+//   corrector, in double-double: at most corsteps LU Newton steps, converged
 //     when max |dx| <= tolres, plus one extra step; on failure halve the step;
 //   the step size comes from a learned model when one is given (step_mode
 //     1): a proposal whose corrector fails is rejected and the step is
@@ -29,11 +29,10 @@ namespace phc {
 
 
 struct TrackLayout {
-  long xs, V, G, hs, J, dx, rhs, Q, R, Ri, M, num, den, xp, xc, dxc, hc, Jc, Qc, Rc, Ric, Vc, Gc, wv, dense, feat, mag,
-      degs, hbuf, total;
+  long xs, V, G, hs, J, dx, rhs, R, M, num, den, xp, xc, hc, Jc, Vc, Gc, red, piv, dinv, feat, mag, degs, hbuf, total;
 };
 
-__host__ __device__ inline TrackLayout track_layout(int n, int K, int M, int nm, int mv, int Wp, int Wr) {
+__host__ __device__ inline TrackLayout track_layout(int n, int K, int M, int nm, int mv, int Wp, int Wr, int gst) {
   TrackLayout L;
   long o = 0;
   auto take = [&](long doubles) {
@@ -49,7 +48,9 @@ __host__ __device__ inline TrackLayout track_layout(int n, int K, int M, int nm,
   L.den = take(n * (M + 1) * Wp);
   L.xp = take(n * Wp);
   const int Wm = Wp > Wr ? Wp : Wr;
-  L.dense = take(dense_smem_doubles(n, n, Wm));
+  L.red = take(32 * Wm);
+  L.piv = take(24);  // 32 pivot rows and the info word, as ints
+  L.dinv = take(n * Wm);
   L.feat = take(32);
   L.mag = take(n * K1);
   L.degs = take(n);
@@ -57,28 +58,21 @@ __host__ __device__ inline TrackLayout track_layout(int n, int K, int M, int nm,
   // scratch of the series Newton and the predictor feedback ...
   const long ov = o;
   L.V = take(nm * K1 * Wp);
-  L.G = take(nm * mv * K1 * Wp);
+  L.G = take(gst ? nm * mv * K1 * Wp : 0);  // only monomials of degree >= 3 stage partials
   L.hs = take(n * K1 * Wp);
   L.J = take(K1 * n * n * Wp);
   L.dx = take(K1 * n * Wp);
   L.rhs = take(n * Wp);
-  L.Q = take(n * n * Wp);
   L.R = take(n * n * Wp);
-  L.Ri = take(n * n * Wp);
   L.M = take(n * n * Wp);
   const long pend = o;
   // ... overlaid by the scratch of the corrector and the refinement, which
   // run after the Pade approximants are formed
   o = ov;
-  L.dxc = take(n * Wr);
   L.hc = take(n * Wr);
   L.Jc = take(n * n * Wr);
-  L.Qc = take(n * n * Wr);
-  L.Rc = take(n * n * Wr);
-  L.Ric = take(n * n * Wr);
   L.Vc = take(nm * Wr);
-  L.Gc = take(nm * mv * Wr);
-  L.wv = take(n * Wr);
+  L.Gc = take(gst ? nm * mv * Wr : 0);
   L.total = o > pend ? o : pend;
   return L;
 }
@@ -94,28 +88,38 @@ __device__ double cta_maxmag(int n, const double *v, double *red) {
 }
 
 // Newton at a point in precision N (the corrector and the refinement):
-// x (shared, n numbers) updated in place; returns converged.  lastdx: the
-// last max |dx|.
+// LU_Newton_Steps of Curves/corrector_convolutions.adb:1193-1224 restated:
+// each step factors J(x) by cta_lufac and solves J dx = -h(x) (a singular
+// Jacobian ends the steps unconverged, x unchanged), converged when
+// max |dx| <= tol, then extra more steps.  x (shared, n numbers) is updated
+// in place; lastdx: the last max |dx|.
 template <class N>
-__device__ bool point_newton(const TrackDev &S, int s, int n, double t, double *x, double *dx, double *h, double *Jm,
-                             double *Q, double *Rm, double *Ri, double *Vc, double *Gc, double *w, dense_smem &D,
-                             int maxit, double tol, int extra, double *lastdx) {
+__device__ bool point_newton(const TrackDev &S, int s, int n, double t, double *x, double *h, double *Jm, double *Vc,
+                             double *Gc, int *piv, double *dinv, double *red, int maxit, double tol, int extra,
+                             double *lastdx) {
   bool conv = false;
   int extra_left = extra;
   *lastdx = 1e300;
   for (int it = 0; it < maxit + extra; ++it) {
     if (it >= maxit && !conv) break;
     hom_eval_cta<N>(S, s, 0, t, x, 1, Vc, Gc, h, Jm);
-    small_qr<N>(n, Q, Jm, Ri, D);
-    for (int i = threadIdx.x; i < n; i += blockDim.x) stn_at<N>(h, i, N::neg(ldn_at<N>(h, i)));
+    const int info = cta_lufac<N>(n, Jm, piv, dinv, piv + 32);
+    if (threadIdx.x < 32) {
+      const typename N::T v = warp_lusolve<N>(n, Jm, piv, dinv, h, true);
+      double m = 0.0;
+      if ((threadIdx.x & 31) < n) {
+        m = N::mag(v);
+        if (!(m == m)) m = INFINITY;
+        if (info == 0) stn_at<N>(x, threadIdx.x, N::add(ldn_at<N>(x, threadIdx.x), v));
+      }
+      m = warp_max(m);
+      if (threadIdx.x == 0) red[0] = info ? INFINITY : m;
+    }
     __syncthreads();
-    cta_matvec_h<N>(n, Q, h, w);
-    cta_matvec<N>(n, Ri, w, dx);
-    for (int i = threadIdx.x; i < n; i += blockDim.x) stn_at<N>(x, i, N::add(ldn_at<N>(x, i), ldn_at<N>(dx, i)));
+    const double m = red[0];
     __syncthreads();
-    const double m = cta_maxmag<N>(n, dx, D.red);
     *lastdx = m;
-    if (!(m == m) || m > 1e300) return false;
+    if (!(m <= 1e300)) return false;
     if (conv) {
       if (--extra_left <= 0) break;
     } else if (m <= tol) {
@@ -129,9 +133,9 @@ __device__ bool point_newton(const TrackDev &S, int s, int n, double t, double *
 // max_i |h_i(x, t)| at a point, in precision N
 template <class N>
 __device__ double point_residual(const TrackDev &S, int s, int n, double t, const double *x, double *h, double *Vc,
-                                 double *Gc, dense_smem &D) {
+                                 double *Gc, double *red) {
   hom_eval_cta<N>(S, s, 0, t, x, 1, Vc, Gc, h, nullptr);
-  return cta_maxmag<N>(n, h, D.red);
+  return cta_maxmag<N>(n, h, red);
 }
 
 // Pade [L/M] of component i's series c (K+1 numbers), Gaussian elimination
@@ -203,7 +207,7 @@ __device__ typename N::T horner(const double *a, int deg, const typename N::T &z
 template <class PN>
 __device__ double pade_mixres(const TrackDev &S, int s, int n, int K, int dendeg, double t, double st,
                               const double *num, const double *den, const int *degs, double *xp, double *V,
-                              double *G, double *hs, dense_smem &D) {
+                              double *G, double *hs, double *red) {
   const int Wp = PN::width;
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
     const typename PN::T z = PN::from(st);
@@ -213,11 +217,13 @@ __device__ double pade_mixres(const TrackDev &S, int s, int n, int K, int dendeg
   }
   __syncthreads();
   hom_eval_cta<PN>(S, s, 0, t + st, xp, 1, V, G, hs, nullptr);
+  // one warp per equation, lanes over its terms
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   double part = 0.0;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+  for (int i = warp; i < n; i += nw) {
     double ab = 0.0;
     const int eq = S.eq_off[s] + i;
-    for (int tr = S.term_off[eq]; tr < S.term_off[eq + 1]; ++tr) {
+    for (int tr = S.term_off[eq] + lane; tr < S.term_off[eq + 1]; tr += 32) {
       const int gm = S.term_mono[tr];
       double v = hypot(fma(S.term_b[2 * tr], t + st, S.term_a[2 * tr]),
                        fma(S.term_b[2 * tr + 1], t + st, S.term_a[2 * tr + 1]));
@@ -227,9 +233,10 @@ __device__ double pade_mixres(const TrackDev &S, int s, int n, int K, int dendeg
       }
       ab += v;
     }
-    part += PN::mag(ldn_at<PN>(hs, i)) / (ab + 1.0);
+    for (int o = 16; o > 0; o >>= 1) ab += __shfl_xor_sync(0xffffffffu, ab, o);
+    if (lane == 0) part += PN::mag(ldn_at<PN>(hs, i)) / (ab + 1.0);
   }
-  return block_sum<md::num<double, false> >(part, D.red) / n;
+  return block_sum<md::num<double, false> >(part, red) / n;
 }
 
 // Track the paths of one CTA.  PN: predictor numbers, CN: corrector
@@ -248,8 +255,10 @@ __global__ void __launch_bounds__(kTrackThreads)
   const int n_max = S.maxdim;
   int nm_max = 0;
   for (int s = 0; s < S.nsys; ++s) nm_max = max(nm_max, S.mono_off[s + 1] - S.mono_off[s]);
-  const TrackLayout L = track_layout(n_max, K, P.dendeg, nm_max, S.maxvar, Wp, Wr);
-  dense_smem D = carve<RN>(sm + L.dense, n_max, n_max);
+  const TrackLayout L = track_layout(n_max, K, P.dendeg, nm_max, S.maxvar, Wp, Wr, S.gstaged);
+  double *red = sm + L.red;
+  int *piv = reinterpret_cast<int *>(sm + L.piv);
+  double *dinv = sm + L.dinv;
   int next_static = blockIdx.x;
   for (;;) {
     if (queue) {
@@ -274,8 +283,8 @@ __global__ void __launch_bounds__(kTrackThreads)
     }
     __syncthreads();
     double t = 0.0, dxn;
-    point_newton<CN>(S, s, n, 0.0, xc, sm + L.dxc, sm + L.hc, sm + L.Jc, sm + L.Qc, sm + L.Rc, sm + L.Ric, sm + L.Vc,
-                     sm + L.Gc, sm + L.wv, D, P.corsteps, P.tolres, 1, &dxn);
+    point_newton<CN>(S, s, n, 0.0, xc, sm + L.hc, sm + L.Jc, sm + L.Vc, sm + L.Gc, piv, dinv, red, P.corsteps,
+                     P.tolres, 1, &dxn);
     int status = 2, nsteps = 0, nrej = 0;
     bool failed = false;
     for (int step_it = 0; step_it < P.maxsteps; ++step_it) {
@@ -293,24 +302,15 @@ __global__ void __launch_bounds__(kTrackThreads)
         if (w > K) w = K;
         hom_eval_cta<PN>(S, s, w, t, xs, K + 1, sm + L.V, sm + L.G, sm + L.hs, sm + L.J);
         if (it == 0) {
-          // QR of J_0 once per step: the corrected point changes the
-          // constant term only at roundoff level in later iterations (the
-          // reuse the reference makes with its noqr rule,
-          // Newton/dbl2_bals_host.cpp:43-60).  small_qr overwrites its
-          // argument with R, so J_0 is copied first.
+          // J_0 factored once per step (LU_Prediction,
+          // Curves/standard_predictor_convolutions.adb:1142-1185, factors
+          // J_0 once by lufac and reuses it for every coefficient): the LU
+          // of a copy of J_0, then M = J_0^{-1}, so that each coefficient's
+          // solve below is one matrix-vector product.
           for (int q = threadIdx.x; q < n * n; q += blockDim.x) stn_at<PN>(sm + L.R, q, ldn_at<PN>(sm + L.J, q));
           __syncthreads();
-          small_qr<PN>(n, sm + L.Q, sm + L.R, sm + L.Ri, D);
-          // M = R^{-1} Q^H
-          for (int q = threadIdx.x; q < n * n; q += blockDim.x) {
-            const int i = q / n, j = q % n;
-            typename PN::T acc = PN::zero();
-            for (int l = i; l < n; ++l)
-              acc = PN::add(acc, PN::mul(ldn_at<PN>(sm + L.Ri, (long)i * n + l),
-                                         PN::conj(ldn_at<PN>(sm + L.Q, (long)j * n + l))));
-            stn_at<PN>(sm + L.M, q, acc);
-          }
-          __syncthreads();
+          cta_lufac<PN>(n, sm + L.R, piv, dinv, piv + 32);
+          cta_luinverse<PN>(n, sm + L.R, piv, dinv, sm + L.M);
         }
         for (int k = 0; k <= w; ++k) {
           for (int i = threadIdx.x; i < n; i += blockDim.x) {
@@ -350,7 +350,7 @@ __global__ void __launch_bounds__(kTrackThreads)
         degs[2 * threadIdx.x] = pdeg_i;
         degs[2 * threadIdx.x + 1] = qdeg_i;
       }
-      const double r = block_min(rmin, D.red);
+      const double r = block_min(rmin, red);
       const bool rfail = !(r < 1e299);
       double pole_step = rfail ? P.maxsize : P.pbeta * r;
       if (pole_step > P.maxsize) pole_step = P.maxsize;
@@ -384,7 +384,7 @@ __global__ void __launch_bounds__(kTrackThreads)
         bool ok = false;
         for (int h = 0; h < 64; ++h) {
           const double mixres = pade_mixres<PN>(S, s, n, K, P.dendeg, t, step, num, den, degs, xp, sm + L.V,
-                                                sm + L.G, sm + L.hs, D);
+                                                sm + L.G, sm + L.hs, red);
           if (mixres < P.alpha) { ok = true; break; }
           step *= 0.5;
           ++nrej;
@@ -401,8 +401,8 @@ __global__ void __launch_bounds__(kTrackThreads)
           for (int i = threadIdx.x; i < n; i += blockDim.x)
             stn_at<CN>(xc, i, conv_num<PN, CN>::go(ldn_at<PN>(xp, i)));
           __syncthreads();
-          if (point_newton<CN>(S, s, n, t + step, xc, sm + L.dxc, sm + L.hc, sm + L.Jc, sm + L.Qc, sm + L.Rc,
-                               sm + L.Ric, sm + L.Vc, sm + L.Gc, sm + L.wv, D, P.corsteps, P.tolres, 1, &dxn)) {
+          if (point_newton<CN>(S, s, n, t + step, xc, sm + L.hc, sm + L.Jc, sm + L.Vc, sm + L.Gc, piv, dinv, red,
+                               P.corsteps, P.tolres, 1, &dxn)) {
             cok = true;
             break;
           }
@@ -435,7 +435,7 @@ __global__ void __launch_bounds__(kTrackThreads)
           if (t + sp > 1.0) sp = 1.0 - t;
           if (sp <= best) continue;
           const double mr = pade_mixres<PN>(S, s, n, K, P.dendeg, t, sp, num, den, degs, sm + L.xp, sm + L.V,
-                                            sm + L.G, sm + L.hs, D);
+                                            sm + L.G, sm + L.hs, red);
           if (mr < P.alpha) best = sp;
         }
         if (threadIdx.x == 0) {
@@ -468,12 +468,12 @@ __global__ void __launch_bounds__(kTrackThreads)
     }
     double res;
     if (!failed && status == 0) {
-      point_newton<RN>(S, s, n, 1.0, xr, sm + L.dxc, sm + L.hc, sm + L.Jc, sm + L.Qc, sm + L.Rc, sm + L.Ric,
-                       sm + L.Vc, sm + L.Gc, sm + L.wv, D, P.refine_steps, 0.0, 0, &dxn);
-      res = point_residual<RN>(S, s, n, 1.0, xr, sm + L.hc, sm + L.Vc, sm + L.Gc, D);
+      point_newton<RN>(S, s, n, 1.0, xr, sm + L.hc, sm + L.Jc, sm + L.Vc, sm + L.Gc, piv, dinv, red, P.refine_steps,
+                       0.0, 0, &dxn);
+      res = point_residual<RN>(S, s, n, 1.0, xr, sm + L.hc, sm + L.Vc, sm + L.Gc, red);
       status = (res <= P.restol) ? 0 : 3;
     } else {
-      res = point_residual<RN>(S, s, n, t, xr, sm + L.hc, sm + L.Vc, sm + L.Gc, D);
+      res = point_residual<RN>(S, s, n, t, xr, sm + L.hc, sm + L.Vc, sm + L.Gc, red);
       status = failed ? 1 : 2;
     }
     for (int q = threadIdx.x; q < n_max * 8; q += blockDim.x) {
@@ -501,16 +501,16 @@ __global__ void __launch_bounds__(kTrackThreads)
 
 namespace phc {
 
-long track_smem_bytes(int maxdim, int K, int M, int nmono_max, int maxvar, int pmode, int rmode) {
+long track_smem_bytes(int maxdim, int K, int M, int nmono_max, int maxvar, int pmode, int rmode, int gst) {
   const int Wp = 2 * pmode, Wr = 2 * rmode;
-  return track_layout(maxdim, K, M, nmono_max, maxvar, Wp, Wr).total * (long)sizeof(double);
+  return track_layout(maxdim, K, M, nmono_max, maxvar, Wp, Wr, gst).total * (long)sizeof(double);
 }
 
 template <class PN, class CN, class RN>
 static int track_launch(const TrackDev &S, const TrackParDev &P, int nmono_max, int npaths, const int *path_sys,
                         const double *x0, const void *model, double *xend, int *info, double *dinfo, float *log,
                         int log_cap, int *log_count, int *queue, int one_per_launch, cudaStream_t st) {
-  const long smem = track_smem_bytes(S.maxdim, P.deg, P.dendeg, nmono_max, S.maxvar, PN::tr::limbs, RN::tr::limbs);
+  const long smem = track_smem_bytes(S.maxdim, P.deg, P.dendeg, nmono_max, S.maxvar, PN::tr::limbs, RN::tr::limbs, S.gstaged);
   if (smem > 227 * 1024) {
     set_error("track: %ld bytes of shared memory needed (dim %d, degree %d, %d monomials)", smem, S.maxdim, P.deg,
               nmono_max);

@@ -26,8 +26,16 @@ struct TrackDev {
   const double *term_b;  // [nterm*2]
   const int *jg_off;     // [neq*maxdim+1] Jacobian gather lists per (equation, variable)
   const int *jg_term;    // [njg] term id
-  const int *jg_slot;    // [njg] slot of the variable in the term's monomial
+  const int *jg_slot;    // [njg] >= 0: slot of the variable in the term's monomial (staged partial);
+                         // -1: the partial is 1; -2: it is 2 x_j; -3-l: it is x_l
+  int gstaged;           // some gather entry needs a staged partial
 };
+
+// A monomial of total degree <= 2 has partial derivatives that are a
+// variable's series, 2 x_j or 1: they are read in place, not staged.
+__host__ __device__ inline bool simple_monomial(int k, const int *ex) {
+  return (k == 1 && ex[0] >= 1 && ex[0] <= 2) || (k == 2 && ex[0] == 1 && ex[1] == 1);
+}
 
 // Tracking parameters (include/phc_b200.h, phc_track: ipar and dpar)
 struct TrackParDev {
@@ -85,7 +93,8 @@ __device__ __forceinline__ typename N::T cnum(double re, double im) {
 //   h[i*(w+1)+k]        value series of equation i,
 //   J[(k*n + i)*n + j]  Jacobian series (when J != nullptr).
 // V, G: shared staging for the distinct monomials, nm*(w+1) and
-// nm*maxvar*(w+1) numbers.
+// nm*maxvar*(w+1) numbers; G is written only when S.gstaged and J is wanted
+// (monomials of total degree <= 2 stage no partials).
 // Phase 1: one thread per distinct monomial computes its value and its
 // partials (exponent included) by the common-factor method and products of
 // the distinct variables.  Phase 2: one thread per output coefficient
@@ -102,11 +111,28 @@ __device__ void hom_eval_cta(const TrackDev &S, int s, int w, double t0, const d
   const int m0 = S.mono_off[s];
   const int nm = S.mono_off[s + 1] - m0;
   const int mv = S.maxvar;
+  const bool stage = S.gstaged && J != nullptr;
   for (int m = threadIdx.x; m < nm; m += blockDim.x) {
     const int gm = m0 + m;
     const int k = S.mono_nvr[gm];
     const int *ix = S.mono_idx + (long)gm * mv;
     const int *ex = S.mono_exp + (long)gm * mv;
+    if (k >= 1 && simple_monomial(k, ex)) {
+      // value only: x_j, x_j^2 or x_j x_l (the partials are read in place)
+      double *Vm = V + (long)m * n1 * W;
+      const double *xa = x + (long)ix[0] * xld * W;
+      const double *xb = (k == 2) ? x + (long)ix[1] * xld * W : xa;
+      if (k == 1 && ex[0] == 1) {
+        for (int i = 0; i < n1; ++i) stn_at<N>(Vm, i, ldn_at<N>(xa, i));
+      } else {
+        for (int kk = 0; kk < n1; ++kk) {
+          T a = N::zero();
+          for (int i = 0; i <= kk; ++i) a = N::add(a, N::mul(ldn_at<N>(xa, i), ldn_at<N>(xb, kk - i)));
+          stn_at<N>(Vm, kk, a);
+        }
+      }
+      continue;
+    }
     T F[kTrackKmax + 1], acc[kTrackKmax + 1];
     bool unitF = true;
     for (int i = 0; i < n1; ++i) F[i] = (i == 0) ? N::one() : N::zero();
@@ -126,7 +152,7 @@ __device__ void hom_eval_cta(const TrackDev &S, int s, int w, double t0, const d
       for (int i = 0; i < n1; ++i) stn_at<N>(Vm, i, F[i]);
       continue;
     }
-    for (int v = 0; v < k; ++v) {
+    for (int v = 0; v < (stage ? k : 1); ++v) {
       for (int i = 0; i < n1; ++i) acc[i] = F[i];
       bool unit = unitF;
       for (int u = 0; u < k; ++u) {
@@ -151,6 +177,7 @@ __device__ void hom_eval_cta(const TrackDev &S, int s, int w, double t0, const d
           stn_at<N>(Vm, kk, a);
         }
       }
+      if (!stage) continue;
       const double e = (double)ex[v];
       for (int i = 0; i < n1; ++i) stn_at<N>(Gm + (long)v * n1 * W, i, e == 1.0 ? acc[i] : N::scale_d(acc[i], e));
     }
@@ -159,11 +186,15 @@ __device__ void hom_eval_cta(const TrackDev &S, int s, int w, double t0, const d
   const int e0 = S.eq_off[s];
   const int nval = n * n1;
   const int njac = J ? n * n * n1 : 0;
-  for (int it = threadIdx.x; it < nval + njac; it += blockDim.x) {
-    T acc = N::zero();
-    if (it < nval) {
+  // values: one warp per (equation, coefficient), lanes over the equation's
+  // terms, a shuffle reduction (an equation has up to O(n^2) terms, so one
+  // thread per value would serialise the evaluation)
+  {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int it = warp; it < nval; it += nw) {
       const int i = it / n1, kk = it % n1;
-      for (int tr = S.term_off[e0 + i]; tr < S.term_off[e0 + i + 1]; ++tr) {
+      T acc = N::zero();
+      for (int tr = S.term_off[e0 + i] + lane; tr < S.term_off[e0 + i + 1]; tr += 32) {
         const T a = cnum<N>(S.term_a[2 * tr], S.term_a[2 * tr + 1]);
         const T b = cnum<N>(S.term_b[2 * tr], S.term_b[2 * tr + 1]);
         const T c0 = N::add(a, N::scale_d(b, t0));
@@ -171,9 +202,14 @@ __device__ void hom_eval_cta(const TrackDev &S, int s, int w, double t0, const d
         acc = N::add(acc, N::mul(c0, ldn_at<N>(Vm, kk)));
         if (kk > 0) acc = N::add(acc, N::mul(b, ldn_at<N>(Vm, kk - 1)));
       }
-      stn_at<N>(h, (long)i * n1 + kk, acc);
-    } else {
-      const int r = it - nval;
+      acc = warp_sum<N>(acc);
+      if (lane == 0) stn_at<N>(h, (long)i * n1 + kk, acc);
+    }
+  }
+  for (int it = threadIdx.x; it < njac; it += blockDim.x) {
+    T acc = N::zero();
+    {
+      const int r = it;
       const int kk = r / (n * n), i = (r / n) % n, j = r % n;
       const int g = (e0 + i) * S.maxdim + j;
       for (int q = S.jg_off[g]; q < S.jg_off[g + 1]; ++q) {
@@ -181,9 +217,27 @@ __device__ void hom_eval_cta(const TrackDev &S, int s, int w, double t0, const d
         const T a = cnum<N>(S.term_a[2 * tr], S.term_a[2 * tr + 1]);
         const T b = cnum<N>(S.term_b[2 * tr], S.term_b[2 * tr + 1]);
         const T c0 = N::add(a, N::scale_d(b, t0));
-        const double *Gm = G + ((long)(S.term_mono[tr] - m0) * mv + S.jg_slot[q]) * n1 * W;
-        acc = N::add(acc, N::mul(c0, ldn_at<N>(Gm, kk)));
-        if (kk > 0) acc = N::add(acc, N::mul(b, ldn_at<N>(Gm, kk - 1)));
+        const int sl = S.jg_slot[q];
+        T g0, g1 = N::zero();  // the partial's coefficients kk and kk-1
+        if (sl >= 0) {
+          const double *Gm = G + ((long)(S.term_mono[tr] - m0) * mv + sl) * n1 * W;
+          g0 = ldn_at<N>(Gm, kk);
+          if (kk > 0) g1 = ldn_at<N>(Gm, kk - 1);
+        } else if (sl == -1) {
+          g0 = (kk == 0) ? N::one() : N::zero();
+          g1 = (kk == 1) ? N::one() : N::zero();
+        } else {
+          const int l = (sl == -2) ? j : -sl - 3;
+          const double *xl = x + (long)l * xld * W;
+          g0 = ldn_at<N>(xl, kk);
+          if (kk > 0) g1 = ldn_at<N>(xl, kk - 1);
+          if (sl == -2) {
+            g0 = N::add(g0, g0);
+            g1 = N::add(g1, g1);
+          }
+        }
+        acc = N::add(acc, N::mul(c0, g0));
+        if (kk > 0) acc = N::add(acc, N::mul(b, g1));
       }
       stn_at<N>(J, ((long)kk * n + i) * n + j, acc);
     }
@@ -191,44 +245,131 @@ __device__ void hom_eval_cta(const TrackDev &S, int s, int w, double t0, const d
   __syncthreads();
 }
 
-// Q <- Q (I - beta v v^H) on columns c..n-1 of the n x n matrix Q
-// (Matrices/dbl2_factorizations.cpp:629/:662)
+// LU factorization with partial pivoting of the n x n matrix A (row-major,
+// shared memory, n <= 32), in place: lufac of
+// Math_Lib/Reduction/standard_complex_linear_solvers.adb:123-178 (LINPACK's
+// zgefa).  Column k pivots on the first row of largest |re| + |im| (leading
+// limbs), rows k and ell swap in columns k..n-1, and the multipliers
+// -a_ik / a_kk overwrite column k below the diagonal.  Besides ipvt the
+// reciprocals dinv[k] = 1 / u_kk are kept for the back substitution (NaN
+// for a zero pivot).
+// Warp 0 picks the pivot, swaps and forms the multipliers; the CTA updates
+// the trailing block: two barriers per column.  Returns info (every
+// thread): 0, or k + 1 for the first column k without a nonzero pivot.
+// sh: one shared int.
 template <class N>
-__device__ void block_apply_reflector_right(int n, int c, double *Q, dense_smem &S) {
+__device__ int cta_lufac(int n, double *A, int *ipvt, double *dinv, int *sh) {
   typedef typename N::T T;
-  typedef typename N::real R;
-  typedef md::num<R, false> RN;
-  const R beta = ldn_at<RN>(S.misc, 0);
-  if (md::is_zero(beta)) return;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    T acc = N::zero();
-    for (int j = c; j < n; ++j) acc = N::add(acc, N::mul(ldn_at<N>(Q, (long)i * n + j), ldn_at<N>(S.v, j - c)));
-    stn_at<N>(S.w, i, N::scale(acc, beta));
+  const int lane = threadIdx.x & 31;
+  int info = 0;  // meaningful in warp 0
+  for (int k = 0; k < n; ++k) {
+    if (threadIdx.x < 32) {
+      const int i = k + lane;
+      double v = -1.0;
+      if (i < n) {
+        v = N::lead(ldn_at<N>(A, (long)i * n + k));
+        if (!(v == v)) v = INFINITY;  // a NaN pivot candidate reads as infinity
+      }
+      int ix = i < n ? i : n;
+      for (int o = 16; o > 0; o >>= 1) {  // largest value, the first row on ties
+        const double v2 = __shfl_xor_sync(0xffffffffu, v, o);
+        const int ix2 = __shfl_xor_sync(0xffffffffu, ix, o);
+        if (v2 > v || (v2 == v && ix2 < ix)) { v = v2; ix = ix2; }
+      }
+      const int ell = ix < n ? ix : n - 1;
+      if (lane == 0) ipvt[k] = ell;
+      if (v == 0.0) {
+        if (info == 0) info = k + 1;  // this column is already triangularized
+        if (lane == 0) stn_at<N>(dinv, k, N::from(NAN));  // a solve with these factors gives NaN
+      } else {
+        if (ell != k)
+          for (int j = k + lane; j < n; j += 32) {
+            const T a = ldn_at<N>(A, (long)ell * n + j);
+            stn_at<N>(A, (long)ell * n + j, ldn_at<N>(A, (long)k * n + j));
+            stn_at<N>(A, (long)k * n + j, a);
+          }
+        __syncwarp();
+        const T inv = N::div(N::one(), ldn_at<N>(A, (long)k * n + k));
+        if (lane == 0) stn_at<N>(dinv, k, inv);
+        const T temp = N::neg(inv);
+        if (i > k && i < n) stn_at<N>(A, (long)i * n + k, N::mul(temp, ldn_at<N>(A, (long)i * n + k)));
+      }
+      if (k == n - 1 && lane == 0) *sh = info;
+    }
+    __syncthreads();
+    const int m = n - k - 1;
+    for (int e = threadIdx.x; e < m * m; e += blockDim.x) {
+      const int i = k + 1 + e / m, j = k + 1 + e % m;
+      const long o = (long)i * n + j;
+      stn_at<N>(A, o, N::add(ldn_at<N>(A, o), N::mul(ldn_at<N>(A, (long)k * n + j), ldn_at<N>(A, (long)i * n + k))));
+    }
+    __syncthreads();
   }
-  __syncthreads();
-  const int nc = n - c;
-  for (int t = threadIdx.x; t < n * nc; t += blockDim.x) {
-    const int i = t / nc, j = c + t % nc;
-    const long o = (long)i * n + j;
-    stn_at<N>(Q, o, N::sub(ldn_at<N>(Q, o), N::mul(ldn_at<N>(S.w, i), N::conj(ldn_at<N>(S.v, j - c)))));
-  }
-  __syncthreads();
+  return *sh;
 }
 
-// Householder QR of the n x n matrix in Rm (overwritten by R), Q formed
-// explicitly, then Minv = R^{-1} (upper triangular inverse).  Unblocked:
-// the systems the tracker solves are small.
+// Solve A x = b with the factors of cta_lufac: lusolve of
+// standard_complex_linear_solvers.adb:552-583 (row interchanges applied in
+// order with the multipliers, then back substitution), except that the back
+// substitution multiplies by dinv[k] = 1 / u_kk where lusolve divides.
+// Called by warp 0 alone, lane i holding b_i (n <= 32); returns x_i in
+// lane i (zero in lanes >= n).  negate: solve with -b.
 template <class N>
-__device__ void small_qr(int n, double *Q, double *Rm, double *Rinv, dense_smem &S) {
-  for (int t = threadIdx.x; t < n * n; t += blockDim.x)
-    stn_at<N>(Q, t, (t / n == t % n) ? N::one() : N::zero());
-  __syncthreads();
-  for (int c = 0; c < n; ++c) {
-    block_house<N>(n - c, Rm + (long)c * n * N::width + (long)c * N::width, n, S);
-    block_apply_reflector<N>(n, n, c, n, Rm, S);
-    block_apply_reflector_right<N>(n, c, Q, S);
+__device__ typename N::T warp_lusolve(int n, const double *A, const int *ipvt, const double *dinv, const double *b,
+                                      bool negate) {
+  typedef typename N::T T;
+  const int lane = threadIdx.x & 31;
+  T v = N::zero();
+  if (lane < n) {
+    v = ldn_at<N>(b, lane);
+    if (negate) v = N::neg(v);
   }
-  block_invert_tiles<N>(n, n, Rm, n, Rinv);
+  for (int k = 0; k < n - 1; ++k) {  // L y = P b
+    const int ell = ipvt[k];
+    const T t = md::shfl(v, ell);
+    const T bk = md::shfl(v, k);
+    if (lane == ell) v = bk;
+    if (lane == k) v = t;
+    if (lane > k && lane < n) v = N::add(v, N::mul(t, ldn_at<N>(A, (long)lane * n + k)));
+  }
+  for (int kb = n - 1; kb >= 0; --kb) {  // U x = y
+    if (lane == kb) v = N::mul(v, ldn_at<N>(dinv, kb));
+    const T t = md::shfl(v, kb);
+    if (lane < kb) v = N::sub(v, N::mul(t, ldn_at<N>(A, (long)lane * n + kb)));
+  }
+  return v;
+}
+
+// M = A^{-1} from the factors of cta_lufac, one thread per column c: the
+// column of M is the work vector of lusolve applied to e_c (same order of
+// operations as warp_lusolve).
+template <class N>
+__device__ void cta_luinverse(int n, const double *A, const int *ipvt, const double *dinv, double *M) {
+  typedef typename N::T T;
+  for (int c = threadIdx.x; c < n; c += blockDim.x) {
+    for (int i = 0; i < n; ++i) stn_at<N>(M, (long)i * n + c, i == c ? N::one() : N::zero());
+    for (int k = 0; k < n - 1; ++k) {
+      const int ell = ipvt[k];
+      const T t = ldn_at<N>(M, (long)ell * n + c);
+      if (ell != k) {
+        stn_at<N>(M, (long)ell * n + c, ldn_at<N>(M, (long)k * n + c));
+        stn_at<N>(M, (long)k * n + c, t);
+      }
+      for (int i = k + 1; i < n; ++i) {
+        const long o = (long)i * n + c;
+        stn_at<N>(M, o, N::add(ldn_at<N>(M, o), N::mul(t, ldn_at<N>(A, (long)i * n + k))));
+      }
+    }
+    for (int kb = n - 1; kb >= 0; --kb) {
+      const T x = N::mul(ldn_at<N>(M, (long)kb * n + c), ldn_at<N>(dinv, kb));
+      stn_at<N>(M, (long)kb * n + c, x);
+      for (int j = 0; j < kb; ++j) {
+        const long o = (long)j * n + c;
+        stn_at<N>(M, o, N::sub(ldn_at<N>(M, o), N::mul(x, ldn_at<N>(A, (long)j * n + kb))));
+      }
+    }
+  }
+  __syncthreads();
 }
 
 // y = M b, M n x n, one thread per row
@@ -238,18 +379,6 @@ __device__ void cta_matvec(int n, const double *M, const double *b, double *y) {
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
     T acc = N::zero();
     for (int j = 0; j < n; ++j) acc = N::add(acc, N::mul(ldn_at<N>(M, (long)i * n + j), ldn_at<N>(b, j)));
-    stn_at<N>(y, i, acc);
-  }
-  __syncthreads();
-}
-
-// y = M^H b
-template <class N>
-__device__ void cta_matvec_h(int n, const double *M, const double *b, double *y) {
-  typedef typename N::T T;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    T acc = N::zero();
-    for (int j = 0; j < n; ++j) acc = N::add(acc, N::mul(N::conj(ldn_at<N>(M, (long)j * n + i)), ldn_at<N>(b, j)));
     stn_at<N>(y, i, acc);
   }
   __syncthreads();

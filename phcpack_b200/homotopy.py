@@ -272,10 +272,11 @@ def gather_lists(pb: TrackProblem):
     jg_off = np.zeros(neq * pb.maxdim + 1, np.int32)
     jg_term = np.zeros(max(1, njg), np.int32)
     jg_slot = np.zeros(max(1, njg), np.int32)
-    _lib.call("phc_track_prepare", pb.nsys, _lib.ptr(pb.dim), pb.maxvar, _lib.ptr(pb.mono_off),
-              _lib.ptr(pb.mono_nvr), _lib.ptr(pb.mono_idx), _lib.ptr(pb.eq_off), _lib.ptr(pb.term_off),
-              _lib.ptr(pb.term_mono), pb.maxdim, _lib.ptr(jg_off), _lib.ptr(jg_term), _lib.ptr(jg_slot))
-    return jg_off, jg_term, jg_slot
+    staged = _lib.call("phc_track_prepare", pb.nsys, _lib.ptr(pb.dim), pb.maxvar, _lib.ptr(pb.mono_off),
+                       _lib.ptr(pb.mono_nvr), _lib.ptr(pb.mono_idx), _lib.ptr(pb.mono_exp), _lib.ptr(pb.eq_off),
+                       _lib.ptr(pb.term_off), _lib.ptr(pb.term_mono), pb.maxdim, _lib.ptr(jg_off), _lib.ptr(jg_term),
+                       _lib.ptr(jg_slot))
+    return jg_off, jg_term, jg_slot, staged
 
 
 class DeviceTracker:
@@ -289,7 +290,8 @@ class DeviceTracker:
         jg = gather_lists(pb)
         self.arr = {k: t(getattr(pb, k)) for k in ("dim", "mono_off", "mono_nvr", "mono_idx", "mono_exp", "eq_off",
                                                     "term_off", "term_mono", "term_a", "term_b", "path_sys", "x0")}
-        self.arr["jg_off"], self.arr["jg_term"], self.arr["jg_slot"] = (t(a) for a in jg)
+        self.arr["jg_off"], self.arr["jg_term"], self.arr["jg_slot"] = (t(a) for a in jg[:3])
+        self.gstaged = int(jg[3])
         self.xend = torch.zeros(pb.npaths * pb.maxdim * 8, dtype=torch.float64, device=device)
         self.info = torch.zeros(pb.npaths * 3, dtype=torch.int32, device=device)
         self.dinfo = torch.zeros(pb.npaths * 2, dtype=torch.float64, device=device)
@@ -313,7 +315,7 @@ class DeviceTracker:
         _lib.call("phc_track", pb.nsys, _lib.ptr(a["dim"]), pb.maxvar, pb.maxdim, pb.nmono_max, _lib.ptr(a["mono_off"]),
                   _lib.ptr(a["mono_nvr"]), _lib.ptr(a["mono_idx"]), _lib.ptr(a["mono_exp"]), _lib.ptr(a["eq_off"]),
                   _lib.ptr(a["term_off"]), _lib.ptr(a["term_mono"]), _lib.ptr(a["term_a"]), _lib.ptr(a["term_b"]),
-                  _lib.ptr(a["jg_off"]), _lib.ptr(a["jg_term"]), _lib.ptr(a["jg_slot"]), pb.npaths,
+                  _lib.ptr(a["jg_off"]), _lib.ptr(a["jg_term"]), _lib.ptr(a["jg_slot"]), self.gstaged, pb.npaths,
                   _lib.ptr(a["path_sys"]), _lib.ptr(a["x0"]), _lib.ptr(ipar), _lib.ptr(dpar), pmode, rmode, step_mode,
                   _lib.ptr(self.model) if (step_mode and self.model is not None) else _lib.c_void_p(0),
                   _lib.ptr(self.xend), _lib.ptr(self.info), _lib.ptr(self.dinfo),
