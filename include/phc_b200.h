@@ -185,8 +185,10 @@ int phc_newton_host(int prec, int cplx, int nsys, int dim, int deg, int szt, int
  *   steps), corsteps, maxsteps, refine_steps.
  * dpar: pbeta, alpha, maxsize, minsize, tolres, epsilon, restol (endpoint
  *   residual bound), learn_scale (multiplies learned proposals; 0 = 1).
- * pmode: predictor precision 1 (double) or 2 (double-double); the corrector
- *   is double-double; rmode: refinement precision 2 or 4 (quad-double).
+ * pmode: 1 (double) or 2 (double-double), the precision of the predictor
+ *   and of the corrector's Jacobian and linear solves; the corrector's
+ *   residuals and updates are double-double; rmode: refinement precision 2
+ *   or 4 (quad-double), all of its arithmetic.
  * step_mode 1 with a model (phc_mlp_*) uses the learned step proposer; a
  *   proposal whose feedback or corrector fails is redone with the plain step.
  * Output per path: xend maxdim complex quad-doubles (lower limbs zero below
@@ -224,7 +226,8 @@ int phc_track_host(int nsys, const int *dim, int maxvar, const int *mono_off, co
  * and curvature steps only).  A 24 -> 128 -> 128 -> 1 ReLU network predicts
  * log(accepted step / pole step) from 24 features of the predictor's series
  * (phcpack_b200/csrc/mlp.cuh).  Model buffer: FP32 normalisation and biases,
- * BF16 weights, phc_mlp_model_bytes() bytes.  Training keeps FP32 master
+ * BF16 weights, phc_mlp_model_bytes() bytes, 16-byte aligned (phc_track
+ * checks).  Training keeps FP32 master
  * parameters (phc_mlp_param_count() floats: W1[128][24], b1[128],
  * W2[128][128], b2[128], W3[128], b3) and Adam moments of the same size. */
 long long phc_mlp_model_bytes(void);

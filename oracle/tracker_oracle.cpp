@@ -26,7 +26,8 @@
 //  * predictor feedback: halve the step until the mixed residual of the
 //    Pade prediction is below alpha (fail below minsize);
 //  * corrector: at most corsteps LU Newton steps at the new t (LU_Newton_Steps,
-//    Curves/corrector_convolutions.adb:1193-1224), converged when
+//    Curves/corrector_convolutions.adb:1193-1224), residuals in double-double,
+//    the Jacobian and its solve in the predictor's precision, converged when
 //    max |dx_i| <= tolres, followed by one extra step; on failure halve the
 //    step and re-evaluate the Pade approximant (fail below minsize);
 //  * stop when |1 - t| < epsilon; refine the endpoint at t = 1 and classify
@@ -340,23 +341,42 @@ template <class T> static T horner(const std::vector<T> &a, int deg, const T &z)
   return acc;
 }
 
-// Newton at a point (the corrector / refinement), returns converged
-template <class T>
+// conversions between the precisions (round to nearest double; widen exactly)
+template <class PT, class CT> static void convert(const CT &a, PT &b);
+template <> void convert(const cx<dd> &a, cx<double> &b) { b = cx<double>(a.re.hi + a.re.lo, a.im.hi + a.im.lo); }
+template <> void convert(const cx<dd> &a, cx<dd> &b) { b = a; }
+template <> void convert(const cx<double> &a, cx<dd> &b) { b = cx<dd>(dd(a.re), dd(a.im)); }
+template <> void convert(const cx<dd> &a, cx<qd> &b) { b = cx<qd>(qd(a.re), qd(a.im)); }
+template <> void convert(const cx<qd> &a, cx<qd> &b) { b = a; }
+
+// Newton at a point (the corrector / refinement), returns converged:
+// LU_Newton_Steps (Curves/corrector_convolutions.adb:1193-1224) with h in
+// precision T and the Jacobian, its LU and the solve in precision JT (T, or
+// double in the precision-split tracker, as on the GPU); x += dx in T.
+template <class T, class JT>
 static bool point_newton(const TrackSys &S, int s, double t, std::vector<T> &x, int maxit, double tol, int extra,
                          double *lastdx) {
   const int n = S.dim[s];
   std::vector<std::vector<T> > xs(n, std::vector<T>(1)), h;
-  std::vector<T> jac, dx(n);
-  lu_solver<T> lu;
+  std::vector<std::vector<JT> > xj(n, std::vector<JT>(1)), hj;
+  std::vector<JT> jac, dx(n);
+  lu_solver<JT> lu;
   bool conv = false;
   int extra_left = extra;
   *lastdx = 1e300;
   for (int it = 0; it < maxit + extra; ++it) {
     if (it >= maxit && !conv) break;
-    for (int i = 0; i < n; ++i) xs[i][0] = x[i];
-    hom_eval(S, s, 0, t, xs, h, &jac);
+    for (int i = 0; i < n; ++i) {
+      xs[i][0] = x[i];
+      convert(x[i], xj[i][0]);
+    }
+    hom_eval<T>(S, s, 0, t, xs, h, nullptr);
+    hom_eval(S, s, 0, t, xj, hj, &jac);
     lu.factor(n, jac);
-    for (int i = 0; i < n; ++i) dx[i] = -h[i][0];
+    for (int i = 0; i < n; ++i) {
+      convert(h[i][0], dx[i]);
+      dx[i] = -dx[i];
+    }
     lu.solve(dx.data(), dx.data());
     if (lu.info != 0) {  // singular Jacobian: x unchanged, not converged
       *lastdx = INFINITY;
@@ -364,7 +384,9 @@ static bool point_newton(const TrackSys &S, int s, double t, std::vector<T> &x, 
     }
     double m = 0.0;
     for (int i = 0; i < n; ++i) {
-      x[i] = x[i] + dx[i];
+      T d;
+      convert(dx[i], d);
+      x[i] = x[i] + d;
       const double a = cabs(dx[i]);
       m = (a > m || std::isnan(a)) ? a : m;
     }
@@ -390,12 +412,6 @@ template <class T> static double maxres(const TrackSys &S, int s, double t, cons
   return r;
 }
 
-template <class PT, class CT> static void convert(const CT &a, PT &b);
-template <> void convert(const cx<dd> &a, cx<double> &b) { b = cx<double>(a.re.hi + a.re.lo, a.im.hi + a.im.lo); }
-template <> void convert(const cx<dd> &a, cx<dd> &b) { b = a; }
-template <> void convert(const cx<double> &a, cx<dd> &b) { b = cx<dd>(dd(a.re), dd(a.im)); }
-template <> void convert(const cx<dd> &a, cx<qd> &b) { b = cx<qd>(qd(a.re), qd(a.im)); }
-template <> void convert(const cx<qd> &a, cx<qd> &b) { b = a; }
 
 struct PathOut {
   int status, nsteps, nreject;
@@ -412,7 +428,7 @@ static PathOut track_path(const TrackSys &S, int s, const TrackPar &P, const dou
   std::vector<CT> x(n);
   for (int i = 0; i < n; ++i) convert(cx<double>(x0[2 * i], x0[2 * i + 1]), x[i]);
   double t = 0.0, dxn;
-  point_newton(S, s, 0.0, x, P.corsteps, P.tolres, 1, &dxn);
+  point_newton<CT, PT>(S, s, 0.0, x, P.corsteps, P.tolres, 1, &dxn);
   std::vector<std::vector<PT> > xs(n, std::vector<PT>(K + 1));
   std::vector<std::vector<PT> > num(n), den(n);
   std::vector<CT> xc(n);
@@ -470,7 +486,7 @@ static PathOut track_path(const TrackSys &S, int s, const TrackPar &P, const dou
     // corrector with step halving
     for (;;) {
       for (int i = 0; i < n; ++i) convert(xp[i], xc[i]);
-      if (point_newton(S, s, t + step, xc, P.corsteps, P.tolres, 1, &dxn)) break;
+      if (point_newton<CT, PT>(S, s, t + step, xc, P.corsteps, P.tolres, 1, &dxn)) break;
       step *= 0.5;
       ++o.nreject;
       if (step < P.minsize) break;
@@ -486,7 +502,7 @@ static PathOut track_path(const TrackSys &S, int s, const TrackPar &P, const dou
   std::vector<RT> xr(n);
   for (int i = 0; i < n; ++i) convert(x[i], xr[i]);
   if (!failed && std::fabs(1.0 - t) < P.epsilon) {
-    point_newton(S, s, 1.0, xr, P.refine_steps, 0.0, 0, &dxn);
+    point_newton<RT, RT>(S, s, 1.0, xr, P.refine_steps, 0.0, 0, &dxn);
     o.residual = maxres(S, s, 1.0, xr);
     o.status = (o.residual <= P.restol) ? 0 : 3;
   } else {

@@ -44,10 +44,13 @@ __host__ __device__ inline MlpView mlp_view(const void *base) {
 //   f[8..15]  log of the ratio radius min_i |c_i,k-1| / |c_ik|, k = 1..8
 //   f[16..19] log pole step, t, log(1 - t), log n
 //   f[20..23] log max_i |c_ik| for k = 0..3
-// Orders beyond K repeat the last one.
-__device__ inline void track_features(int n, int K, double t, double pole_step, const double *mag, float *f) {
+// Orders beyond K repeat the last one.  Every thread of the CTA calls it
+// with its number tid; threads 0..12 compute a share each.
+__device__ inline void track_features(int tid, int n, int K, double t, double pole_step, const double *mag,
+                                      float *f) {
   const double tiny = 1e-300;
-  for (int q = 0; q < 8; ++q) {
+  if (tid < 8) {
+    const int q = tid;
     const int k = (q + 1 <= K) ? q + 1 : K;
     double mx = 0.0, rmin = 1e300;
     for (int i = 0; i < n; ++i) {
@@ -59,16 +62,17 @@ __device__ inline void track_features(int n, int K, double t, double pole_step, 
     double rr = (rmin < 1e299) ? log(rmin + tiny) : 30.0;
     f[q] = (float)fmin(fmax(rt, -30.0), 30.0);
     f[8 + q] = (float)fmin(fmax(rr, -30.0), 30.0);
-  }
-  f[16] = (float)log(pole_step + tiny);
-  f[17] = (float)t;
-  f[18] = (float)log(fmax(1.0 - t, 1e-16));
-  f[19] = (float)log((double)n);
-  for (int q = 0; q < 4; ++q) {
+  } else if (tid < 12) {
+    const int q = tid - 8;
     const int k = q <= K ? q : K;
     double mx = 0.0;
     for (int i = 0; i < n; ++i) mx = fmax(mx, mag[i * (K + 1) + k]);
     f[20 + q] = (float)fmin(fmax(log(mx + tiny), -60.0), 60.0);
+  } else if (tid == 12) {
+    f[16] = (float)log(pole_step + tiny);
+    f[17] = (float)t;
+    f[18] = (float)log(fmax(1.0 - t, 1e-16));
+    f[19] = (float)log((double)n);
   }
 }
 
@@ -79,17 +83,33 @@ __device__ inline float mlp_forward_cta(const void *model, const float *feat, fl
   const MlpView M = mlp_view(model);
   const int j = threadIdx.x;
   float *h1 = hbuf, *h2 = hbuf + kMlpH, *red = hbuf + 2 * kMlpH;
+  // rows of W1 and W2 read 8 weights (16 bytes) at a time; the sums keep
+  // the order i = 0, 1, ... (the model buffer is 16-byte aligned)
   if (j < kMlpH) {
     float a = M.b1[j];
-    for (int i = 0; i < kMlpIn; ++i)
-      a = fmaf(__bfloat162float(M.W1[j * kMlpIn + i]), (feat[i] - M.mean[i]) * M.inv_std[i], a);
+    const uint4 *w = reinterpret_cast<const uint4 *>(M.W1 + j * kMlpIn);
+    for (int c = 0; c < kMlpIn / 8; ++c) {
+      const uint4 u = __ldg(w + c);
+      const __nv_bfloat16 *e = reinterpret_cast<const __nv_bfloat16 *>(&u);
+#pragma unroll
+      for (int r = 0; r < 8; ++r) {
+        const int i = 8 * c + r;
+        a = fmaf(__bfloat162float(e[r]), (feat[i] - M.mean[i]) * M.inv_std[i], a);
+      }
+    }
     h1[j] = fmaxf(a, 0.0f);
   }
   __syncthreads();
   float contrib = 0.0f;
   if (j < kMlpH) {
     float a = M.b2[j];
-    for (int i = 0; i < kMlpH; ++i) a = fmaf(__bfloat162float(M.W2[j * kMlpH + i]), h1[i], a);
+    const uint4 *w = reinterpret_cast<const uint4 *>(M.W2 + j * kMlpH);
+    for (int c = 0; c < kMlpH / 8; ++c) {
+      const uint4 u = __ldg(w + c);
+      const __nv_bfloat16 *e = reinterpret_cast<const __nv_bfloat16 *>(&u);
+#pragma unroll
+      for (int r = 0; r < 8; ++r) a = fmaf(__bfloat162float(e[r]), h1[8 * c + r], a);
+    }
     h2[j] = fmaxf(a, 0.0f);
     contrib = __bfloat162float(M.W3[j]) * h2[j];
   }

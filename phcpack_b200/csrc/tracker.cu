@@ -12,8 +12,10 @@
 //     [L/M] Pade approximant per component; pole step pbeta * r, r the
 //     smallest Fabry radius |c_{K-3}/c_{K-2}|; step <= maxsize, cut at t = 1;
 //     predictor feedback: halve until the mixed residual < alpha;
-//   corrector, in double-double: at most corsteps LU Newton steps, converged
-//     when max |dx| <= tolres, plus one extra step; on failure halve the step;
+//   corrector: at most corsteps LU Newton steps with residuals and updates
+//     in double-double and the Jacobian and its solve in PN precision,
+//     converged when max |dx| <= tolres, plus one extra step; on failure
+//     halve the step;
 //   the step size comes from a learned model when one is given (step_mode
 //     1): a proposal whose corrector fails is rejected and the step is
 //     redone with the plain pole step;
@@ -80,7 +82,7 @@ __host__ __device__ inline TrackLayout track_layout(int n, int K, int M, int nm,
 template <class N>
 __device__ double cta_maxmag(int n, const double *v, double *red) {
   double a = 0.0;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+  for (int i = ctid(); i < n; i += blockDim.x) {
     const double m = N::mag(ldn_at<N>(v, i));
     a = (m != m) ? INFINITY : fmax(a, m);  // a NaN reads as infinity
   }
@@ -89,11 +91,15 @@ __device__ double cta_maxmag(int n, const double *v, double *red) {
 
 // Newton at a point in precision N (the corrector and the refinement):
 // LU_Newton_Steps of Curves/corrector_convolutions.adb:1193-1224 restated:
-// each step factors J(x) by cta_lufac and solves J dx = -h(x) (a singular
-// Jacobian ends the steps unconverged, x unchanged), converged when
-// max |dx| <= tol, then extra more steps.  x (shared, n numbers) is updated
-// in place; lastdx: the last max |dx|.
-template <class N>
+// each step evaluates h(x) in precision N and J(x) in precision JN (N, or
+// double in the precision-split tracker: Newton with a double Jacobian and
+// a residual in N still converges to the accuracy of N, each step gaining
+// about 16 digits near the solution), factors J by cta_lufac and solves
+// J dx = -h(x) (a singular Jacobian ends the steps unconverged, x
+// unchanged); converged when max |dx| <= tol, then extra more steps.  x
+// (shared, n numbers of precision N) is updated in place; lastdx: the last
+// max |dx|.
+template <class N, class JN>
 __device__ bool point_newton(const TrackDev &S, int s, int n, double t, double *x, double *h, double *Jm, double *Vc,
                              double *Gc, int *piv, double *dinv, double *red, int maxit, double tol, int extra,
                              double *lastdx) {
@@ -102,18 +108,21 @@ __device__ bool point_newton(const TrackDev &S, int s, int n, double t, double *
   *lastdx = 1e300;
   for (int it = 0; it < maxit + extra; ++it) {
     if (it >= maxit && !conv) break;
-    hom_eval_cta<N>(S, s, 0, t, x, 1, Vc, Gc, h, Jm);
-    const int info = cta_lufac<N>(n, Jm, piv, dinv, piv + 32);
-    if (threadIdx.x < 32) {
-      const typename N::T v = warp_lusolve<N>(n, Jm, piv, dinv, h, true);
+    hom_eval_cta<N, 1, JN>(S, s, 0, t, x, 1, Vc, Gc, h, Jm);
+    const int info = cta_lufac<JN>(n, Jm, piv, dinv, piv + 32);
+    if (ctid() < 32) {
+      const int lane = ctid();
+      typename JN::T b = JN::zero();
+      if (lane < n) b = JN::neg(conv_num<N, JN>::go(ldn_at<N>(h, lane)));
+      const typename JN::T v = warp_lusolve<JN>(n, Jm, piv, dinv, b);
       double m = 0.0;
-      if ((threadIdx.x & 31) < n) {
-        m = N::mag(v);
+      if (lane < n) {
+        m = JN::mag(v);
         if (!(m == m)) m = INFINITY;
-        if (info == 0) stn_at<N>(x, threadIdx.x, N::add(ldn_at<N>(x, threadIdx.x), v));
+        if (info == 0) stn_at<N>(x, lane, N::add(ldn_at<N>(x, lane), conv_num<JN, N>::go(v)));
       }
       m = warp_max(m);
-      if (threadIdx.x == 0) red[0] = info ? INFINITY : m;
+      if (lane == 0) red[0] = info ? INFINITY : m;
     }
     __syncthreads();
     const double m = red[0];
@@ -209,7 +218,7 @@ __device__ double pade_mixres(const TrackDev &S, int s, int n, int K, int dendeg
                               const double *num, const double *den, const int *degs, double *xp, double *V,
                               double *G, double *hs, double *red) {
   const int Wp = PN::width;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+  for (int i = ctid(); i < n; i += blockDim.x) {
     const typename PN::T z = PN::from(st);
     const typename PN::T nv = horner<PN>(num + (long)i * (K + 1) * Wp, degs[2 * i], z);
     const typename PN::T dv = horner<PN>(den + (long)i * (dendeg + 1) * Wp, degs[2 * i + 1], z);
@@ -218,7 +227,7 @@ __device__ double pade_mixres(const TrackDev &S, int s, int n, int K, int dendeg
   __syncthreads();
   hom_eval_cta<PN>(S, s, 0, t + st, xp, 1, V, G, hs, nullptr);
   // one warp per equation, lanes over its terms
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int lane = ctid() & 31, warp = ctid() >> 5, nw = blockDim.x >> 5;
   double part = 0.0;
   for (int i = warp; i < n; i += nw) {
     double ab = 0.0;
@@ -259,13 +268,14 @@ __global__ void __launch_bounds__(kTrackThreads)
   double *red = sm + L.red;
   int *piv = reinterpret_cast<int *>(sm + L.piv);
   double *dinv = sm + L.dinv;
+  track_pick_lead();
   int next_static = blockIdx.x;
   for (;;) {
     if (queue) {
-      if (threadIdx.x == 0) cur = atomicAdd(queue, 1);
+      if (ctid() == 0) cur = atomicAdd(queue, 1);
       __syncthreads();
     } else {
-      if (threadIdx.x == 0) cur = next_static;
+      if (ctid() == 0) cur = next_static;
       __syncthreads();
       next_static += gridDim.x;
     }
@@ -277,20 +287,20 @@ __global__ void __launch_bounds__(kTrackThreads)
     const int n = S.dim[s];
     double *xc = sm + L.xc;
     // start point, refined at t = 0
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    for (int i = ctid(); i < n; i += blockDim.x) {
       const double *z = x0 + ((long)path * n_max + i) * 2;
       stn_at<CN>(xc, i, cnum<CN>(z[0], z[1]));
     }
     __syncthreads();
     double t = 0.0, dxn;
-    point_newton<CN>(S, s, n, 0.0, xc, sm + L.hc, sm + L.Jc, sm + L.Vc, sm + L.Gc, piv, dinv, red, P.corsteps,
+    point_newton<CN, PN>(S, s, n, 0.0, xc, sm + L.hc, sm + L.Jc, sm + L.Vc, sm + L.Gc, piv, dinv, red, P.corsteps,
                      P.tolres, 1, &dxn);
     int status = 2, nsteps = 0, nrej = 0;
     bool failed = false;
     for (int step_it = 0; step_it < P.maxsteps; ++step_it) {
       // ---------------- predictor: Newton on power series in PN
       double *xs = sm + L.xs;
-      for (int t2 = threadIdx.x; t2 < n * (K + 1); t2 += blockDim.x) {
+      for (int t2 = ctid(); t2 < n * (K + 1); t2 += blockDim.x) {
         const int i = t2 / (K + 1), k = t2 % (K + 1);
         typename PN::T v = PN::zero();
         if (k == 0) v = conv_num<CN, PN>::go(ldn_at<CN>(xc, i));
@@ -300,20 +310,22 @@ __global__ void __launch_bounds__(kTrackThreads)
       for (int it = 0; it < P.nit; ++it) {
         int w = (2 << it) - 1;
         if (w > K) w = K;
-        hom_eval_cta<PN>(S, s, w, t, xs, K + 1, sm + L.V, sm + L.G, sm + L.hs, sm + L.J);
+        // 9 coefficients per pass (the degree-8 series in one) for double
+        // predictors, 5 for double-double (register pressure)
+        hom_eval_cta<PN, (PN::width <= 2 ? 9 : 5)>(S, s, w, t, xs, K + 1, sm + L.V, sm + L.G, sm + L.hs, sm + L.J);
         if (it == 0) {
           // J_0 factored once per step (LU_Prediction,
           // Curves/standard_predictor_convolutions.adb:1142-1185, factors
           // J_0 once by lufac and reuses it for every coefficient): the LU
           // of a copy of J_0, then M = J_0^{-1}, so that each coefficient's
           // solve below is one matrix-vector product.
-          for (int q = threadIdx.x; q < n * n; q += blockDim.x) stn_at<PN>(sm + L.R, q, ldn_at<PN>(sm + L.J, q));
+          for (int q = ctid(); q < n * n; q += blockDim.x) stn_at<PN>(sm + L.R, q, ldn_at<PN>(sm + L.J, q));
           __syncthreads();
           cta_lufac<PN>(n, sm + L.R, piv, dinv, piv + 32);
           cta_luinverse<PN>(n, sm + L.R, piv, dinv, sm + L.M);
         }
         for (int k = 0; k <= w; ++k) {
-          for (int i = threadIdx.x; i < n; i += blockDim.x) {
+          for (int i = ctid(); i < n; i += blockDim.x) {
             typename PN::T acc = PN::neg(ldn_at<PN>(sm + L.hs, (long)i * (w + 1) + k));
             for (int j = 1; j <= k; ++j)
               for (int l = 0; l < n; ++l)
@@ -324,7 +336,7 @@ __global__ void __launch_bounds__(kTrackThreads)
           __syncthreads();
           cta_matvec<PN>(n, sm + L.M, sm + L.rhs, sm + L.dx + (long)k * n * Wp);
         }
-        for (int t2 = threadIdx.x; t2 < n * (w + 1); t2 += blockDim.x) {
+        for (int t2 = ctid(); t2 < n * (w + 1); t2 += blockDim.x) {
           const int i = t2 / (w + 1), k = t2 % (w + 1);
           const long o = (long)i * (K + 1) + k;
           stn_at<PN>(xs, o, PN::add(ldn_at<PN>(xs, o), ldn_at<PN>(sm + L.dx, (long)k * n + i)));
@@ -335,7 +347,7 @@ __global__ void __launch_bounds__(kTrackThreads)
       int pdeg_i = 0, qdeg_i = 0;
       double rmin = 1e300;
       double *num = sm + L.num, *den = sm + L.den;
-      for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      for (int i = ctid(); i < n; i += blockDim.x) {
         const double *ci = xs + (long)i * (K + 1) * Wp;
         pdeg_i = pade_one<PN>(P.numdeg, P.dendeg, K, ci, num + (long)i * (K + 1) * Wp, den + (long)i * (P.dendeg + 1) * Wp);
         qdeg_i = (pdeg_i == P.numdeg) ? P.dendeg : 0;
@@ -346,9 +358,9 @@ __global__ void __launch_bounds__(kTrackThreads)
       }
       // per-component Pade degrees go to shared memory for the evaluations
       int *degs = reinterpret_cast<int *>(sm + L.degs);
-      if (threadIdx.x < n) {
-        degs[2 * threadIdx.x] = pdeg_i;
-        degs[2 * threadIdx.x + 1] = qdeg_i;
+      if (ctid() < n) {
+        degs[2 * ctid()] = pdeg_i;
+        degs[2 * ctid() + 1] = qdeg_i;
       }
       const double r = block_min(rmin, red);
       const bool rfail = !(r < 1e299);
@@ -358,7 +370,7 @@ __global__ void __launch_bounds__(kTrackThreads)
       bool learned = false;
       float *feat = reinterpret_cast<float *>(sm + L.feat);
       if ((P.step_mode == 1 && model != nullptr) || log != nullptr) {
-        if (threadIdx.x == 0) track_features(n, K, t, pole_step, sm + L.mag, feat);
+        track_features(ctid(), n, K, t, pole_step, sm + L.mag, feat);
         __syncthreads();
       }
       if (P.step_mode == 1 && model != nullptr) {
@@ -398,10 +410,10 @@ __global__ void __launch_bounds__(kTrackThreads)
         // corrector with step halving
         bool cok = false;
         for (int h = 0; h < 64; ++h) {
-          for (int i = threadIdx.x; i < n; i += blockDim.x)
+          for (int i = ctid(); i < n; i += blockDim.x)
             stn_at<CN>(xc, i, conv_num<PN, CN>::go(ldn_at<PN>(xp, i)));
           __syncthreads();
-          if (point_newton<CN>(S, s, n, t + step, xc, sm + L.hc, sm + L.Jc, sm + L.Vc, sm + L.Gc, piv, dinv, red,
+          if (point_newton<CN, PN>(S, s, n, t + step, xc, sm + L.hc, sm + L.Jc, sm + L.Vc, sm + L.Gc, piv, dinv, red,
                                P.corsteps, P.tolres, 1, &dxn)) {
             cok = true;
             break;
@@ -410,7 +422,7 @@ __global__ void __launch_bounds__(kTrackThreads)
           if (learned) break;  // rejected proposal: retry with the plain step
           step *= 0.5;
           if (step < P.minsize) break;
-          for (int i = threadIdx.x; i < n; i += blockDim.x) {
+          for (int i = ctid(); i < n; i += blockDim.x) {
             const typename PN::T z = PN::from(step);
             const int pd = degs[2 * i], qd = degs[2 * i + 1];
             stn_at<PN>(xp, i, PN::div(horner<PN>(num + (long)i * (K + 1) * Wp, pd, z),
@@ -438,7 +450,7 @@ __global__ void __launch_bounds__(kTrackThreads)
                                             sm + L.G, sm + L.hs, red);
           if (mr < P.alpha) best = sp;
         }
-        if (threadIdx.x == 0) {
+        if (ctid() == 0) {
           const int slot = atomicAdd(log_count, 1);
           if (slot < log_cap) {
             float *f = log + (long)slot * 32;
@@ -461,14 +473,14 @@ __global__ void __launch_bounds__(kTrackThreads)
     // xc holds CN numbers: widen in place from the top (RN width >= CN width)
     if (RN::width != CN::width) {  // n <= blockDim.x: one number per thread
       typename CN::T v = CN::zero();
-      if (threadIdx.x < n) v = ldn_at<CN>(xc, threadIdx.x);
+      if (ctid() < n) v = ldn_at<CN>(xc, ctid());
       __syncthreads();
-      if (threadIdx.x < n) stn_at<RN>(xr, threadIdx.x, conv_num<CN, RN>::go(v));
+      if (ctid() < n) stn_at<RN>(xr, ctid(), conv_num<CN, RN>::go(v));
       __syncthreads();
     }
     double res;
     if (!failed && status == 0) {
-      point_newton<RN>(S, s, n, 1.0, xr, sm + L.hc, sm + L.Jc, sm + L.Vc, sm + L.Gc, piv, dinv, red, P.refine_steps,
+      point_newton<RN, RN>(S, s, n, 1.0, xr, sm + L.hc, sm + L.Jc, sm + L.Vc, sm + L.Gc, piv, dinv, red, P.refine_steps,
                        0.0, 0, &dxn);
       res = point_residual<RN>(S, s, n, 1.0, xr, sm + L.hc, sm + L.Vc, sm + L.Gc, red);
       status = (res <= P.restol) ? 0 : 3;
@@ -476,7 +488,7 @@ __global__ void __launch_bounds__(kTrackThreads)
       res = point_residual<RN>(S, s, n, t, xr, sm + L.hc, sm + L.Vc, sm + L.Gc, red);
       status = failed ? 1 : 2;
     }
-    for (int q = threadIdx.x; q < n_max * 8; q += blockDim.x) {
+    for (int q = ctid(); q < n_max * 8; q += blockDim.x) {
       const int i = q / 8, c = q % 8;
       double v = 0.0;
       if (i < n) {
@@ -486,7 +498,7 @@ __global__ void __launch_bounds__(kTrackThreads)
       }
       xend[((long)path * n_max) * 8 + q] = v;
     }
-    if (threadIdx.x == 0) {
+    if (ctid() == 0) {
       info[3 * path] = status;
       info[3 * path + 1] = nsteps;
       info[3 * path + 2] = nrej;
@@ -552,6 +564,7 @@ int track(const TrackDev &S, const TrackParDev &P, int nmono_max, int npaths, co
   PHC_REQUIRE(P.deg >= 3 && P.deg <= kTrackKmax && P.numdeg + P.dendeg == P.deg && P.dendeg <= 8 && P.nit >= 1,
               "track: need 3 <= deg = numdeg + dendeg <= %d, dendeg <= 8", kTrackKmax);
   PHC_REQUIRE(queue != nullptr || one_per_launch, "track: the batched launch needs a queue counter");
+  PHC_REQUIRE(model == nullptr || (reinterpret_cast<unsigned long long>(model) & 15) == 0, "track: the model buffer is not 16-byte aligned");
   if (npaths == 0) return PHC_OK;
   typedef md::num<double, true> Z1;
   typedef md::num<md::dd, true> Z2;

@@ -11,6 +11,40 @@ namespace phc {
 static const int kTrackThreads = 128;
 static const int kTrackKmax = 16;   // largest series degree of the predictor
 
+// Thread numbering of the tracker's CTA.  The first warp of the numbering
+// does the serial parts of a step (pivots, the point solves, the scalar
+// decisions).  Warps are spread over an SM's four sub-partitions by their
+// hardware slot (%warpid mod 4) and a CTA takes consecutive slots, so with
+// threadIdx.x the first warps of all CTAs on an SM would queue on one
+// sub-partition.  Each CTA instead numbers its threads from a lead warp
+// picked by its slot: ctid() is threadIdx.x rotated by whole warps (lanes
+// and warp membership unchanged).  track_pick_lead sets the rotation once
+// per CTA; blockDim.x == kTrackThreads.
+__shared__ int track_rot;
+
+__device__ __forceinline__ int ctid() { return (threadIdx.x + track_rot) & (kTrackThreads - 1); }
+
+__device__ inline void track_pick_lead() {
+  __shared__ int slot[kTrackThreads / 32];
+  const int nw = kTrackThreads / 32;
+  if ((threadIdx.x & 31) == 0) {
+    unsigned w;
+    asm volatile("mov.u32 %0, %%warpid;" : "=r"(w));
+    slot[threadIdx.x >> 5] = (int)w;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int mn = slot[0];
+    for (int v = 1; v < nw; ++v) mn = min(mn, slot[v]);
+    const int want = (mn / nw) & 3;
+    int lead = 0;
+    for (int v = nw - 1; v >= 0; --v)
+      if ((slot[v] & 3) == want) lead = v;
+    track_rot = (kTrackThreads - 32 * lead) & (kTrackThreads - 1);
+  }
+  __syncthreads();
+}
+
 // Homotopy systems, flat (see include/phc_b200.h, phc_track):
 struct TrackDev {
   int nsys, maxvar, maxdim;
@@ -90,21 +124,26 @@ __device__ __forceinline__ typename N::T cnum(double re, double im) {
 
 // Evaluate the homotopy of system s at the series x (n series of degree w,
 // leading dimension xld numbers per variable) and t = t0 + s:
-//   h[i*(w+1)+k]        value series of equation i,
-//   J[(k*n + i)*n + j]  Jacobian series (when J != nullptr).
+//   h[i*(w+1)+k]        value series of equation i, in precision N,
+//   J[(k*n + i)*n + j]  Jacobian series (when J != nullptr), in precision
+//                       JN (N, or double for a Newton step whose linear
+//                       solve runs in double).
 // V, G: shared staging for the distinct monomials, nm*(w+1) and
 // nm*maxvar*(w+1) numbers; G is written only when S.gstaged and J is wanted
 // (monomials of total degree <= 2 stage no partials).
 // Phase 1: one thread per distinct monomial computes its value and its
 // partials (exponent included) by the common-factor method and products of
-// the distinct variables.  Phase 2: one thread per output coefficient
-// gathers the coefficient series (a + b t0) + b s times the monomial series
-// over the terms of its equation (value) or over the Jacobian gather list
-// of its (equation, variable) pair.
-template <class N>
+// the distinct variables.  Phase 2: the coefficient series (a + b t0) + b s
+// times the monomial series, summed over the terms of an equation (one warp
+// per equation, lanes over the terms, shuffle reductions) or over the
+// Jacobian gather list of an (equation, variable) pair (one thread per
+// pair); KC coefficients at a time, so that each term's data is loaded once
+// per KC coefficients.
+template <class N, int KC = 1, class JN = N>
 __device__ void hom_eval_cta(const TrackDev &S, int s, int w, double t0, const double *x, int xld, double *V,
                              double *G, double *h, double *J) {
   typedef typename N::T T;
+  typedef typename JN::T JT;
   const int W = N::width;
   const int n = S.dim[s];
   const int n1 = w + 1;
@@ -112,7 +151,7 @@ __device__ void hom_eval_cta(const TrackDev &S, int s, int w, double t0, const d
   const int nm = S.mono_off[s + 1] - m0;
   const int mv = S.maxvar;
   const bool stage = S.gstaged && J != nullptr;
-  for (int m = threadIdx.x; m < nm; m += blockDim.x) {
+  for (int m = ctid(); m < nm; m += blockDim.x) {
     const int gm = m0 + m;
     const int k = S.mono_nvr[gm];
     const int *ix = S.mono_idx + (long)gm * mv;
@@ -184,62 +223,79 @@ __device__ void hom_eval_cta(const TrackDev &S, int s, int w, double t0, const d
   }
   __syncthreads();
   const int e0 = S.eq_off[s];
-  const int nval = n * n1;
-  const int njac = J ? n * n * n1 : 0;
-  // values: one warp per (equation, coefficient), lanes over the equation's
-  // terms, a shuffle reduction (an equation has up to O(n^2) terms, so one
-  // thread per value would serialise the evaluation)
-  {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (int it = warp; it < nval; it += nw) {
-      const int i = it / n1, kk = it % n1;
-      T acc = N::zero();
-      for (int tr = S.term_off[e0 + i] + lane; tr < S.term_off[e0 + i + 1]; tr += 32) {
+  const int lane = ctid() & 31, warp = ctid() >> 5, nw = blockDim.x >> 5;
+  for (int i = warp; i < n; i += nw) {
+    const int tb = S.term_off[e0 + i], te = S.term_off[e0 + i + 1];
+    for (int k0 = 0; k0 < n1; k0 += KC) {
+      T acc[KC];
+#pragma unroll
+      for (int r = 0; r < KC; ++r) acc[r] = N::zero();
+      for (int tr = tb + lane; tr < te; tr += 32) {
         const T a = cnum<N>(S.term_a[2 * tr], S.term_a[2 * tr + 1]);
         const T b = cnum<N>(S.term_b[2 * tr], S.term_b[2 * tr + 1]);
         const T c0 = N::add(a, N::scale_d(b, t0));
         const double *Vm = V + (long)(S.term_mono[tr] - m0) * n1 * W;
-        acc = N::add(acc, N::mul(c0, ldn_at<N>(Vm, kk)));
-        if (kk > 0) acc = N::add(acc, N::mul(b, ldn_at<N>(Vm, kk - 1)));
-      }
-      acc = warp_sum<N>(acc);
-      if (lane == 0) stn_at<N>(h, (long)i * n1 + kk, acc);
-    }
-  }
-  for (int it = threadIdx.x; it < njac; it += blockDim.x) {
-    T acc = N::zero();
-    {
-      const int r = it;
-      const int kk = r / (n * n), i = (r / n) % n, j = r % n;
-      const int g = (e0 + i) * S.maxdim + j;
-      for (int q = S.jg_off[g]; q < S.jg_off[g + 1]; ++q) {
-        const int tr = S.jg_term[q];
-        const T a = cnum<N>(S.term_a[2 * tr], S.term_a[2 * tr + 1]);
-        const T b = cnum<N>(S.term_b[2 * tr], S.term_b[2 * tr + 1]);
-        const T c0 = N::add(a, N::scale_d(b, t0));
-        const int sl = S.jg_slot[q];
-        T g0, g1 = N::zero();  // the partial's coefficients kk and kk-1
-        if (sl >= 0) {
-          const double *Gm = G + ((long)(S.term_mono[tr] - m0) * mv + sl) * n1 * W;
-          g0 = ldn_at<N>(Gm, kk);
-          if (kk > 0) g1 = ldn_at<N>(Gm, kk - 1);
-        } else if (sl == -1) {
-          g0 = (kk == 0) ? N::one() : N::zero();
-          g1 = (kk == 1) ? N::one() : N::zero();
-        } else {
-          const int l = (sl == -2) ? j : -sl - 3;
-          const double *xl = x + (long)l * xld * W;
-          g0 = ldn_at<N>(xl, kk);
-          if (kk > 0) g1 = ldn_at<N>(xl, kk - 1);
-          if (sl == -2) {
-            g0 = N::add(g0, g0);
-            g1 = N::add(g1, g1);
+        T prev = k0 > 0 ? ldn_at<N>(Vm, k0 - 1) : N::zero();
+#pragma unroll
+        for (int r = 0; r < KC; ++r) {
+          const int kk = k0 + r;
+          if (kk < n1) {
+            const T v = ldn_at<N>(Vm, kk);
+            acc[r] = N::add(acc[r], N::mul(c0, v));
+            if (kk > 0) acc[r] = N::add(acc[r], N::mul(b, prev));
+            prev = v;
           }
         }
-        acc = N::add(acc, N::mul(c0, g0));
-        if (kk > 0) acc = N::add(acc, N::mul(b, g1));
       }
-      stn_at<N>(J, ((long)kk * n + i) * n + j, acc);
+#pragma unroll
+      for (int r = 0; r < KC; ++r)
+        if (k0 + r < n1) {
+          const T sum = warp_sum<N>(acc[r]);
+          if (lane == 0) stn_at<N>(h, (long)i * n1 + k0 + r, sum);
+        }
+    }
+  }
+  if (J != nullptr) {
+    for (int it = ctid(); it < n * n; it += blockDim.x) {
+      const int i = it / n, j = it % n;
+      const int g = (e0 + i) * S.maxdim + j;
+      const int qb = S.jg_off[g], qe = S.jg_off[g + 1];
+      for (int k0 = 0; k0 < n1; k0 += KC) {
+        JT acc[KC];
+#pragma unroll
+        for (int r = 0; r < KC; ++r) acc[r] = JN::zero();
+        for (int q = qb; q < qe; ++q) {
+          const int tr = S.jg_term[q];
+          const int sl = S.jg_slot[q];
+          const JT a = cnum<JN>(S.term_a[2 * tr], S.term_a[2 * tr + 1]);
+          const JT b = cnum<JN>(S.term_b[2 * tr], S.term_b[2 * tr + 1]);
+          const JT c0 = JN::add(a, JN::scale_d(b, t0));
+          // the partial's series: staged (sl >= 0), the constant 1 (-1),
+          // 2 x_j (-2) or x_l (-3-l)
+          const double *gp = nullptr;
+          if (sl >= 0) gp = G + ((long)(S.term_mono[tr] - m0) * mv + sl) * n1 * W;
+          else if (sl <= -2) gp = x + (long)((sl == -2) ? j : -sl - 3) * xld * W;
+          auto gload = [&](int kk) -> JT {
+            if (gp == nullptr) return kk == 0 ? JN::one() : JN::zero();
+            const JT v = conv_num<N, JN>::go(ldn_at<N>(gp, kk));
+            return sl == -2 ? JN::add(v, v) : v;
+          };
+          JT prev = k0 > 0 ? gload(k0 - 1) : JN::zero();
+#pragma unroll
+          for (int r = 0; r < KC; ++r) {
+            const int kk = k0 + r;
+            if (kk < n1) {
+              const JT v = gload(kk);
+              acc[r] = JN::add(acc[r], JN::mul(c0, v));
+              if (kk > 0) acc[r] = JN::add(acc[r], JN::mul(b, prev));
+              prev = v;
+            }
+          }
+        }
+#pragma unroll
+        for (int r = 0; r < KC; ++r)
+          if (k0 + r < n1) stn_at<JN>(J, ((long)(k0 + r) * n + i) * n + j, acc[r]);
+      }
     }
   }
   __syncthreads();
@@ -260,10 +316,10 @@ __device__ void hom_eval_cta(const TrackDev &S, int s, int w, double t0, const d
 template <class N>
 __device__ int cta_lufac(int n, double *A, int *ipvt, double *dinv, int *sh) {
   typedef typename N::T T;
-  const int lane = threadIdx.x & 31;
+  const int lane = ctid() & 31;
   int info = 0;  // meaningful in warp 0
   for (int k = 0; k < n; ++k) {
-    if (threadIdx.x < 32) {
+    if (ctid() < 32) {
       const int i = k + lane;
       double v = -1.0;
       if (i < n) {
@@ -298,7 +354,7 @@ __device__ int cta_lufac(int n, double *A, int *ipvt, double *dinv, int *sh) {
     }
     __syncthreads();
     const int m = n - k - 1;
-    for (int e = threadIdx.x; e < m * m; e += blockDim.x) {
+    for (int e = ctid(); e < m * m; e += blockDim.x) {
       const int i = k + 1 + e / m, j = k + 1 + e % m;
       const long o = (long)i * n + j;
       stn_at<N>(A, o, N::add(ldn_at<N>(A, o), N::mul(ldn_at<N>(A, (long)k * n + j), ldn_at<N>(A, (long)i * n + k))));
@@ -312,18 +368,13 @@ __device__ int cta_lufac(int n, double *A, int *ipvt, double *dinv, int *sh) {
 // standard_complex_linear_solvers.adb:552-583 (row interchanges applied in
 // order with the multipliers, then back substitution), except that the back
 // substitution multiplies by dinv[k] = 1 / u_kk where lusolve divides.
-// Called by warp 0 alone, lane i holding b_i (n <= 32); returns x_i in
-// lane i (zero in lanes >= n).  negate: solve with -b.
+// Called by one warp alone, lane i passing b_i (n <= 32, lanes >= n pass
+// zero); returns x_i in lane i.
 template <class N>
-__device__ typename N::T warp_lusolve(int n, const double *A, const int *ipvt, const double *dinv, const double *b,
-                                      bool negate) {
+__device__ typename N::T warp_lusolve(int n, const double *A, const int *ipvt, const double *dinv,
+                                      typename N::T v) {
   typedef typename N::T T;
   const int lane = threadIdx.x & 31;
-  T v = N::zero();
-  if (lane < n) {
-    v = ldn_at<N>(b, lane);
-    if (negate) v = N::neg(v);
-  }
   for (int k = 0; k < n - 1; ++k) {  // L y = P b
     const int ell = ipvt[k];
     const T t = md::shfl(v, ell);
@@ -346,7 +397,7 @@ __device__ typename N::T warp_lusolve(int n, const double *A, const int *ipvt, c
 template <class N>
 __device__ void cta_luinverse(int n, const double *A, const int *ipvt, const double *dinv, double *M) {
   typedef typename N::T T;
-  for (int c = threadIdx.x; c < n; c += blockDim.x) {
+  for (int c = ctid(); c < n; c += blockDim.x) {
     for (int i = 0; i < n; ++i) stn_at<N>(M, (long)i * n + c, i == c ? N::one() : N::zero());
     for (int k = 0; k < n - 1; ++k) {
       const int ell = ipvt[k];
@@ -376,7 +427,7 @@ __device__ void cta_luinverse(int n, const double *A, const int *ipvt, const dou
 template <class N>
 __device__ void cta_matvec(int n, const double *M, const double *b, double *y) {
   typedef typename N::T T;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+  for (int i = ctid(); i < n; i += blockDim.x) {
     T acc = N::zero();
     for (int j = 0; j < n; ++j) acc = N::add(acc, N::mul(ldn_at<N>(M, (long)i * n + j), ldn_at<N>(b, j)));
     stn_at<N>(y, i, acc);

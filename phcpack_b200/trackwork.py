@@ -37,12 +37,16 @@ def track_flops(pb: hm.TrackProblem, steps, rejected, pmode=1):
     multiplications + 2 additions, accumulation 2 additions):
       series Newton (4 steps at working degrees 1, 3, 7, 8): per step one
         evaluation (a series product per distinct monomial, the coefficient
-        gathers), the QR of J_0 with explicit Q, R^{-1} and R^{-1} Q^H
-        (about 4 n^3), the block-Toeplitz solve ((w+1)(w+2)/2 n^2);
-      predictor feedback: one point evaluation;
-      corrector: 2 double-double Newton iterations (point evaluation, 4 n^3);
+        gathers of the values and of the Jacobian), the block-Toeplitz
+        right-hand sides ((w+1)(w+2)/2 n^2) and the products with J_0^{-1}
+        ((w+1) n^2); once per predictor step the LU of J_0 (n^3/3) and the
+        inverse (2 n^3/3); all in the predictor's precision;
+      predictor feedback: one point evaluation of the values;
+      corrector: 2 Newton iterations, each a point evaluation of the values
+        in double-double and of the Jacobian, its LU (n^3/3) and solve (n^2)
+        in the predictor's precision;
       a rejected step costs one feedback and one corrector.
-    Returns (flops, the cost weights used)."""
+    Returns the total."""
     n = pb.maxdim
     nmono = pb.nmono_max
     nterm = int(np.diff(pb.term_off).mean())
@@ -51,16 +55,18 @@ def track_flops(pb: hm.TrackProblem, steps, rejected, pmode=1):
     def cma(prec):  # flops of one complex multiply-add in precision prec
         return 4 * MD_MUL[prec] + 4 * MD_ADD[prec]
 
-    def series_eval(w):
+    def evals(w):  # (values, Jacobian) complex multiply-adds at degree w
         conv = (w + 1) * (w + 2) // 2
-        return nmono * conv + 2 * (n * (w + 1) * nterm + n * (w + 1) * njg)
+        return nmono * conv + 2 * n * (w + 1) * nterm, 2 * n * (w + 1) * njg
 
     def newton_step(w):
-        return series_eval(w) + 4 * n ** 3 + (w + 1) * (w + 2) // 2 * n * n
+        v, j = evals(w)
+        return v + j + (w + 1) * (w + 2) // 2 * n * n + (w + 1) * n * n
 
-    pred = sum(newton_step(w) for w in (1, 3, 7, 8)) * cma(pmode)
-    feed = series_eval(0) * cma(pmode)
-    corr = 2 * (series_eval(0) + 4 * n ** 3 + n * n) * cma(2)
+    pred = (sum(newton_step(w) for w in (1, 3, 7, 8)) + n ** 3) * cma(pmode)
+    v0, j0 = evals(0)
+    feed = v0 * cma(pmode)
+    corr = 2 * (v0 * cma(2) + (j0 + n ** 3 / 3 + n * n) * cma(pmode))
     steps = np.asarray(steps, dtype=np.float64)
     rej = np.asarray(rejected, dtype=np.float64)
     total = float((steps * (pred + feed + corr) + rej * (feed + corr)).sum())
