@@ -156,8 +156,10 @@ int phc_newton_host(int prec, int cplx, int nsys, int dim, int deg, int szt, int
 
 /* ------------------------------------------------------------------ Track
  * Batched series-Pade path tracking of homotopies
- *   h(x, t) = sum over terms (a + b t) x^e,  t from 0 to 1,
- * which covers (1 - t) gamma q(x) + t p(x) (a = gamma c_q, b = c_p - gamma c_q).
+ *   h(x, t) = sum over terms ((1 - t) a + t b) x^e,  t from 0 to 1,
+ * which is (1 - t) gamma q(x) + t p(x) with a = gamma c_q, b = c_p (the
+ * form of Path/Path_GPU/eval_coef.cu:27-28; at t = 1 the target's
+ * coefficients are used exactly).
  * Replaces the tracker behind the Ada/phcpy C interface:
  * Ada/PHCtoC/gpumanypaths_dd.h:27 gpumanypaths_dd (and _d, _qd), whose
  * internal GPU_Path_mult (Path/Path_GPU/path_gpu.h:38) tracks many paths and
@@ -169,7 +171,7 @@ int phc_newton_host(int prec, int cplx, int nsys, int dim, int deg, int szt, int
  *   mono_nvr[m] (0 = the constant 1) distinct variables mono_idx[m*maxvar+v]
  *   with exponents mono_exp[m*maxvar+v];
  *   equations eq_off[s] .. eq_off[s+1]-1 (dim[s] of them), equation e has
- *   terms term_off[e] .. term_off[e+1]-1, term r is (a + b t) times monomial
+ *   terms term_off[e] .. term_off[e+1]-1, term r is ((1 - t) a + t b) times monomial
  *   term_mono[r] (global id), a = term_a[2r] + i term_a[2r+1], b likewise.
  * Jacobian gather lists (from phc_track_prepare): for (equation e, variable
  *   j) the entries jg_off[e*maxdim+j] .. jg_off[e*maxdim+j+1]-1 of jg_term,

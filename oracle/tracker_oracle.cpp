@@ -32,8 +32,9 @@
 //    step and re-evaluate the Pade approximant (fail below minsize);
 //  * stop when |1 - t| < epsilon; refine the endpoint at t = 1 and classify
 //    success when the max-norm residual is at most restol.
-// The homotopy is h(x, t) = sum_terms (a + b t) x^e, which covers
-// (1 - t) gamma q(x) + t p(x) with a = gamma c_q, b = c_p - gamma c_q.
+// The homotopy is h(x, t) = sum_terms ((1 - t) a + t b) x^e, which is
+// (1 - t) gamma q(x) + t p(x) with a = gamma c_q, b = c_p
+// (Path/Path_GPU/eval_coef.cu:27-28).
 #include <vector>
 #include <thread>
 #include <atomic>
@@ -71,7 +72,8 @@ template <class R> static cx<R> cplx(double re, double im) { return cx<R>(R(re),
 // jac[k][i][j].  Per distinct monomial: common factor, then products of the
 // distinct variables (the reference's common-factor + Speelpenning method
 // restated for a monomial without coefficient); per term the coefficient
-// series (a + b t0) + b s multiplies the monomial and its partials.
+// series c0 + c1 s, c1 = b - a, c0 = a + t0 c1, multiplies the monomial and
+// its partials.
 template <class T>
 static void hom_eval(const TrackSys &S, int s, int w, double t0, const std::vector<std::vector<T> > &x,
                      std::vector<std::vector<T> > &h, std::vector<T> *jac) {
@@ -121,7 +123,7 @@ static void hom_eval(const TrackSys &S, int s, int w, double t0, const std::vect
     for (int tr = S.term_off[eq]; tr < S.term_off[eq + 1]; ++tr) {
       const int m = S.term_mono[tr] - m0;
       const T a = cplx<R>(S.term_a[2 * tr], S.term_a[2 * tr + 1]);
-      const T b = cplx<R>(S.term_b[2 * tr], S.term_b[2 * tr + 1]);
+      const T b = cplx<R>(S.term_b[2 * tr], S.term_b[2 * tr + 1]) - a;  // d/dt
       const T c0 = a + b * T(R(t0));
       for (int kk = 0; kk < n1; ++kk) {
         T v = c0 * V[m][kk];
@@ -156,8 +158,8 @@ static void hom_abs_eval(const TrackSys &S, int s, double t, const std::vector<d
   for (int i = 0; i < n; ++i)
     for (int tr = S.term_off[e0 + i]; tr < S.term_off[e0 + i + 1]; ++tr) {
       const int gm = S.term_mono[tr];
-      const double cr = S.term_a[2 * tr] + S.term_b[2 * tr] * t;
-      const double ci = S.term_a[2 * tr + 1] + S.term_b[2 * tr + 1] * t;
+      const double cr = std::fma(S.term_b[2 * tr] - S.term_a[2 * tr], t, S.term_a[2 * tr]);
+      const double ci = std::fma(S.term_b[2 * tr + 1] - S.term_a[2 * tr + 1], t, S.term_a[2 * tr + 1]);
       double v = std::hypot(cr, ci);
       for (int u = 0; u < S.mono_nvr[gm]; ++u)
         v *= std::pow(ax[S.mono_idx[(long)gm * S.maxvar + u]], S.mono_exp[(long)gm * S.maxvar + u]);

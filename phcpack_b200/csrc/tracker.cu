@@ -234,8 +234,9 @@ __device__ double pade_mixres(const TrackDev &S, int s, int n, int K, int dendeg
     const int eq = S.eq_off[s] + i;
     for (int tr = S.term_off[eq] + lane; tr < S.term_off[eq + 1]; tr += 32) {
       const int gm = S.term_mono[tr];
-      double v = hypot(fma(S.term_b[2 * tr], t + st, S.term_a[2 * tr]),
-                       fma(S.term_b[2 * tr + 1], t + st, S.term_a[2 * tr + 1]));
+      // |(1 - t') a + t' b| at t' = t + st
+      double v = hypot(fma(S.term_b[2 * tr] - S.term_a[2 * tr], t + st, S.term_a[2 * tr]),
+                       fma(S.term_b[2 * tr + 1] - S.term_a[2 * tr + 1], t + st, S.term_a[2 * tr + 1]));
       for (int u = 0; u < S.mono_nvr[gm]; ++u) {
         const double xa = PN::mag(ldn_at<PN>(xp, S.mono_idx[(long)gm * S.maxvar + u]));
         for (int e = 0; e < S.mono_exp[(long)gm * S.maxvar + u]; ++e) v *= xa;

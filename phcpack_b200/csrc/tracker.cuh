@@ -1,5 +1,5 @@
 // tracker.cuh -- CTA-level building blocks of the path tracker: evaluation
-// of a homotopy h(x, t) = sum_terms (a + b t) x^e and its Jacobian at a
+// of a homotopy h(x, t) = sum_terms ((1 - t) a + t b) x^e and its Jacobian at a
 // vector of power series in s = t - t0, the small dense solves, the Pade
 // approximants and the conversions between precisions.
 #pragma once
@@ -133,7 +133,8 @@ __device__ __forceinline__ typename N::T cnum(double re, double im) {
 // (monomials of total degree <= 2 stage no partials).
 // Phase 1: one thread per distinct monomial computes its value and its
 // partials (exponent included) by the common-factor method and products of
-// the distinct variables.  Phase 2: the coefficient series (a + b t0) + b s
+// the distinct variables.  Phase 2: the coefficient series c0 + c1 s, with
+// c1 = b - a and c0 = a + t0 c1 (exactly b at t0 = 1 in double-double),
 // times the monomial series, summed over the terms of an equation (one warp
 // per equation, lanes over the terms, shuffle reductions) or over the
 // Jacobian gather list of an (equation, variable) pair (one thread per
@@ -232,7 +233,7 @@ __device__ void hom_eval_cta(const TrackDev &S, int s, int w, double t0, const d
       for (int r = 0; r < KC; ++r) acc[r] = N::zero();
       for (int tr = tb + lane; tr < te; tr += 32) {
         const T a = cnum<N>(S.term_a[2 * tr], S.term_a[2 * tr + 1]);
-        const T b = cnum<N>(S.term_b[2 * tr], S.term_b[2 * tr + 1]);
+        const T b = N::sub(cnum<N>(S.term_b[2 * tr], S.term_b[2 * tr + 1]), a);  // d/dt
         const T c0 = N::add(a, N::scale_d(b, t0));
         const double *Vm = V + (long)(S.term_mono[tr] - m0) * n1 * W;
         T prev = k0 > 0 ? ldn_at<N>(Vm, k0 - 1) : N::zero();
@@ -268,7 +269,7 @@ __device__ void hom_eval_cta(const TrackDev &S, int s, int w, double t0, const d
           const int tr = S.jg_term[q];
           const int sl = S.jg_slot[q];
           const JT a = cnum<JN>(S.term_a[2 * tr], S.term_a[2 * tr + 1]);
-          const JT b = cnum<JN>(S.term_b[2 * tr], S.term_b[2 * tr + 1]);
+          const JT b = JN::sub(cnum<JN>(S.term_b[2 * tr], S.term_b[2 * tr + 1]), a);  // d/dt
           const JT c0 = JN::add(a, JN::scale_d(b, t0));
           // the partial's series: staged (sl >= 0), the constant 1 (-1),
           // 2 x_j (-2) or x_l (-3-l)

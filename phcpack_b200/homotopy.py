@@ -116,19 +116,23 @@ class TrackProblem:
         return int(np.diff(self.mono_off).max())
 
 
-def total_degree_problem(targets, gamma, max_paths_per_system=None, rng=None, maxvar=2) -> TrackProblem:
-    """Total-degree homotopies for a list of target systems.  Start
-    solutions are all products of roots of unity; when a system has more
-    than max_paths_per_system of them, a seeded uniform sample (without
-    replacement, rng) of that many is kept."""
+def homotopy_problem(pairs, gamma, starts, maxvar=None) -> TrackProblem:
+    """Flatten homotopies h = (1 - t) gamma q + t p for a list of (p, q)
+    pairs (target and start systems, polynomials as lists of (monomial,
+    coefficient), a monomial a tuple of (variable, exponent)) with start
+    points starts = [(system index, complex vector), ...].  maxvar: the most
+    distinct variables in a monomial (None: from the systems)."""
+    if maxvar is None:
+        maxvar = max(1, max(len(m) for p, q in pairs for poly in list(p) + list(q) for m, _ in poly))
     dim, mono_off, nvr, idx, exps = [], [0], [], [], []
     eq_off, term_off, term_mono, ta, tb = [0], [0], [], [], []
-    path_sys, x0 = [], []
-    maxdim = max(len(p) for p in targets)
-    for s, polys in enumerate(targets):
+    maxdim = max(len(p) for p, _ in pairs)
+    for s, (polys, qpolys) in enumerate(pairs):
         n = len(polys)
-        degs = [degree(p) for p in polys]
-        # distinct monomials of the system: target monomials, x_i^{d_i}, 1
+        if len(qpolys) != n:
+            raise ValueError(f"system {s}: {n} target and {len(qpolys)} start polynomials")
+        # distinct monomials of the system: the constant, then target and
+        # start monomials in order of appearance
         table = {}
 
         def mono_id(m):
@@ -137,54 +141,85 @@ def total_degree_problem(targets, gamma, max_paths_per_system=None, rng=None, ma
             return table[m]
 
         mono_id(())
-        for p in polys:
+        for p in list(polys) + list(qpolys):
             for m, _ in p:
                 mono_id(m)
-        for i in range(n):
-            mono_id(((i, degs[i]),))
         base = mono_off[-1]
         for m, k in sorted(table.items(), key=lambda kv: kv[1]):
-            nvr.append(len(m))
-            row_i = [v for v, _ in m] + [0] * (maxvar - len(m))
-            row_e = [e for _, e in m] + [0] * (maxvar - len(m))
             if len(m) > maxvar:
                 raise ValueError("monomial with more than maxvar variables")
-            idx.append(row_i)
-            exps.append(row_e)
+            nvr.append(len(m))
+            idx.append([v for v, _ in m] + [0] * (maxvar - len(m)))
+            exps.append([e for _, e in m] + [0] * (maxvar - len(m)))
         mono_off.append(base + len(table))
-        for i, p in enumerate(polys):
-            cp = {}
-            for m, c in p:
+        for i in range(n):
+            cp, cq = {}, {}
+            for m, c in polys[i]:
                 cp[m] = cp.get(m, 0) + c
-            cq = {((i, degs[i]),): 1.0, (): -1.0}
+            for m, c in qpolys[i]:
+                cq[m] = cq.get(m, 0) + c
             for m in sorted(set(cp) | set(cq), key=lambda mm: table[mm]):
                 a = gamma * cq.get(m, 0.0)
-                b = cp.get(m, 0.0) - a
+                b = complex(cp.get(m, 0.0))
                 term_mono.append(base + table[m])
                 ta.append([a.real, a.imag])
                 tb.append([b.real, b.imag])
             term_off.append(len(term_mono))
         eq_off.append(eq_off[-1] + n)
         dim.append(n)
-        total = int(np.prod(degs))
-        roots = [np.exp(2j * np.pi * np.arange(d) / d) for d in degs]
-        if max_paths_per_system is not None and total > max_paths_per_system:
-            pick = np.sort(rng.choice(total, size=max_paths_per_system, replace=False))
-        else:
-            pick = np.arange(total)
-        for flat in pick:
-            rem = int(flat)
-            pt = np.zeros(maxdim, complex)
-            for i in range(n):
-                pt[i] = roots[i][rem % degs[i]]
-                rem //= degs[i]
-            path_sys.append(s)
-            x0.append(np.stack([pt.real, pt.imag], axis=-1).reshape(-1))
+    path_sys, x0 = [], []
+    for s, pt in starts:
+        v = np.zeros(maxdim, complex)
+        v[:len(pt)] = pt
+        path_sys.append(s)
+        x0.append(np.stack([v.real, v.imag], axis=-1).reshape(-1))
     i32 = lambda a: np.ascontiguousarray(np.asarray(a, dtype=np.int32))
     f64 = lambda a: np.ascontiguousarray(np.asarray(a, dtype=np.float64).reshape(-1))
-    return TrackProblem(len(targets), maxvar, i32(dim), i32(mono_off), i32(nvr), i32(idx).reshape(-1),
+    return TrackProblem(len(pairs), maxvar, i32(dim), i32(mono_off), i32(nvr), i32(idx).reshape(-1),
                         i32(exps).reshape(-1), i32(eq_off), i32(term_off), i32(term_mono), f64(ta), f64(tb),
                         i32(path_sys), f64(x0))
+
+
+def total_degree_start(polys):
+    """The total-degree start system q_i = x_i^{d_i} - 1 of a target system
+    (Root_Counts/Product/total_degree_start_systems.adb:108-160) and its
+    degrees."""
+    degs = [degree(p) for p in polys]
+    return [[(((i, d),), 1.0), ((), -1.0)] for i, d in enumerate(degs)], degs
+
+
+def total_degree_solutions(degs, pick=None):
+    """All products of roots of unity (the start solutions of
+    x_i^{d_i} - 1), or those with the flat indices in pick (the index runs
+    fastest over the first variable)."""
+    roots = [np.exp(2j * np.pi * np.arange(d) / d) for d in degs]
+    total = int(np.prod(degs))
+    out = []
+    for flat in (range(total) if pick is None else pick):
+        rem = int(flat)
+        pt = np.zeros(len(degs), complex)
+        for i, d in enumerate(degs):
+            pt[i] = roots[i][rem % d]
+            rem //= d
+        out.append(pt)
+    return out
+
+
+def total_degree_problem(targets, gamma, max_paths_per_system=None, rng=None, maxvar=2) -> TrackProblem:
+    """Total-degree homotopies for a list of target systems.  Start
+    solutions are all products of roots of unity; when a system has more
+    than max_paths_per_system of them, a seeded uniform sample (without
+    replacement, rng) of that many is kept."""
+    pairs, starts = [], []
+    for s, polys in enumerate(targets):
+        q, degs = total_degree_start(polys)
+        pairs.append((polys, q))
+        total = int(np.prod(degs))
+        pick = None
+        if max_paths_per_system is not None and total > max_paths_per_system:
+            pick = np.sort(rng.choice(total, size=max_paths_per_system, replace=False))
+        starts.extend((s, pt) for pt in total_degree_solutions(degs, pick))
+    return homotopy_problem(pairs, gamma, starts, maxvar=maxvar)
 
 
 def config4(seed=4):

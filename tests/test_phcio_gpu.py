@@ -1,0 +1,74 @@
+"""Text-in/text-out tracking (phcpack_b200.phcio.manypaths, the counterpart of
+gpumanypaths_dd / _qd) on the GPU."""
+from decimal import Decimal, getcontext
+from fractions import Fraction
+
+import numpy as np
+import pytest
+
+from phcpack_b200 import homotopy as hm
+from phcpack_b200 import phcio
+
+pytestmark = pytest.mark.gpu
+
+
+def _inv_sqrt2(digits=80):
+    getcontext().prec = digits
+    return Fraction(Decimal(1) / Decimal(2).sqrt())
+
+
+@pytest.mark.parametrize("rmode,tol", [(2, 1e-30), (4, 1e-60)])
+def test_circle_and_line_dd_qd(rmode, tol):
+    text, r = phcio.manypaths("2\n x^2 + y^2 - 1;\n x - y;\n", rmode=rmode, restol=1e-24 if rmode == 2 else 1e-48)
+    assert (r.status == 0).all()
+    sols = phcio.parse_solutions(text, symbols=["x", "y"], nlimbs=rmode)
+    assert len(sols) == 2
+    c = _inv_sqrt2()
+    signs = sorted(np.sign(s["x"][0, 0, 0]) for s in sols)
+    assert signs == [-1.0, 1.0]
+    for s in sols:
+        sg = 1 if s["x"][0, 0, 0] > 0 else -1
+        for j in range(2):
+            re_ = phcio.limbs_to_fraction(s["x"][j, 0])
+            im_ = phcio.limbs_to_fraction(s["x"][j, 1])
+            assert abs(re_ - sg * c) <= tol and abs(im_) <= tol
+        assert s["t"] == 1.0 and s["res"] <= (1e-24 if rmode == 2 else 1e-48)
+
+
+def cyclic_text(n):
+    x = [f"x{i + 1}" for i in range(n)]
+    rows = [" + ".join("*".join(x[(i + j) % n] for j in range(k)) for i in range(n)) + ";" for k in range(1, n)]
+    return f"{n}\n" + "\n".join(rows) + "\n" + "*".join(x) + " - 1;\n"
+
+
+def test_cyclic5_endpoints():
+    """cyclic 5-roots: 120 total-degree paths, 70 isolated regular roots;
+    the other paths diverge.  Every path classified as success ends at a
+    root (residual <= 1e-24 in double-double) and the roots found are
+    distinct solutions of the system."""
+    text, r = phcio.manypaths(cyclic_text(5), seed=2, maxsteps=2000)
+    polys, sym = phcio.parse_system(cyclic_text(5))
+    sols = phcio.parse_solutions(text, symbols=sym)
+    assert len(sols) == 120
+    ok = np.flatnonzero(r.status == 0)
+    assert len(ok) >= 60
+    pts = np.array([sols[p]["x"] for p in ok])
+    for p in ok:
+        assert sols[p]["res"] <= 1e-24
+    # distinct roots among the successes
+    d = np.abs(pts[:, None, :] - pts[None, :, :]).max(axis=2) + np.eye(len(ok))
+    assert (d > 1e-6).all()
+
+
+def test_given_start_system_and_solutions_match_total_degree():
+    target = "3\n x^2 + y*z - 1;\n y^2 + x - 2*i;\n z^2 + x*y - 3;\n"
+    polys, sym = phcio.parse_system(target)
+    q, degs = hm.total_degree_start(polys)
+    start = phcio.write_system(q, sym)
+    sols = [dict(t=0.0, m=1, x=x, err=0.0, rco=1.0, res=0.0) for x in hm.total_degree_solutions(degs)]
+    start_sols = phcio.write_solutions(sols, sym, digits=17)
+    g = complex(hm.unit(np.random.default_rng(0)))
+    t1, r1 = phcio.manypaths(target, gamma=g)
+    t2, r2 = phcio.manypaths(target, start, start_sols, gamma=g)
+    assert np.array_equal(r1.status, r2.status)
+    assert np.abs(r1.endpoints(3) - r2.endpoints(3)).max() <= 1e-28

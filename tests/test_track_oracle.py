@@ -19,7 +19,7 @@ def target_residual(pb, xend, p):
         v = 0j
         for tr in range(pb.term_off[e], pb.term_off[e + 1]):
             m = pb.term_mono[tr]
-            c = complex(*pb.term_a[2 * tr:2 * tr + 2]) + complex(*pb.term_b[2 * tr:2 * tr + 2])
+            c = complex(*pb.term_b[2 * tr:2 * tr + 2])  # the coefficient at t = 1
             for u in range(pb.mono_nvr[m]):
                 c *= x[pb.mono_idx[m * pb.maxvar + u]] ** pb.mono_exp[m * pb.maxvar + u]
             v += c
