@@ -183,8 +183,10 @@ int phc_newton_host(int prec, int cplx, int nsys, int dim, int deg, int szt, int
  *   (0 drops the staging buffer from shared memory).
  * Paths: path p belongs to system path_sys[p] and starts at x0 (maxdim complex
  *   doubles per path).
- * ipar: deg (series degree K), numdeg (L), dendeg (M), nit (series Newton
- *   steps), corsteps, maxsteps, refine_steps.
+ * ipar: deg (series degree K), numdeg (L), dendeg (M), nit (>= 1; the
+ *   reference's number of Newton steps on the series, unused: the Taylor
+ *   coefficients are computed one degree at a time, the fixed point those
+ *   steps approach), corsteps, maxsteps, refine_steps.
  * dpar: pbeta, alpha, maxsize, minsize, tolres, epsilon, restol (endpoint
  *   residual bound), learn_scale (multiplies learned proposals; 0 = 1).
  * pmode: 1 (double) or 2 (double-double), the precision of the predictor

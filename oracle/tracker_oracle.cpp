@@ -14,11 +14,11 @@
 //   Curves/homotopy_continuation_parameters.adb:6-24 defaults
 // restated here on top of this oracle's multiple-double arithmetic.  What is
 // restated and what is left out:
-//  * predictor: Newton on power series in s = t - t0 to degree K (working
-//    degree doubling 1, 3, 7, ... K), each step a block-Toeplitz solve with
-//    the LU of J_0 (factored once per step and reused, as LU_Prediction
-//    does; applied as the explicit inverse); [L/M] Pade approximant per
-//    component; pole step
+//  * predictor: the Taylor series of the path in s = t - t0 to degree K,
+//    x_k = -J_0^{-1} [h(x_0 + ... + x_{k-1} s^{k-1})]_k one degree at a
+//    time (the fixed point of LU_Prediction's Newton on power series, with
+//    J_0 factored once and applied as its inverse); [L/M] Pade approximant
+//    per component; pole step
 //    pbeta * r with r the smallest Fabry radius |c_{K-3}/c_{K-2}| (offset 2
 //    as in Newton_Fabry); step = min(pole step, maxsize), cut at t = 1;
 //  * the Hessian curvature step (Hesse_Pade, singular values of Hessians)
@@ -239,41 +239,37 @@ template <class T> struct lu_solver {
   }
 };
 
-// Newton on power series (the predictor): x[i] series of degree K, on
-// entry the constant terms hold the current point
+// The predictor's Taylor series: x[i] series of degree K, on entry the
+// constant terms hold the current point.  x_k = -J_0^{-1} [h(x truncated
+// below degree k)]_k for k = 1..K, with J_0 factored once by lufac and
+// applied as its inverse; the fixed point of Newton's method on power series
+// (LU_Prediction, Curves/standard_predictor_convolutions.adb:1142-1185)
+// computed one degree at a time, as the GPU tracker does.
 template <class T>
-static void series_newton(const TrackSys &S, int s, const TrackPar &P, double t0, std::vector<std::vector<T> > &x) {
+static void taylor_series(const TrackSys &S, int s, const TrackPar &P, double t0, std::vector<std::vector<T> > &x) {
   const int n = S.dim[s];
   const int K = P.deg;
   std::vector<std::vector<T> > h;
-  std::vector<T> jac, rhs(n), dx((long)(K + 1) * n), M;
+  std::vector<T> jac, M, r(n);
   lu_solver<T> lu;
-  for (int it = 0; it < P.nit; ++it) {
-    int w = (2 << it) - 1;
-    if (w > K) w = K;
-    std::vector<std::vector<T> > xw(n, std::vector<T>(w + 1));
+  {
+    std::vector<std::vector<T> > x0(n, std::vector<T>(1));
+    for (int i = 0; i < n; ++i) x0[i][0] = x[i][0];
+    hom_eval(S, s, 0, t0, x0, h, &jac);
+    lu.factor(n, jac);
+    lu.inverse(M);
+  }
+  for (int k = 1; k <= K; ++k) {
+    std::vector<std::vector<T> > xw(n, std::vector<T>(k + 1));
     for (int i = 0; i < n; ++i)
-      for (int k = 0; k <= w; ++k) xw[i][k] = x[i][k];
-    hom_eval(S, s, w, t0, xw, h, &jac);
-    if (it == 0) {  // J_0 factored once per step (LU_Prediction), M = J_0^{-1}
-      lu.factor(n, jac);
-      lu.inverse(M);
+      for (int j = 0; j < k; ++j) xw[i][j] = x[i][j];
+    hom_eval<T>(S, s, k, t0, xw, h, nullptr);
+    for (int i = 0; i < n; ++i) r[i] = h[i][k];
+    for (int i = 0; i < n; ++i) {
+      T acc = T();
+      for (int j = 0; j < n; ++j) acc = acc + M[(long)i * n + j] * r[j];
+      x[i][k] = -acc;
     }
-    for (int k = 0; k <= w; ++k) {
-      for (int i = 0; i < n; ++i) {
-        T acc = -h[i][k];
-        for (int j = 1; j <= k; ++j)
-          for (int l = 0; l < n; ++l) acc = acc - jac[((long)j * n + i) * n + l] * dx[(long)(k - j) * n + l];
-        rhs[i] = acc;
-      }
-      for (int i = 0; i < n; ++i) {
-        T acc = T();
-        for (int j = 0; j < n; ++j) acc = acc + M[(long)i * n + j] * rhs[j];
-        dx[(long)k * n + i] = acc;
-      }
-    }
-    for (int i = 0; i < n; ++i)
-      for (int k = 0; k <= w; ++k) x[i][k] = x[i][k] + dx[(long)k * n + i];
   }
 }
 
@@ -444,7 +440,7 @@ static PathOut track_path(const TrackSys &S, int s, const TrackPar &P, const dou
       xs[i].assign(K + 1, PT());
       convert(x[i], xs[i][0]);
     }
-    series_newton(S, s, P, t, xs);
+    taylor_series(S, s, P, t, xs);
     double r = 1e300;
     bool rfail = true;
     for (int i = 0; i < n; ++i) {

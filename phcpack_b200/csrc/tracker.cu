@@ -6,9 +6,9 @@
 // Per step (the Ada Predictor_Corrector_Loop, predictor_corrector_loops.adb
 // :37-85, restated):
 //   predictor, in PN precision (double or double-double):
-//     Newton on power series in s = t - t0 to degree K, working degree
-//     1, 3, 7, ..., K, each step a block-Toeplitz solve with the LU of J_0
-//     (factored and J_0^{-1} formed once per predictor step);
+//     the Taylor series of the path in s = t - t0 to degree K, one
+//     coefficient at a time with the LU of J_0 (factored and J_0^{-1}
+//     formed once per predictor step);
 //     [L/M] Pade approximant per component; pole step pbeta * r, r the
 //     smallest Fabry radius |c_{K-3}/c_{K-2}|; step <= maxsize, cut at t = 1;
 //     predictor feedback: halve until the mixed residual < alpha;
@@ -27,11 +27,15 @@
 #include "mlp.cuh"
 #include "../../include/phc_b200.h"
 
+#ifndef TRACK_MINB
+#define TRACK_MINB 8
+#endif
+
 namespace phc {
 
 
 struct TrackLayout {
-  long xs, V, G, hs, J, dx, rhs, R, M, num, den, xp, xc, hc, Jc, Vc, Gc, red, piv, dinv, feat, mag, degs, hbuf, total;
+  long xs, V, G, hs, J0, M, r, num, den, xp, xc, hc, Jc, Vc, Gc, red, piv, dinv, feat, mag, degs, hbuf, total;
 };
 
 __host__ __device__ inline TrackLayout track_layout(int n, int K, int M, int nm, int mv, int Wp, int Wr, int gst) {
@@ -57,16 +61,14 @@ __host__ __device__ inline TrackLayout track_layout(int n, int K, int M, int nm,
   L.mag = take(n * K1);
   L.degs = take(n);
   L.hbuf = take(2 * 128 + 8);
-  // scratch of the series Newton and the predictor feedback ...
+  // scratch of the Taylor series and the predictor feedback ...
   const long ov = o;
-  L.V = take(nm * K1 * Wp);
-  L.G = take(gst ? nm * mv * K1 * Wp : 0);  // only monomials of degree >= 3 stage partials
-  L.hs = take(n * K1 * Wp);
-  L.J = take(K1 * n * n * Wp);
-  L.dx = take(K1 * n * Wp);
-  L.rhs = take(n * Wp);
-  L.R = take(n * n * Wp);
+  L.V = take(nm * 2 * Wp);  // two coefficients per monomial (point evaluations use one)
+  L.G = take(gst ? nm * mv * Wp : 0);  // only monomials of degree >= 3 stage partials
+  L.hs = take(n * Wp);
+  L.J0 = take(n * n * Wp);
   L.M = take(n * n * Wp);
+  L.r = take(n * Wp);
   const long pend = o;
   // ... overlaid by the scratch of the corrector and the refinement, which
   // run after the Pade approximants are formed
@@ -252,8 +254,16 @@ __device__ double pade_mixres(const TrackDev &S, int s, int n, int K, int dendeg
 // Track the paths of one CTA.  PN: predictor numbers, CN: corrector
 // (double-double), RN: refinement.  Output per path: xend (maxdim complex
 // quad-doubles), info (status, steps, rejected), dinfo (t, residual).
+// Resident CTAs per SM asked of the compiler (a register budget): 8 for the
+// precision-split tracker (double predictor, double-double refinement), whose
+// shared memory per path is small enough for 8 paths per SM; 1 otherwise.
+template <class PN, class RN>
+struct track_min_blocks {
+  static const int value = (PN::width <= 2 && RN::width <= 4) ? TRACK_MINB : 1;
+};
+
 template <class PN, class CN, class RN>
-__global__ void __launch_bounds__(kTrackThreads)
+__global__ void __launch_bounds__(kTrackThreads, (track_min_blocks<PN, RN>::value))
     k_track(TrackDev S, TrackParDev P, int npaths, int path_begin, const int *__restrict__ path_sys,
             const double *__restrict__ x0, int *queue, const float *__restrict__ model, double *__restrict__ xend,
             int *__restrict__ info, double *__restrict__ dinfo, float *__restrict__ log, int log_cap,
@@ -299,7 +309,15 @@ __global__ void __launch_bounds__(kTrackThreads)
     int status = 2, nsteps = 0, nrej = 0;
     bool failed = false;
     for (int step_it = 0; step_it < P.maxsteps; ++step_it) {
-      // ---------------- predictor: Newton on power series in PN
+      // ---------------- predictor: the Taylor series of the path in PN
+      // x(s) = x_0 + x_1 s + ... + x_K s^K solves h(x(s), t + s) = 0 to
+      // degree K.  Its coefficients follow one degree at a time from the
+      // LU of J_0 = dh/dx at the point: x_k = -J_0^{-1} [h(x_0 + ... +
+      // x_{k-1} s^{k-1}, t + s)]_k.  This is the fixed point that Newton's
+      // method on power series (LU_Prediction,
+      // Curves/standard_predictor_convolutions.adb:1142-1185, J_0 factored
+      // once by lufac) converges to, computed without the Jacobian series:
+      // K coefficient evaluations and K products with J_0^{-1}.
       double *xs = sm + L.xs;
       for (int t2 = ctid(); t2 < n * (K + 1); t2 += blockDim.x) {
         const int i = t2 / (K + 1), k = t2 % (K + 1);
@@ -308,39 +326,16 @@ __global__ void __launch_bounds__(kTrackThreads)
         stn_at<PN>(xs, t2, v);
       }
       __syncthreads();
-      for (int it = 0; it < P.nit; ++it) {
-        int w = (2 << it) - 1;
-        if (w > K) w = K;
-        // 9 coefficients per pass (the degree-8 series in one) for double
-        // predictors, 5 for double-double (register pressure)
-        hom_eval_cta<PN, (PN::width <= 2 ? 9 : 5)>(S, s, w, t, xs, K + 1, sm + L.V, sm + L.G, sm + L.hs, sm + L.J);
-        if (it == 0) {
-          // J_0 factored once per step (LU_Prediction,
-          // Curves/standard_predictor_convolutions.adb:1142-1185, factors
-          // J_0 once by lufac and reuses it for every coefficient): the LU
-          // of a copy of J_0, then M = J_0^{-1}, so that each coefficient's
-          // solve below is one matrix-vector product.
-          for (int q = ctid(); q < n * n; q += blockDim.x) stn_at<PN>(sm + L.R, q, ldn_at<PN>(sm + L.J, q));
-          __syncthreads();
-          cta_lufac<PN>(n, sm + L.R, piv, dinv, piv + 32);
-          cta_luinverse<PN>(n, sm + L.R, piv, dinv, sm + L.M);
-        }
-        for (int k = 0; k <= w; ++k) {
-          for (int i = ctid(); i < n; i += blockDim.x) {
-            typename PN::T acc = PN::neg(ldn_at<PN>(sm + L.hs, (long)i * (w + 1) + k));
-            for (int j = 1; j <= k; ++j)
-              for (int l = 0; l < n; ++l)
-                acc = PN::sub(acc, PN::mul(ldn_at<PN>(sm + L.J, ((long)j * n + i) * n + l),
-                                           ldn_at<PN>(sm + L.dx, (long)(k - j) * n + l)));
-            stn_at<PN>(sm + L.rhs, i, acc);
-          }
-          __syncthreads();
-          cta_matvec<PN>(n, sm + L.M, sm + L.rhs, sm + L.dx + (long)k * n * Wp);
-        }
-        for (int t2 = ctid(); t2 < n * (w + 1); t2 += blockDim.x) {
-          const int i = t2 / (w + 1), k = t2 % (w + 1);
-          const long o = (long)i * (K + 1) + k;
-          stn_at<PN>(xs, o, PN::add(ldn_at<PN>(xs, o), ldn_at<PN>(sm + L.dx, (long)k * n + i)));
+      hom_eval_cta<PN>(S, s, 0, t, xs, K + 1, sm + L.V, sm + L.G, sm + L.hs, sm + L.J0);
+      cta_lufac<PN>(n, sm + L.J0, piv, dinv, piv + 32);
+      cta_luinverse<PN>(n, sm + L.J0, piv, dinv, sm + L.M);
+      for (int k = 1; k <= K; ++k) {
+        hom_coef_cta<PN>(S, s, k, t, xs, K + 1, sm + L.V, sm + L.r);
+        for (int i = ctid(); i < n; i += blockDim.x) {
+          typename PN::T acc = PN::zero();
+          for (int j = 0; j < n; ++j)
+            acc = PN::add(acc, PN::mul(ldn_at<PN>(sm + L.M, (long)i * n + j), ldn_at<PN>(sm + L.r, j)));
+          stn_at<PN>(xs, (long)i * (K + 1) + k, PN::neg(acc));
         }
         __syncthreads();
       }

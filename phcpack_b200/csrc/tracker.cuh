@@ -302,6 +302,78 @@ __device__ void hom_eval_cta(const TrackDev &S, int s, int w, double t0, const d
   __syncthreads();
 }
 
+// Coefficient k >= 1 of the homotopy at a series truncated below degree k:
+// with x_k, x_{k+1}, ... zero in x (n series, leading dimension xld numbers),
+//   r[i] = [h_i(x(s), t0 + s)]_k,
+// which, as h is polynomial, leaves out exactly the term J_0 x_k, so that
+// x_k = -J_0^{-1} r (the recursion for Taylor coefficients of the path).
+// V2: shared staging of two numbers per distinct monomial, its series
+// coefficients k-1 and k.  Phase 1: one thread per monomial; phase 2: one
+// warp per equation, lanes over its terms.
+template <class N>
+__device__ void hom_coef_cta(const TrackDev &S, int s, int k, double t0, const double *x, int xld, double *V2,
+                             double *r) {
+  typedef typename N::T T;
+  const int W = N::width;
+  const int n = S.dim[s];
+  const int m0 = S.mono_off[s];
+  const int nm = S.mono_off[s + 1] - m0;
+  const int mv = S.maxvar;
+  for (int m = ctid(); m < nm; m += blockDim.x) {
+    const int gm = m0 + m;
+    const int kv = S.mono_nvr[gm];
+    const int *ix = S.mono_idx + (long)gm * mv;
+    const int *ex = S.mono_exp + (long)gm * mv;
+    T c1 = N::zero(), c2 = N::zero();  // coefficients k-1 and k
+    if (kv == 0) {
+      if (k == 1) c1 = N::one();
+    } else if (simple_monomial(kv, ex)) {
+      const double *xa = x + (long)ix[0] * xld * W;
+      const double *xb = (kv == 2) ? x + (long)ix[1] * xld * W : xa;
+      if (kv == 1 && ex[0] == 1) {
+        c1 = ldn_at<N>(xa, k - 1);
+        c2 = ldn_at<N>(xa, k);
+      } else {
+        for (int i = 0; i <= k - 1; ++i) c1 = N::add(c1, N::mul(ldn_at<N>(xa, i), ldn_at<N>(xb, k - 1 - i)));
+        for (int i = 0; i <= k; ++i) c2 = N::add(c2, N::mul(ldn_at<N>(xa, i), ldn_at<N>(xb, k - i)));
+      }
+    } else {
+      T F[kTrackKmax + 1];
+      for (int i = 0; i <= k; ++i) F[i] = (i == 0) ? N::one() : N::zero();
+      for (int v = 0; v < kv; ++v)
+        for (int e = 0; e < ex[v]; ++e) {
+          const double *xv = x + (long)ix[v] * xld * W;
+          for (int kk = k; kk >= 0; --kk) {  // in place: F[kk] only needs F[<= kk]
+            T a = N::zero();
+            for (int i = 0; i <= kk; ++i) a = N::add(a, N::mul(ldn_at<N>(xv, i), F[kk - i]));
+            F[kk] = a;
+          }
+        }
+      c1 = F[k - 1];
+      c2 = F[k];
+    }
+    stn_at<N>(V2, 2L * m, c1);
+    stn_at<N>(V2, 2L * m + 1, c2);
+  }
+  __syncthreads();
+  const int e0 = S.eq_off[s];
+  const int lane = ctid() & 31, warp = ctid() >> 5, nw = blockDim.x >> 5;
+  for (int i = warp; i < n; i += nw) {
+    T acc = N::zero();
+    for (int tr = S.term_off[e0 + i] + lane; tr < S.term_off[e0 + i + 1]; tr += 32) {
+      const T a = cnum<N>(S.term_a[2 * tr], S.term_a[2 * tr + 1]);
+      const T b = N::sub(cnum<N>(S.term_b[2 * tr], S.term_b[2 * tr + 1]), a);  // d/dt
+      const T c0 = N::add(a, N::scale_d(b, t0));
+      const long mm = 2L * (S.term_mono[tr] - m0);
+      acc = N::add(acc, N::mul(c0, ldn_at<N>(V2, mm + 1)));
+      acc = N::add(acc, N::mul(b, ldn_at<N>(V2, mm)));
+    }
+    acc = warp_sum<N>(acc);
+    if (lane == 0) stn_at<N>(r, i, acc);
+  }
+  __syncthreads();
+}
+
 // LU factorization with partial pivoting of the n x n matrix A (row-major,
 // shared memory, n <= 32), in place: lufac of
 // Math_Lib/Reduction/standard_complex_linear_solvers.adb:123-178 (LINPACK's

@@ -23,6 +23,9 @@ from .benchwork import MD_ADD, MD_MUL, _threads_run, cpu_info
 MODEL_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "models", "step_mlp.npz")
 
 
+DEFAULT_K = hm.DEFAULT_IPAR["deg"]
+
+
 def load_model_bytes():
     if not os.path.exists(MODEL_PATH):
         return None
@@ -35,12 +38,12 @@ def track_flops(pb: hm.TrackProblem, steps, rejected, pmode=1):
     multiply-adds per phase weighted with the reference's convention
     (double-double add 20, mul 23; double 1 and 1; complex product = 4
     multiplications + 2 additions, accumulation 2 additions):
-      series Newton (4 steps at working degrees 1, 3, 7, 8): per step one
-        evaluation (a series product per distinct monomial, the coefficient
-        gathers of the values and of the Jacobian), the block-Toeplitz
-        right-hand sides ((w+1)(w+2)/2 n^2) and the products with J_0^{-1}
-        ((w+1) n^2); once per predictor step the LU of J_0 (n^3/3) and the
-        inverse (2 n^3/3); all in the predictor's precision;
+      predictor (Taylor series to degree K, in the predictor's precision):
+        the values and Jacobian at the point, the LU of J_0 (n^3/3) and its
+        inverse (2 n^3/3); per degree k = 1..K the coefficients k-1 and k of
+        every distinct monomial (2k + 1 products for a product of two
+        series), the coefficient gathers of the values (2 per term) and the
+        product with J_0^{-1} (n^2);
       predictor feedback: one point evaluation of the values;
       corrector: 2 Newton iterations, each a point evaluation of the values
         in double-double and of the Jacobian, its LU (n^3/3) and solve (n^2)
@@ -51,20 +54,15 @@ def track_flops(pb: hm.TrackProblem, steps, rejected, pmode=1):
     nmono = pb.nmono_max
     nterm = int(np.diff(pb.term_off).mean())
     njg = 2 * nterm  # Jacobian gather entries per equation (quadratic monomials)
+    K = DEFAULT_K
 
     def cma(prec):  # flops of one complex multiply-add in precision prec
         return 4 * MD_MUL[prec] + 4 * MD_ADD[prec]
 
-    def evals(w):  # (values, Jacobian) complex multiply-adds at degree w
-        conv = (w + 1) * (w + 2) // 2
-        return nmono * conv + 2 * n * (w + 1) * nterm, 2 * n * (w + 1) * njg
-
-    def newton_step(w):
-        v, j = evals(w)
-        return v + j + (w + 1) * (w + 2) // 2 * n * n + (w + 1) * n * n
-
-    pred = (sum(newton_step(w) for w in (1, 3, 7, 8)) + n ** 3) * cma(pmode)
-    v0, j0 = evals(0)
+    v0 = nmono + 2 * n * nterm  # values at a point
+    j0 = 2 * n * njg  # Jacobian at a point
+    pred = v0 + j0 + n ** 3 + sum(nmono * (2 * k + 1) + 2 * n * nterm + n * n for k in range(1, K + 1))
+    pred *= cma(pmode)
     feed = v0 * cma(pmode)
     corr = 2 * (v0 * cma(2) + (j0 + n ** 3 / 3 + n * n) * cma(pmode))
     steps = np.asarray(steps, dtype=np.float64)
@@ -125,9 +123,11 @@ class TrackWork:
                            "dd add 20 mul 23, double 1; from the launch's own step and rejection counts")
         return r
 
-    def e2e(self, stream, reps=2):
+    def e2e(self, stream, reps=3):
         torch = self.torch
         times = []
+        hm.track_host(self.pb, pmode=1, rmode=2, step_mode=self.step_mode, model=self.model,
+                      stream_ptr=stream.cuda_stream)  # warm-up call, untimed
         for _ in range(reps):
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
