@@ -96,13 +96,13 @@ __device__ double cta_maxmag(int n, const double *v, double *red) {
 // each step evaluates h(x) in precision N and J(x) in precision JN (N, or
 // double in the precision-split tracker: Newton with a double Jacobian and
 // a residual in N still converges to the accuracy of N, each step gaining
-// about 16 digits near the solution), factors J by cta_lufac and solves
+// about 16 digits near the solution), factors J by warp_lufac and solves
 // J dx = -h(x) (a singular Jacobian ends the steps unconverged, x
 // unchanged); converged when max |dx| <= tol, then extra more steps.  x
 // (shared, n numbers of precision N) is updated in place; lastdx: the last
 // max |dx|.
 template <class N, class JN>
-__device__ bool point_newton(const TrackDev &S, int s, int n, double t, double *x, double *h, double *Jm, double *Vc,
+__device__ TRACK_FN bool point_newton(const TrackDev &S, int s, int n, double t, double *x, double *h, double *Jm, double *Vc,
                              double *Gc, int *piv, double *dinv, double *red, int maxit, double tol, int extra,
                              double *lastdx) {
   bool conv = false;
@@ -111,9 +111,9 @@ __device__ bool point_newton(const TrackDev &S, int s, int n, double t, double *
   for (int it = 0; it < maxit + extra; ++it) {
     if (it >= maxit && !conv) break;
     hom_eval_cta<N, 1, JN>(S, s, 0, t, x, 1, Vc, Gc, h, Jm);
-    const int info = cta_lufac<JN>(n, Jm, piv, dinv, piv + 32);
     if (ctid() < 32) {
       const int lane = ctid();
+      const int info = warp_lufac<JN>(n, Jm, piv, dinv);
       typename JN::T b = JN::zero();
       if (lane < n) b = JN::neg(conv_num<N, JN>::go(ldn_at<N>(h, lane)));
       const typename JN::T v = warp_lusolve<JN>(n, Jm, piv, dinv, b);
@@ -154,7 +154,7 @@ __device__ double point_residual(const TrackDev &S, int s, int n, double t, cons
 // Curves/standard_rational_approximations.ads:67-100.  Returns the numerator
 // degree used (L, or K for the fallback); the denominator degree is M or 0.
 template <class N>
-__device__ int pade_one(int L, int M, int K, const double *c, double *num, double *den) {
+__device__ TRACK_FN int pade_one(int L, int M, int K, const double *c, double *num, double *den) {
   typedef typename N::T T;
   T A[kTrackKmax * kTrackKmax / 4 + 16], b[kTrackKmax / 2 + 8], q[kTrackKmax / 2 + 9];
   bool ok = true;
@@ -216,7 +216,7 @@ __device__ typename N::T horner(const double *a, int deg, const typename N::T &z
 // the coefficients at t+st.  Predictor_Feedback,
 // Curves/standard_predictor_convolutions.adb:958-993.
 template <class PN>
-__device__ double pade_mixres(const TrackDev &S, int s, int n, int K, int dendeg, double t, double st,
+__device__ TRACK_FN double pade_mixres(const TrackDev &S, int s, int n, int K, int dendeg, double t, double st,
                               const double *num, const double *den, const int *degs, double *xp, double *V,
                               double *G, double *hs, double *red) {
   const int Wp = PN::width;
@@ -327,7 +327,8 @@ __global__ void __launch_bounds__(kTrackThreads, (track_min_blocks<PN, RN>::valu
       }
       __syncthreads();
       hom_eval_cta<PN>(S, s, 0, t, xs, K + 1, sm + L.V, sm + L.G, sm + L.hs, sm + L.J0);
-      cta_lufac<PN>(n, sm + L.J0, piv, dinv, piv + 32);
+      if (ctid() < 32) warp_lufac<PN>(n, sm + L.J0, piv, dinv);
+      __syncthreads();
       cta_luinverse<PN>(n, sm + L.J0, piv, dinv, sm + L.M);
       for (int k = 1; k <= K; ++k) {
         hom_coef_cta<PN>(S, s, k, t, xs, K + 1, sm + L.V, sm + L.r);

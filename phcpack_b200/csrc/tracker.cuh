@@ -8,6 +8,17 @@
 
 namespace phc {
 
+// TRACK_OUTLINE=1 compiles the large CTA-level routines as calls instead of
+// inlining them at every call site (less code for the instruction cache).
+#ifndef TRACK_OUTLINE
+#define TRACK_OUTLINE 0
+#endif
+#if TRACK_OUTLINE
+#define TRACK_FN __noinline__
+#else
+#define TRACK_FN
+#endif
+
 static const int kTrackThreads = 128;
 static const int kTrackKmax = 16;   // largest series degree of the predictor
 
@@ -141,7 +152,7 @@ __device__ __forceinline__ typename N::T cnum(double re, double im) {
 // pair); KC coefficients at a time, so that each term's data is loaded once
 // per KC coefficients.
 template <class N, int KC = 1, class JN = N>
-__device__ void hom_eval_cta(const TrackDev &S, int s, int w, double t0, const double *x, int xld, double *V,
+__device__ TRACK_FN void hom_eval_cta(const TrackDev &S, int s, int w, double t0, const double *x, int xld, double *V,
                              double *G, double *h, double *J) {
   typedef typename N::T T;
   typedef typename JN::T JT;
@@ -311,7 +322,7 @@ __device__ void hom_eval_cta(const TrackDev &S, int s, int w, double t0, const d
 // coefficients k-1 and k.  Phase 1: one thread per monomial; phase 2: one
 // warp per equation, lanes over its terms.
 template <class N>
-__device__ void hom_coef_cta(const TrackDev &S, int s, int k, double t0, const double *x, int xld, double *V2,
+__device__ TRACK_FN void hom_coef_cta(const TrackDev &S, int s, int k, double t0, const double *x, int xld, double *V2,
                              double *r) {
   typedef typename N::T T;
   const int W = N::width;
@@ -381,63 +392,58 @@ __device__ void hom_coef_cta(const TrackDev &S, int s, int k, double t0, const d
 // limbs), rows k and ell swap in columns k..n-1, and the multipliers
 // -a_ik / a_kk overwrite column k below the diagonal.  Besides ipvt the
 // reciprocals dinv[k] = 1 / u_kk are kept for the back substitution (NaN
-// for a zero pivot).
-// Warp 0 picks the pivot, swaps and forms the multipliers; the CTA updates
-// the trailing block: two barriers per column.  Returns info (every
-// thread): 0, or k + 1 for the first column k without a nonzero pivot.
-// sh: one shared int.
+// for a zero pivot).  One warp alone, lane i owning row i: no CTA barrier,
+// the other warps of the CTA stay free.  Called by all lanes of the warp;
+// returns info to every lane: 0, or k + 1 for the first column k without a
+// nonzero pivot.
 template <class N>
-__device__ int cta_lufac(int n, double *A, int *ipvt, double *dinv, int *sh) {
+__device__ TRACK_FN int warp_lufac(int n, double *A, int *ipvt, double *dinv) {
   typedef typename N::T T;
-  const int lane = ctid() & 31;
-  int info = 0;  // meaningful in warp 0
+  const int lane = threadIdx.x & 31;
+  int info = 0;
   for (int k = 0; k < n; ++k) {
-    if (ctid() < 32) {
-      const int i = k + lane;
-      double v = -1.0;
-      if (i < n) {
-        v = N::lead(ldn_at<N>(A, (long)i * n + k));
-        if (!(v == v)) v = INFINITY;  // a NaN pivot candidate reads as infinity
-      }
-      int ix = i < n ? i : n;
-      for (int o = 16; o > 0; o >>= 1) {  // largest value, the first row on ties
-        const double v2 = __shfl_xor_sync(0xffffffffu, v, o);
-        const int ix2 = __shfl_xor_sync(0xffffffffu, ix, o);
-        if (v2 > v || (v2 == v && ix2 < ix)) { v = v2; ix = ix2; }
-      }
-      const int ell = ix < n ? ix : n - 1;
-      if (lane == 0) ipvt[k] = ell;
-      if (v == 0.0) {
-        if (info == 0) info = k + 1;  // this column is already triangularized
-        if (lane == 0) stn_at<N>(dinv, k, N::from(NAN));  // a solve with these factors gives NaN
-      } else {
-        if (ell != k)
-          for (int j = k + lane; j < n; j += 32) {
-            const T a = ldn_at<N>(A, (long)ell * n + j);
-            stn_at<N>(A, (long)ell * n + j, ldn_at<N>(A, (long)k * n + j));
-            stn_at<N>(A, (long)k * n + j, a);
-          }
-        __syncwarp();
-        const T inv = N::div(N::one(), ldn_at<N>(A, (long)k * n + k));
-        if (lane == 0) stn_at<N>(dinv, k, inv);
-        const T temp = N::neg(inv);
-        if (i > k && i < n) stn_at<N>(A, (long)i * n + k, N::mul(temp, ldn_at<N>(A, (long)i * n + k)));
-      }
-      if (k == n - 1 && lane == 0) *sh = info;
+    double v = -1.0;
+    if (lane >= k && lane < n) {
+      v = N::lead(ldn_at<N>(A, (long)lane * n + k));
+      if (!(v == v)) v = INFINITY;  // a NaN pivot candidate reads as infinity
     }
-    __syncthreads();
-    const int m = n - k - 1;
-    for (int e = ctid(); e < m * m; e += blockDim.x) {
-      const int i = k + 1 + e / m, j = k + 1 + e % m;
-      const long o = (long)i * n + j;
-      stn_at<N>(A, o, N::add(ldn_at<N>(A, o), N::mul(ldn_at<N>(A, (long)k * n + j), ldn_at<N>(A, (long)i * n + k))));
+    int ix = (lane >= k && lane < n) ? lane : n;
+    for (int o = 16; o > 0; o >>= 1) {  // largest value, the first row on ties
+      const double v2 = __shfl_xor_sync(0xffffffffu, v, o);
+      const int ix2 = __shfl_xor_sync(0xffffffffu, ix, o);
+      if (v2 > v || (v2 == v && ix2 < ix)) { v = v2; ix = ix2; }
     }
-    __syncthreads();
+    const int ell = ix < n ? ix : n - 1;
+    if (lane == 0) ipvt[k] = ell;
+    if (v == 0.0) {
+      if (info == 0) info = k + 1;  // this column is already triangularized
+      if (lane == 0) stn_at<N>(dinv, k, N::from(NAN));
+      __syncwarp();
+      continue;
+    }
+    if (ell != k)
+      for (int j = k + lane; j < n; j += 32) {
+        const T a = ldn_at<N>(A, (long)ell * n + j);
+        stn_at<N>(A, (long)ell * n + j, ldn_at<N>(A, (long)k * n + j));
+        stn_at<N>(A, (long)k * n + j, a);
+      }
+    __syncwarp();
+    const T inv = N::div(N::one(), ldn_at<N>(A, (long)k * n + k));
+    if (lane == 0) stn_at<N>(dinv, k, inv);
+    if (lane > k && lane < n) {
+      const T m = N::mul(N::neg(inv), ldn_at<N>(A, (long)lane * n + k));
+      stn_at<N>(A, (long)lane * n + k, m);
+      for (int j = k + 1; j < n; ++j) {
+        const long o = (long)lane * n + j;
+        stn_at<N>(A, o, N::add(ldn_at<N>(A, o), N::mul(ldn_at<N>(A, (long)k * n + j), m)));
+      }
+    }
+    __syncwarp();
   }
-  return *sh;
+  return info;
 }
 
-// Solve A x = b with the factors of cta_lufac: lusolve of
+// Solve A x = b with the factors of warp_lufac: lusolve of
 // standard_complex_linear_solvers.adb:552-583 (row interchanges applied in
 // order with the multipliers, then back substitution), except that the back
 // substitution multiplies by dinv[k] = 1 / u_kk where lusolve divides.
@@ -464,11 +470,11 @@ __device__ typename N::T warp_lusolve(int n, const double *A, const int *ipvt, c
   return v;
 }
 
-// M = A^{-1} from the factors of cta_lufac, one thread per column c: the
+// M = A^{-1} from the factors of warp_lufac, one thread per column c: the
 // column of M is the work vector of lusolve applied to e_c (same order of
 // operations as warp_lusolve).
 template <class N>
-__device__ void cta_luinverse(int n, const double *A, const int *ipvt, const double *dinv, double *M) {
+__device__ TRACK_FN void cta_luinverse(int n, const double *A, const int *ipvt, const double *dinv, double *M) {
   typedef typename N::T T;
   for (int c = ctid(); c < n; c += blockDim.x) {
     for (int i = 0; i < n; ++i) stn_at<N>(M, (long)i * n + c, i == c ? N::one() : N::zero());
