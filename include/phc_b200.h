@@ -191,12 +191,12 @@ int phc_newton_host(int prec, int cplx, int nsys, int dim, int deg, int szt, int
  *   residual bound), learn_scale (multiplies learned proposals; 0 = 1).
  * pmode: 1 (double) or 2 (double-double), the precision of the predictor
  *   and of the corrector's Jacobian and linear solves; the corrector's
- *   residuals and updates are double-double; rmode: refinement precision 2
- *   or 4 (quad-double), all of its arithmetic.
+ *   residuals and updates are double-double; rmode: refinement precision 2,
+ *   4 (quad-double) or 8 (octo-double), all of its arithmetic.
  * step_mode 1 with a model (phc_mlp_*) uses the learned step proposer; a
  *   proposal whose feedback or corrector fails is redone with the plain step.
- * Output per path: xend maxdim complex quad-doubles (lower limbs zero below
- *   rmode), info[3p..3p+2] = status (0 success, 1 step below minsize,
+ * Output per path: xend maxdim complex quad-doubles, octo-doubles for rmode
+ *   8 (lower limbs zero below rmode), info[3p..3p+2] = status (0 success, 1 step below minsize,
  *   2 maxsteps reached, 3 endpoint residual above restol), steps, rejected
  *   steps; dinfo[2p..2p+1] = final t, endpoint residual.
  * log: when not NULL, each accepted step appends 32 floats (24 features,

@@ -210,6 +210,103 @@ static inline double lead(const qd &a) { return a.x[0]; }
 static inline bool is_zero(const qd &a) { return a.x[0] == 0.0 && a.x[1] == 0.0 && a.x[2] == 0.0 && a.x[3] == 0.0; }
 static inline qd abs(const qd &a) { return a.x[0] < 0.0 ? -a : a; }
 
+// ---------------------------------------------------------------- od
+// Octo-double: the qd scheme above on eight limbs (nine accumulators, the
+// order-8 products summed plainly), the scheme of the reference's
+// octo-doubles (odf_add, odf_mul, odf_mul_od_d, odf_div and odf_fast_renorm
+// of Norms/octo_double_functions.cpp, CAMPARY's baileyAdd/Mul_fast<8,8,8>)
+// written as loops.  The device code (phcpack_b200/csrc/md.cuh) sums the
+// order-8 products by fused multiply-adds.
+struct od {
+  double x[8];
+  od() { for (int i = 0; i < 8; ++i) x[i] = 0.0; }
+  od(double a) { x[0] = a; for (int i = 1; i < 8; ++i) x[i] = 0.0; }
+  od(const dd &a) { x[0] = a.hi; x[1] = a.lo; for (int i = 2; i < 8; ++i) x[i] = 0.0; }
+  od(const qd &a) { for (int i = 0; i < 4; ++i) x[i] = a.x[i]; for (int i = 4; i < 8; ++i) x[i] = 0.0; }
+};
+
+static inline od renorm9(const double *in) {
+  double f[9];
+  double s = in[8];
+  for (int i = 7; i >= 0; --i) s = quick_two_sum(in[i], s, &f[i + 1]);
+  f[0] = s;
+  od r;
+  int k = 0;
+  double acc = f[0];
+  for (int i = 1; i <= 8; ++i) {
+    double e;
+    const double t = quick_two_sum(acc, f[i], &e);
+    if (e != 0.0 && k < 8) {
+      r.x[k++] = t;
+      acc = e;
+    } else {
+      acc = t;
+    }
+  }
+  if (k < 8 && acc != 0.0) r.x[k] = acc;
+  return r;
+}
+
+static inline void accumulate9(double *f, int lvl, double v) {
+  for (int j = lvl; j < 8; ++j) f[j] = two_sum(f[j], v, &v);
+  f[8] += v;
+}
+
+static inline od operator+(const od &a, const od &b) {
+  double f[9] = {0.0};
+  for (int k = 7; k >= 0; --k) {
+    double e;
+    f[k] = two_sum(a.x[k], b.x[k], &e);
+    accumulate9(f, k + 1, e);
+  }
+  return renorm9(f);
+}
+static inline od operator-(const od &a) {
+  od r;
+  for (int i = 0; i < 8; ++i) r.x[i] = -a.x[i];
+  return r;
+}
+static inline od operator-(const od &a, const od &b) { return a + (-b); }
+static inline od operator*(const od &a, const od &b) {
+  double f[9] = {0.0};
+  f[8] = a.x[1] * b.x[7];
+  for (int i = 2; i < 8; ++i) f[8] += a.x[i] * b.x[8 - i];
+  for (int k = 7; k >= 0; --k)
+    for (int i = 0; i <= k; ++i) {
+      double e;
+      const double p = two_prod(a.x[i], b.x[k - i], &e);
+      accumulate9(f, k + 1, e);
+      accumulate9(f, k, p);
+    }
+  return renorm9(f);
+}
+static inline od mul_d(const od &a, double b) {
+  double f[9] = {0.0};
+  for (int k = 7; k >= 0; --k) {
+    double e;
+    f[k] = two_prod(a.x[k], b, &e);
+    accumulate9(f, k + 1, e);
+  }
+  return renorm9(f);
+}
+static inline od operator/(const od &a, const od &b) {
+  double q[9];
+  od r = a;
+  for (int i = 0; i < 9; ++i) {
+    q[i] = r.x[0] / b.x[0];
+    if (i < 8) r = r - mul_d(b, q[i]);
+  }
+  return renorm9(q);
+}
+static inline double to_double(const od &a) { return a.x[0] + a.x[1]; }
+static inline double lead(const od &a) { return a.x[0]; }
+static inline bool is_zero(const od &a) {
+  for (int i = 0; i < 8; ++i)
+    if (a.x[i] != 0.0) return false;
+  return true;
+}
+static inline od abs(const od &a) { return a.x[0] < 0.0 ? -a : a; }
+
 // ------------------------------------------------------- plain double
 static inline double sqrt(double a) { return std::sqrt(a); }
 static inline double abs(double a) { return std::fabs(a); }
@@ -223,13 +320,16 @@ template <class R> struct limbs;
 template <> struct limbs<double> { static const int n = 1; };
 template <> struct limbs<dd> { static const int n = 2; };
 template <> struct limbs<qd> { static const int n = 4; };
+template <> struct limbs<od> { static const int n = 8; };
 
 static inline void load(const double *p, double &a) { a = p[0]; }
 static inline void load(const double *p, dd &a) { a.hi = p[0]; a.lo = p[1]; }
 static inline void load(const double *p, qd &a) { for (int i = 0; i < 4; ++i) a.x[i] = p[i]; }
+static inline void load(const double *p, od &a) { for (int i = 0; i < 8; ++i) a.x[i] = p[i]; }
 static inline void store(double *p, const double &a) { p[0] = a; }
 static inline void store(double *p, const dd &a) { p[0] = a.hi; p[1] = a.lo; }
 static inline void store(double *p, const qd &a) { for (int i = 0; i < 4; ++i) p[i] = a.x[i]; }
+static inline void store(double *p, const od &a) { for (int i = 0; i < 8; ++i) p[i] = a.x[i]; }
 
 // ------------------------------------------------------- complex
 template <class R> struct cx {
@@ -268,8 +368,10 @@ template <class R> struct is_cx<cx<R> > { static const bool v = true; };
 static inline double conj(double a) { return a; }
 static inline dd conj(const dd &a) { return a; }
 static inline qd conj(const qd &a) { return a; }
+static inline od conj(const od &a) { return a; }
 static inline double norm2(double a) { return a * a; }
 static inline dd norm2(const dd &a) { return a * a; }
 static inline qd norm2(const qd &a) { return a * a; }
+static inline od norm2(const od &a) { return a * a; }
 
 }  // namespace orc

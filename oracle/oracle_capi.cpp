@@ -208,4 +208,21 @@ int orc_newton_step(int prec, int cplx, int dim, int deg, int maxdeg, int maxvar
   return -1;
 }
 
+// Octo-double arithmetic of this oracle: op 0 add, 1 mul, 2 div, 3 multiply
+// by the double b[8k]; n numbers of eight limbs each.
+int orc_od_binop(int op, int n, const double *a, const double *b, double *out) {
+  for (int k = 0; k < n; ++k) {
+    od x, y, z;
+    load(a + 8 * k, x);
+    load(b + 8 * k, y);
+    if (op == 0) z = x + y;
+    else if (op == 1) z = x * y;
+    else if (op == 2) z = x / y;
+    else if (op == 3) z = mul_d(x, y.x[0]);
+    else return -1;
+    store(out + 8 * k, z);
+  }
+  return 0;
+}
+
 }  // extern "C"

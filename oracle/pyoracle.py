@@ -89,6 +89,17 @@ class Lib:
         return sol, rhs, Q, R, fl
 
 
+    def od_binop(self, op, a, b):
+        """Octo-double add (0), mul (1), div (2) or multiply by a double (3,
+        b[k, 0]) of rows of eight limbs."""
+        a = np.ascontiguousarray(a, dtype=np.float64).reshape(-1, 8)
+        b = np.ascontiguousarray(b, dtype=np.float64).reshape(-1, 8)
+        out = np.zeros_like(a)
+        rc = self._fn("od_binop")(op, a.shape[0], _dp(a), _dp(b), _dp(out))
+        assert rc == 0
+        return out
+
+
 _oracle = None
 _ref = None
 
@@ -152,8 +163,9 @@ def newton_steps(lib: Lib, b, deg, nsteps, schedule=0):
 def track(lib: Lib, pb, ipar, dpar, pmode=1, rmode=2, nthreads=1):
     """Track the paths of a homotopy TrackProblem on the CPU (the tracker
     restatement of tracker_oracle.cpp).  Returns (xend, info, dinfo) with
-    the layout of the C ABI."""
-    xend = np.zeros(pb.npaths * pb.maxdim * 8)
+    the layout of the C ABI (16 doubles per complex end point coordinate for
+    rmode 8, 8 otherwise)."""
+    xend = np.zeros(pb.npaths * pb.maxdim * (16 if rmode == 8 else 8))
     info = np.zeros(pb.npaths * 3, np.int32)
     dinfo = np.zeros(pb.npaths * 2)
     f = lib._fn("track")

@@ -15,6 +15,7 @@
 #include <cstdlib>
 #include "double_double_functions.h"
 #include "quad_double_functions.h"
+#include "octo_double_functions.h"
 #include "dbl2_convolutions_host.h"
 #include "dbl2_monomials_host.h"
 #include "dbl4_convolutions_host.h"
@@ -270,6 +271,31 @@ int ref_bals_solve(int prec, int cplx, int dim, int degp1, int tailidx, const do
   Qm.out(Q);
   Rm.out(R);
   flags[0] = zeroQ; flags[1] = noqr; flags[2] = up; flags[3] = bs; flags[4] = nt;
+  return 0;
+}
+
+// Octo-double arithmetic of the reference (Norms/octo_double_functions.cpp):
+// op 0 add, 1 mul, 2 div, 3 multiply by the double b[0]; n numbers of eight
+// limbs each in a, b, out.
+int ref_od_binop(int op, int n, const double *a, const double *b, double *out) {
+  for (int k = 0; k < n; ++k) {
+    const double *x = a + 8 * k, *y = b + 8 * k;
+    double *z = out + 8 * k;
+    if (op == 0)
+      odf_add(x[0], x[1], x[2], x[3], x[4], x[5], x[6], x[7], y[0], y[1], y[2], y[3], y[4], y[5], y[6], y[7], &z[0],
+              &z[1], &z[2], &z[3], &z[4], &z[5], &z[6], &z[7]);
+    else if (op == 1)
+      odf_mul(x[0], x[1], x[2], x[3], x[4], x[5], x[6], x[7], y[0], y[1], y[2], y[3], y[4], y[5], y[6], y[7], &z[0],
+              &z[1], &z[2], &z[3], &z[4], &z[5], &z[6], &z[7]);
+    else if (op == 2)
+      odf_div(x[0], x[1], x[2], x[3], x[4], x[5], x[6], x[7], y[0], y[1], y[2], y[3], y[4], y[5], y[6], y[7], &z[0],
+              &z[1], &z[2], &z[3], &z[4], &z[5], &z[6], &z[7]);
+    else if (op == 3)
+      odf_mul_od_d(x[0], x[1], x[2], x[3], x[4], x[5], x[6], x[7], y[0], &z[0], &z[1], &z[2], &z[3], &z[4], &z[5],
+                   &z[6], &z[7]);
+    else
+      return -1;
+  }
   return 0;
 }
 

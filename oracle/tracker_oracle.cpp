@@ -346,6 +346,12 @@ template <> void convert(const cx<dd> &a, cx<dd> &b) { b = a; }
 template <> void convert(const cx<double> &a, cx<dd> &b) { b = cx<dd>(dd(a.re), dd(a.im)); }
 template <> void convert(const cx<dd> &a, cx<qd> &b) { b = cx<qd>(qd(a.re), qd(a.im)); }
 template <> void convert(const cx<qd> &a, cx<qd> &b) { b = a; }
+template <> void convert(const cx<dd> &a, cx<od> &b) { b = cx<od>(od(a.re), od(a.im)); }
+template <> void convert(const cx<od> &a, cx<od> &b) { b = a; }
+// end points are written as complex quad-doubles, or octo-doubles for an
+// octo-double refinement
+template <class RT> struct out_num { typedef cx<qd> type; };
+template <> struct out_num<cx<od> > { typedef cx<od> type; };
 
 // Newton at a point (the corrector / refinement), returns converged:
 // LU_Newton_Steps (Curves/corrector_convolutions.adb:1193-1224) with h in
@@ -507,11 +513,11 @@ static PathOut track_path(const TrackSys &S, int s, const TrackPar &P, const dou
     o.residual = maxres(S, s, t, xr);
     o.status = failed ? 1 : 2;
   }
-  for (int i = 0; i < n; ++i) store(xend + (long)i * limbs<cx<qd> >::n, cx<qd>());
+  typedef typename out_num<RT>::type XT;
   for (int i = 0; i < n; ++i) {
-    cx<qd> q;
+    XT q;
     convert(xr[i], q);
-    store(xend + (long)i * limbs<cx<qd> >::n, q);
+    store(xend + (long)i * limbs<XT>::n, q);
   }
   return o;
 }
@@ -522,9 +528,10 @@ extern "C" {
 
 // Track npaths paths with nthreads host threads.  pmode: predictor
 // precision (1 double, 2 double-double); rmode: refinement precision
-// (2 dd, 4 qd); the corrector is double-double.  x0: start points, maxdim
-// complex doubles per path; xend: maxdim complex quad-doubles per path
-// (lower limbs zero below the refinement precision); info: per path
+// (2 dd, 4 qd, 8 od); the corrector is double-double.  x0: start points,
+// maxdim complex doubles per path; xend: maxdim complex quad-doubles per
+// path (octo-doubles for rmode 8; lower limbs zero below the refinement
+// precision); info: per path
 // status, nsteps, nreject; dinfo: per path t, residual.
 int orc_track(int nsys, const int *dim, int maxvar, const int *mono_off, const int *mono_nvr, const int *mono_idx,
               const int *mono_exp, const int *eq_off, const int *term_off, const int *term_mono,
@@ -538,6 +545,7 @@ int orc_track(int nsys, const int *dim, int maxvar, const int *mono_off, const i
   P.pbeta = dpar[0]; P.alpha = dpar[1]; P.maxsize = dpar[2]; P.minsize = dpar[3];
   P.tolres = dpar[4]; P.epsilon = dpar[5]; P.restol = dpar[6];
   if (P.numdeg + P.dendeg != P.deg || P.deg < 3) return -1;
+  if ((pmode != 1 && pmode != 2) || (rmode != 2 && rmode != 4 && rmode != 8)) return -1;
   std::atomic<int> next(0);
   auto work = [&]() {
     for (;;) {
@@ -545,12 +553,14 @@ int orc_track(int nsys, const int *dim, int maxvar, const int *mono_off, const i
       if (p >= npaths) return;
       const int s = path_sys[p];
       PathOut o;
-      double *xe = xend + (long)p * maxdim * 8;
+      double *xe = xend + (long)p * maxdim * (rmode == 8 ? 16 : 8);
       const double *xs = x0 + (long)p * maxdim * 2;
       if (pmode == 1 && rmode == 2) o = track_path<cx<double>, cx<dd>, cx<dd> >(S, s, P, xs, xe);
-      else if (pmode == 1) o = track_path<cx<double>, cx<dd>, cx<qd> >(S, s, P, xs, xe);
+      else if (pmode == 1 && rmode == 4) o = track_path<cx<double>, cx<dd>, cx<qd> >(S, s, P, xs, xe);
+      else if (pmode == 1) o = track_path<cx<double>, cx<dd>, cx<od> >(S, s, P, xs, xe);
       else if (rmode == 2) o = track_path<cx<dd>, cx<dd>, cx<dd> >(S, s, P, xs, xe);
-      else o = track_path<cx<dd>, cx<dd>, cx<qd> >(S, s, P, xs, xe);
+      else if (rmode == 4) o = track_path<cx<dd>, cx<dd>, cx<qd> >(S, s, P, xs, xe);
+      else o = track_path<cx<dd>, cx<dd>, cx<od> >(S, s, P, xs, xe);
       info[3 * p] = o.status;
       info[3 * p + 1] = o.nsteps;
       info[3 * p + 2] = o.nreject;

@@ -142,8 +142,9 @@ int phc_track_host(int nsys, const int *dim, int maxvar, const int *mono_off, co
     const size_t b = (i + 1 == ins.size()) ? (ins[i].second ? model_bytes : 0) : ins[i].second;
     total += (b + 255) & ~size_t(255);
   }
+  const size_t xbytes = (size_t)npaths * maxdim * (rmode == 8 ? 128 : 64);  // complex qd (od) per coordinate
   const size_t o_xend = total;
-  total += (((size_t)npaths * maxdim * 64) + 255) & ~size_t(255);
+  total += (xbytes + 255) & ~size_t(255);
   const size_t o_info = total;
   total += (((size_t)npaths * 12) + 255) & ~size_t(255);
   const size_t o_dinfo = total;
@@ -171,7 +172,7 @@ int phc_track_host(int nsys, const int *dim, int maxvar, const int *mono_off, co
                     (int *)(b + o_info), (double *)(b + o_dinfo), nullptr, 0, nullptr, (int *)(b + o_q), 0, st);
   }
   if (out == PHC_OK) {
-    if (cudaMemcpyAsync(xend, b + o_xend, (size_t)npaths * maxdim * 64, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+    if (cudaMemcpyAsync(xend, b + o_xend, xbytes, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaMemcpyAsync(info, b + o_info, (size_t)npaths * 12, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaMemcpyAsync(dinfo, b + o_dinfo, (size_t)npaths * 16, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaStreamSynchronize(st) != cudaSuccess) {

@@ -1,8 +1,8 @@
 // md.cuh -- multiple-double arithmetic on the device (sm_100a).
 //
-// Number formats as in PHCpack src/GPU/Norms: double-double (hi, lo) and
-// quad-double (four limbs, decreasing significance), stored
-// limb-interleaved.  Complex numbers store the real limbs, then the
+// Number formats as in PHCpack src/GPU/Norms: double-double (hi, lo),
+// quad-double and octo-double (four and eight limbs, decreasing
+// significance), stored limb-interleaved.  Complex numbers store the real limbs, then the
 // imaginary limbs.
 //
 // Every floating-point operation goes through __dadd_rn / __dsub_rn /
@@ -249,6 +249,135 @@ MD_INL qd sqrt(const qd &a) {
 MD_INL double lead(const qd &a) { return a.x[0]; }
 MD_INL bool is_zero(const qd &a) { return a.x[0] == 0.0 && a.x[1] == 0.0 && a.x[2] == 0.0 && a.x[3] == 0.0; }
 
+// ------------------------------------------------------------- od
+// Octo-double: eight limbs, decreasing significance.  Add, multiply and
+// divide generalise the qd scheme above to eight limbs: limb-wise (add) or
+// order-wise (multiply: all products a_i b_j with i + j = p by two_prod for
+// p < 8, plainly for p = 8) accumulation with the errors cascaded into the
+// lower-order accumulators, a ninth accumulator for the rest, and a
+// renormalisation of the nine terms: the scheme of the reference's
+// octo-doubles (Norms/octo_double_functions.cpp, CAMPARY's
+// baileyAdd/Mul_fast<8,8,8>), except that the order-8 products are summed
+// by fused multiply-adds.
+struct od {
+  double x[8];
+};
+MD_INL od mko(double a) {
+  od r;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) r.x[i] = 0.0;
+  r.x[0] = a;
+  return r;
+}
+
+// nine overlapping terms (decreasing magnitude) -> eight-term expansion
+MD_INL od renorm9(const double (&f)[9]) {
+  double e[9];
+  double s = quick_two_sum(f[7], f[8], e[8]);
+#pragma unroll
+  for (int i = 6; i >= 0; --i) s = quick_two_sum(f[i], s, e[i + 1]);
+  e[0] = s;
+  od r = mko(0.0);
+  int k = 0;
+  double acc = e[0];
+#pragma unroll
+  for (int i = 1; i <= 8; ++i) {
+    double err;
+    const double t = quick_two_sum(acc, e[i], err);
+    if (err != 0.0 && k < 8) {
+#pragma unroll
+      for (int j = 0; j < 8; ++j) r.x[j] = (k == j) ? t : r.x[j];
+      ++k;
+      acc = err;
+    } else {
+      acc = t;
+    }
+  }
+  if (k < 8 && acc != 0.0) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) r.x[j] = (k == j) ? acc : r.x[j];
+  }
+  return r;
+}
+
+// v added at accumulator level lvl, its rounding errors cascaded down
+MD_INL void accum9(double (&f)[9], int lvl, double v) {
+#pragma unroll
+  for (int j = 0; j < 8; ++j)
+    if (j >= lvl) f[j] = two_sum(f[j], v, v);
+  f[8] = add(f[8], v);
+}
+
+MD_INL od operator+(const od &a, const od &b) {
+  double f[9];
+#pragma unroll
+  for (int j = 0; j < 9; ++j) f[j] = 0.0;
+#pragma unroll
+  for (int i = 7; i >= 0; --i) {
+    double e;
+    f[i] = two_sum(a.x[i], b.x[i], e);
+    accum9(f, i + 1, e);
+  }
+  return renorm9(f);
+}
+MD_INL od operator-(const od &a) {
+  od r;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) r.x[i] = -a.x[i];
+  return r;
+}
+MD_INL od operator-(const od &a, const od &b) { return a + (-b); }
+
+MD_INL od operator*(const od &a, const od &b) {
+  double f[9];
+#pragma unroll
+  for (int j = 0; j < 9; ++j) f[j] = 0.0;
+  // order-8 terms in plain arithmetic
+  f[8] = mul(a.x[1], b.x[7]);
+#pragma unroll
+  for (int i = 2; i < 8; ++i) f[8] = __fma_rn(a.x[i], b.x[8 - i], f[8]);
+#pragma unroll
+  for (int p = 7; p >= 0; --p) {
+#pragma unroll
+    for (int i = 0; i <= p; ++i) {
+      double e;
+      const double q = two_prod(a.x[i], b.x[p - i], e);
+      accum9(f, p + 1, e);
+      accum9(f, p, q);
+    }
+  }
+  return renorm9(f);
+}
+MD_INL od mul_d(const od &a, double b) {
+  double f[9];
+#pragma unroll
+  for (int j = 0; j < 9; ++j) f[j] = 0.0;
+#pragma unroll
+  for (int i = 7; i >= 0; --i) {
+    double e;
+    f[i] = two_prod(a.x[i], b, e);
+    accum9(f, i + 1, e);
+  }
+  return renorm9(f);
+}
+MD_INL od operator/(const od &a, const od &b) {
+  double q[9];
+  od r = a;
+#pragma unroll
+  for (int i = 0; i < 9; ++i) {
+    q[i] = __ddiv_rn(r.x[0], b.x[0]);
+    if (i < 8) r = r - mul_d(b, q[i]);
+  }
+  return renorm9(q);
+}
+MD_INL double lead(const od &a) { return a.x[0]; }
+MD_INL bool is_zero(const od &a) {
+  bool z = true;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) z = z && a.x[i] == 0.0;
+  return z;
+}
+
 // ------------------------------------------------------------- double
 MD_INL double mul_d(double a, double b) { return mul(a, b); }
 MD_INL double lead(double a) { return a; }
@@ -291,6 +420,17 @@ template <> struct real_traits<qd> {
   MD_INL static qd div(const qd &a, const qd &b) { return a / b; }
   MD_INL static qd sqrt(const qd &a) { return md::sqrt(a); }
   MD_INL static qd neg(const qd &a) { return -a; }
+};
+template <> struct real_traits<od> {
+  static const int limbs = 8;
+  MD_INL static od zero() { return mko(0.0); }
+  MD_INL static od one() { return mko(1.0); }
+  MD_INL static od from(double a) { return mko(a); }
+  MD_INL static od add(const od &a, const od &b) { return a + b; }
+  MD_INL static od sub(const od &a, const od &b) { return a - b; }
+  MD_INL static od mul(const od &a, const od &b) { return a * b; }
+  MD_INL static od div(const od &a, const od &b) { return a / b; }
+  MD_INL static od neg(const od &a) { return -a; }
 };
 
 // ------------------------------------------------------------- complex
@@ -375,6 +515,18 @@ MD_INL void str(double *p, const qd &a) {
   reinterpret_cast<double2 *>(p)[0] = make_double2(a.x[0], a.x[1]);
   reinterpret_cast<double2 *>(p)[1] = make_double2(a.x[2], a.x[3]);
 }
+MD_INL void ldr(const double *p, od &a) {
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const double2 v = reinterpret_cast<const double2 *>(p)[i];
+    a.x[2 * i] = v.x;
+    a.x[2 * i + 1] = v.y;
+  }
+}
+MD_INL void str(double *p, const od &a) {
+#pragma unroll
+  for (int i = 0; i < 4; ++i) reinterpret_cast<double2 *>(p)[i] = make_double2(a.x[2 * i], a.x[2 * i + 1]);
+}
 template <class R> MD_INL void ldn(const double *p, R &a) { ldr(p, a); }
 template <class R> MD_INL void ldn(const double *p, cx<R> &a) {
   ldr(p, a.re);
@@ -392,6 +544,12 @@ MD_INL dd shfl_xor(dd a, int m) { return mk(shfl_xor(a.hi, m), shfl_xor(a.lo, m)
 MD_INL qd shfl_xor(const qd &a, int m) {
   return mkq(shfl_xor(a.x[0], m), shfl_xor(a.x[1], m), shfl_xor(a.x[2], m), shfl_xor(a.x[3], m));
 }
+MD_INL od shfl_xor(const od &a, int m) {
+  od r;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) r.x[i] = shfl_xor(a.x[i], m);
+  return r;
+}
 template <class R> MD_INL cx<R> shfl_xor(const cx<R> &a, int m) {
   cx<R> r;
   r.re = shfl_xor(a.re, m);
@@ -401,6 +559,12 @@ template <class R> MD_INL cx<R> shfl_xor(const cx<R> &a, int m) {
 MD_INL double shfl(double a, int src) { return __shfl_sync(0xffffffffu, a, src); }
 MD_INL dd shfl(dd a, int s) { return mk(shfl(a.hi, s), shfl(a.lo, s)); }
 MD_INL qd shfl(const qd &a, int s) { return mkq(shfl(a.x[0], s), shfl(a.x[1], s), shfl(a.x[2], s), shfl(a.x[3], s)); }
+MD_INL od shfl(const od &a, int s) {
+  od r;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) r.x[i] = shfl(a.x[i], s);
+  return r;
+}
 template <class R> MD_INL cx<R> shfl(const cx<R> &a, int s) {
   cx<R> r;
   r.re = shfl(a.re, s);

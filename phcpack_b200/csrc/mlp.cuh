@@ -46,7 +46,7 @@ __host__ __device__ inline MlpView mlp_view(const void *base) {
 //   f[20..23] log max_i |c_ik| for k = 0..3
 // Orders beyond K repeat the last one.  Every thread of the CTA calls it
 // with its number tid; threads 0..12 compute a share each.
-__device__ inline void track_features(int tid, int n, int K, double t, double pole_step, const double *mag,
+__device__ __forceinline__ void track_features(int tid, int n, int K, double t, double pole_step, const double *mag,
                                       float *f) {
   const double tiny = 1e-300;
   if (tid < 8) {
@@ -79,7 +79,7 @@ __device__ inline void track_features(int tid, int n, int K, double t, double po
 // CTA-wide forward pass for one sample (every thread of the block calls
 // it; blockDim.x >= 128).  hbuf: shared scratch of 2*128 floats + 8.
 // Returns log(step / pole_step) to every thread.
-__device__ inline float mlp_forward_cta(const void *model, const float *feat, float *hbuf) {
+__device__ __forceinline__ float mlp_forward_cta(const void *model, const float *feat, float *hbuf) {
   const MlpView M = mlp_view(model);
   const int j = threadIdx.x;
   float *h1 = hbuf, *h2 = hbuf + kMlpH, *red = hbuf + 2 * kMlpH;

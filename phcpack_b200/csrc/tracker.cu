@@ -19,7 +19,7 @@
 //   the step size comes from a learned model when one is given (step_mode
 //     1): a proposal whose corrector fails is rejected and the step is
 //     redone with the plain pole step;
-//   at t = 1: refinement in RN precision (double-double or quad-double) and
+//   at t = 1: refinement in RN precision (double-, quad- or octo-double) and
 //     classification by the max-norm residual.
 // Every loop is bounded (maxsteps, halvings down to minsize); nothing waits.
 #include "common.cuh"
@@ -485,15 +485,18 @@ __global__ void __launch_bounds__(kTrackThreads, (track_min_blocks<PN, RN>::valu
       res = point_residual<RN>(S, s, n, t, xr, sm + L.hc, sm + L.Vc, sm + L.Gc, red);
       status = failed ? 1 : 2;
     }
-    for (int q = ctid(); q < n_max * 8; q += blockDim.x) {
-      const int i = q / 8, c = q % 8;
+    // end points as complex quad-doubles (octo-doubles for an octo-double
+    // refinement), lower limbs zero below the refinement precision
+    const int XL = RN::tr::limbs > 4 ? 8 : 4;
+    for (int q = ctid(); q < n_max * 2 * XL; q += blockDim.x) {
+      const int i = q / (2 * XL), c = q % (2 * XL);
       double v = 0.0;
       if (i < n) {
         const int lim = RN::tr::limbs;
-        const int part = c / 4, limb = c % 4;
+        const int part = c / XL, limb = c % XL;
         if (limb < lim) v = xr[(long)i * RN::width + part * lim + limb];
       }
-      xend[((long)path * n_max) * 8 + q] = v;
+      xend[((long)path * n_max) * 2 * XL + q] = v;
     }
     if (ctid() == 0) {
       info[3 * path] = status;
@@ -556,7 +559,7 @@ int track(const TrackDev &S, const TrackParDev &P, int nmono_max, int npaths, co
           int pmode, int rmode, const void *model, double *xend, int *info, double *dinfo, float *log, int log_cap,
           int *log_count, int *queue, int one_per_launch, cudaStream_t st) {
   PHC_REQUIRE(pmode == 1 || pmode == 2, "track: predictor precision %d not in {1,2}", pmode);
-  PHC_REQUIRE(rmode == 2 || rmode == 4, "track: refinement precision %d not in {2,4}", rmode);
+  PHC_REQUIRE(rmode == 2 || rmode == 4 || rmode == 8, "track: refinement precision %d not in {2,4,8}", rmode);
   PHC_REQUIRE(S.maxdim >= 1 && S.maxdim <= 32, "track: dimension %d not in [1,32]", S.maxdim);
   PHC_REQUIRE(P.deg >= 3 && P.deg <= kTrackKmax && P.numdeg + P.dendeg == P.deg && P.dendeg <= 8 && P.nit >= 1,
               "track: need 3 <= deg = numdeg + dendeg <= %d, dendeg <= 8", kTrackKmax);
@@ -566,6 +569,12 @@ int track(const TrackDev &S, const TrackParDev &P, int nmono_max, int npaths, co
   typedef md::num<double, true> Z1;
   typedef md::num<md::dd, true> Z2;
   typedef md::num<md::qd, true> Z4;
+  typedef md::num<md::od, true> Z8;
+  if (rmode == 8)
+    return pmode == 1 ? track_launch<Z1, Z2, Z8>(S, P, nmono_max, npaths, path_sys, x0, model, xend, info, dinfo, log,
+                                                 log_cap, log_count, queue, one_per_launch, st)
+                      : track_launch<Z2, Z2, Z8>(S, P, nmono_max, npaths, path_sys, x0, model, xend, info, dinfo, log,
+                                                 log_cap, log_count, queue, one_per_launch, st);
   if (pmode == 1 && rmode == 2)
     return track_launch<Z1, Z2, Z2>(S, P, nmono_max, npaths, path_sys, x0, model, xend, info, dinfo, log, log_cap,
                                     log_count, queue, one_per_launch, st);

@@ -8,15 +8,17 @@
 
 namespace phc {
 
-// TRACK_OUTLINE=1 compiles the large CTA-level routines as calls instead of
-// inlining them at every call site (less code for the instruction cache).
+// The large CTA-level routines are inlined at every call site (a routine
+// shared by several kernel instantiations would otherwise become a call,
+// with registers spilled around it); TRACK_OUTLINE=1 compiles them as calls
+// instead (less code for the instruction cache).
 #ifndef TRACK_OUTLINE
 #define TRACK_OUTLINE 0
 #endif
 #if TRACK_OUTLINE
 #define TRACK_FN __noinline__
 #else
-#define TRACK_FN
+#define TRACK_FN __forceinline__
 #endif
 
 static const int kTrackThreads = 128;
@@ -35,7 +37,7 @@ __shared__ int track_rot;
 
 __device__ __forceinline__ int ctid() { return (threadIdx.x + track_rot) & (kTrackThreads - 1); }
 
-__device__ inline void track_pick_lead() {
+__device__ __forceinline__ void track_pick_lead() {
   __shared__ int slot[kTrackThreads / 32];
   const int nw = kTrackThreads / 32;
   if ((threadIdx.x & 31) == 0) {
@@ -114,6 +116,16 @@ template <> struct conv_num<md::num<md::dd, true>, md::num<md::qd, true> > {
     md::cx<md::qd> r;
     r.re = md::mkq(a.re.hi, a.re.lo, 0.0, 0.0);
     r.im = md::mkq(a.im.hi, a.im.lo, 0.0, 0.0);
+    return r;
+  }
+};
+template <> struct conv_num<md::num<md::dd, true>, md::num<md::od, true> > {
+  __device__ __forceinline__ static md::cx<md::od> go(const md::cx<md::dd> &a) {
+    md::cx<md::od> r;
+    r.re = md::mko(a.re.hi);
+    r.re.x[1] = a.re.lo;
+    r.im = md::mko(a.im.hi);
+    r.im.x[1] = a.im.lo;
     return r;
   }
 };

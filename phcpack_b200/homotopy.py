@@ -260,24 +260,31 @@ def subset(pb: TrackProblem, paths) -> TrackProblem:
 
 @dataclass
 class TrackResult:
-    xend: np.ndarray    # npaths x maxdim x 8 (complex quad-double limbs)
+    xend: np.ndarray    # npaths x maxdim x 2 x limbs (complex quad-double limbs; octo-double for rmode 8)
     status: np.ndarray
     steps: np.ndarray
     rejected: np.ndarray
     t: np.ndarray
     residual: np.ndarray
+    limbs: int = 4
 
     def endpoints(self, maxdim):
         """complex128 end points (leading limbs)"""
-        a = self.xend.reshape(-1, maxdim, 8)
-        return (a[..., 0] + a[..., 1]) + 1j * (a[..., 4] + a[..., 5])
+        a = self.xend.reshape(-1, maxdim, 2 * self.limbs)
+        L = self.limbs
+        return (a[..., 0] + a[..., 1]) + 1j * (a[..., L] + a[..., L + 1])
 
 
-def _result(xend, info, dinfo):
+def xend_limbs(rmode):
+    """Limbs per part of an end point coordinate in xend."""
+    return 8 if rmode == 8 else 4
+
+
+def _result(xend, info, dinfo, limbs=4):
     info = info.reshape(-1, 3)
     dinfo = dinfo.reshape(-1, 2)
     return TrackResult(xend, info[:, 0].copy(), info[:, 1].copy(), info[:, 2].copy(), dinfo[:, 0].copy(),
-                       dinfo[:, 1].copy())
+                       dinfo[:, 1].copy(), limbs)
 
 
 def track_host(pb: TrackProblem, pmode=1, rmode=2, step_mode=0, model=None, stream_ptr=0, **kw) -> TrackResult:
@@ -285,7 +292,7 @@ def track_host(pb: TrackProblem, pmode=1, rmode=2, step_mode=0, model=None, stre
     of gpumanypaths_dd: start solutions in, end points and per-path status
     out.  stream_ptr: a cudaStream_t as an int (0 = default stream)."""
     ipar, dpar = params(**kw)
-    xend = np.zeros(pb.npaths * pb.maxdim * 8)
+    xend = np.zeros(pb.npaths * pb.maxdim * 2 * xend_limbs(rmode))
     info = np.zeros(pb.npaths * 3, np.int32)
     dinfo = np.zeros(pb.npaths * 2)
     m = np.ascontiguousarray(model) if model is not None else None
@@ -294,7 +301,7 @@ def track_host(pb: TrackProblem, pmode=1, rmode=2, step_mode=0, model=None, stre
               _lib.ptr(pb.term_mono), _lib.ptr(pb.term_a), _lib.ptr(pb.term_b), pb.npaths, _lib.ptr(pb.path_sys),
               _lib.ptr(pb.x0), _lib.ptr(ipar), _lib.ptr(dpar), pmode, rmode, step_mode, _lib.ptr(m),
               _lib.ptr(xend), _lib.ptr(info), _lib.ptr(dinfo), _lib.c_void_p(stream_ptr))
-    return _result(xend, info, dinfo)
+    return _result(xend, info, dinfo, xend_limbs(rmode))
 
 
 def gather_lists(pb: TrackProblem):
@@ -327,7 +334,8 @@ class DeviceTracker:
                                                     "term_off", "term_mono", "term_a", "term_b", "path_sys", "x0")}
         self.arr["jg_off"], self.arr["jg_term"], self.arr["jg_slot"] = (t(a) for a in jg[:3])
         self.gstaged = int(jg[3])
-        self.xend = torch.zeros(pb.npaths * pb.maxdim * 8, dtype=torch.float64, device=device)
+        self.xend = torch.zeros(pb.npaths * pb.maxdim * 16, dtype=torch.float64, device=device)  # room for rmode 8
+        self.rmode = 2
         self.info = torch.zeros(pb.npaths * 3, dtype=torch.int32, device=device)
         self.dinfo = torch.zeros(pb.npaths * 2, dtype=torch.float64, device=device)
         self.queue = torch.zeros(1, dtype=torch.int32, device=device)
@@ -347,6 +355,7 @@ class DeviceTracker:
         s = 0 if stream is None else stream.cuda_stream
         if self.log is not None:
             self.log_count.zero_()
+        self.rmode = rmode
         _lib.call("phc_track", pb.nsys, _lib.ptr(a["dim"]), pb.maxvar, pb.maxdim, pb.nmono_max, _lib.ptr(a["mono_off"]),
                   _lib.ptr(a["mono_nvr"]), _lib.ptr(a["mono_idx"]), _lib.ptr(a["mono_exp"]), _lib.ptr(a["eq_off"]),
                   _lib.ptr(a["term_off"]), _lib.ptr(a["term_mono"]), _lib.ptr(a["term_a"]), _lib.ptr(a["term_b"]),
@@ -359,4 +368,6 @@ class DeviceTracker:
         return pb.npaths if one_per_launch else 1
 
     def result(self) -> TrackResult:
-        return _result(self.xend.cpu().numpy(), self.info.cpu().numpy(), self.dinfo.cpu().numpy())
+        L = xend_limbs(self.rmode)
+        xe = self.xend[:self.pb.npaths * self.pb.maxdim * 2 * L].cpu().numpy()
+        return _result(xe, self.info.cpu().numpy(), self.dinfo.cpu().numpy(), L)

@@ -376,8 +376,8 @@ def manypaths(target, start=None, start_solutions=None, gamma=None, rmode=2, pmo
               seed=0, **kw):
     """Track all paths of (1 - t) gamma q + t p from the start solutions of
     q to p on the GPU, in PHCpack's text formats: the counterpart of
-    gpumanypaths_dd (rmode 2) and gpumanypaths_qd (rmode 4) with the
-    containers replaced by text.  target, start: systems (text); without a
+    gpumanypaths_dd (rmode 2) and gpumanypaths_qd (rmode 4), and an
+    octo-double refinement (rmode 8), with the containers replaced by text.  target, start: systems (text); without a
     start system the total-degree start system x_i^{d_i} - 1 and all its
     roots-of-unity solutions are used.  gamma: complex (default: random on
     the unit circle from seed).  Returns (solution list text of the end
@@ -400,8 +400,8 @@ def manypaths(target, start=None, start_solutions=None, gamma=None, rmode=2, pmo
     pb = hm.homotopy_problem([(polys, q)], gamma, [(0, x) for x in xs])
     r = hm.track_host(pb, pmode=pmode, rmode=rmode, step_mode=step_mode, model=model, **kw)
     n = len(symbols)
-    nl = 2 if rmode == 2 else 4
-    xe = r.xend.reshape(pb.npaths, pb.maxdim, 2, 4)[:, :n, :, :nl]
+    nl = rmode
+    xe = r.xend.reshape(pb.npaths, pb.maxdim, 2, r.limbs)[:, :n, :, :nl]
     sols = []
     for p in range(pb.npaths):
         x = r.endpoints(pb.maxdim)[p, :n]
@@ -415,4 +415,4 @@ def manypaths(target, start=None, start_solutions=None, gamma=None, rmode=2, pmo
         # a successful path's end point is refined at t = 1 exactly
         t_end = 1.0 if r.status[p] == 0 else float(r.t[p])
         sols.append(dict(t=complex(t_end), m=1, x=xe[p], err=err, rco=rco, res=float(r.residual[p])))
-    return write_solutions(sols, symbols, digits=32 if rmode == 2 else 64), r
+    return write_solutions(sols, symbols, digits={2: 32, 4: 64, 8: 128}[rmode]), r

@@ -74,5 +74,33 @@ def main():
              cplx=int(cplx), n=n, degp1=degp1)
 
 
+def make_od():
+    """Octo-double add, mul, div and multiply-by-double of the reference
+    (Norms/octo_double_functions.cpp) on seeded random normalised inputs."""
+    ref = pyoracle.reference()
+    if ref is None:
+        raise SystemExit("the reference tree is not available here")
+    rng = np.random.default_rng(31)
+    n = 256
+
+    def rand_od():
+        out = np.zeros((n, 8))
+        for k in range(n):
+            limbs = [rng.standard_normal() * 10.0 ** rng.integers(-8, 8)]
+            for _ in range(7):
+                limbs.append(limbs[-1] * 2.0 ** -53 * rng.uniform(-1, 1))
+            out[k] = limbs
+        return ref.od_binop(0, out, np.zeros((n, 8)))  # renormalised by the reference's odf_add
+
+    a, b = rand_od(), rand_od()
+    save("od_ops", a=a, b=b, add=ref.od_binop(0, a, b), mul=ref.od_binop(1, a, b), div=ref.od_binop(2, a, b),
+         mul_d=ref.od_binop(3, a, b))
+
+
 if __name__ == "__main__":
-    main()
+    import sys
+    if sys.argv[1:] == ["od"]:
+        make_od()
+    else:
+        main()
+        make_od()

@@ -71,3 +71,30 @@ def test_eval_oracle_vs_reference_fresh(prec, cplx):
     out = ORC.system_evaldiff(b)
     scale = ORC.system_evaldiff(abs_batch(b))
     assert check_scaled(out, ref, scale, prec, cplx, tol(prec)) <= 1.0
+
+
+def test_od_oracle_vs_golden():
+    """Octo-double add, mul, div and multiply-by-double of the oracle equal the
+    reference's (Norms/octo_double_functions.cpp) bit for bit."""
+    import os
+    d = np.load(os.path.join(os.path.dirname(__file__), "golden", "od_ops.npz"))
+    a, b = d["a"], d["b"]
+    for op, key in enumerate(("add", "mul", "div", "mul_d")):
+        assert np.array_equal(ORC.od_binop(op, a, b), d[key]), key
+
+
+def test_od_oracle_vs_reference_fresh():
+    ref = pyoracle.reference()
+    if ref is None:
+        pytest.skip("the reference tree is not available here")
+    rng = np.random.default_rng(77)
+    raw = np.zeros((500, 8))
+    for k in range(500):
+        limbs = [rng.standard_normal() * 10.0 ** rng.integers(-20, 20)]
+        for _ in range(7):
+            limbs.append(limbs[-1] * 2.0 ** -53 * rng.uniform(-1, 1))
+        raw[k] = limbs
+    a = ref.od_binop(0, raw, np.zeros_like(raw))
+    b = ref.od_binop(0, raw[::-1].copy(), np.zeros_like(raw))
+    for op in range(4):
+        assert np.array_equal(ORC.od_binop(op, a, b), ref.od_binop(op, a, b)), op

@@ -12,14 +12,17 @@ from phcpack_b200 import phcio
 pytestmark = pytest.mark.gpu
 
 
-def _inv_sqrt2(digits=80):
+def _inv_sqrt2(digits=160):
     getcontext().prec = digits
     return Fraction(Decimal(1) / Decimal(2).sqrt())
 
 
-@pytest.mark.parametrize("rmode,tol", [(2, 1e-30), (4, 1e-60)])
-def test_circle_and_line_dd_qd(rmode, tol):
-    text, r = phcio.manypaths("2\n x^2 + y^2 - 1;\n x - y;\n", rmode=rmode, restol=1e-24 if rmode == 2 else 1e-48)
+RESTOL = {2: 1e-24, 4: 1e-48, 8: 1e-100}
+
+
+@pytest.mark.parametrize("rmode,tol", [(2, 1e-30), (4, 1e-60), (8, 1e-120)])
+def test_circle_and_line_dd_qd_od(rmode, tol):
+    text, r = phcio.manypaths("2\n x^2 + y^2 - 1;\n x - y;\n", rmode=rmode, restol=RESTOL[rmode])
     assert (r.status == 0).all()
     sols = phcio.parse_solutions(text, symbols=["x", "y"], nlimbs=rmode)
     assert len(sols) == 2
@@ -32,7 +35,7 @@ def test_circle_and_line_dd_qd(rmode, tol):
             re_ = phcio.limbs_to_fraction(s["x"][j, 0])
             im_ = phcio.limbs_to_fraction(s["x"][j, 1])
             assert abs(re_ - sg * c) <= tol and abs(im_) <= tol
-        assert s["t"] == 1.0 and s["res"] <= (1e-24 if rmode == 2 else 1e-48)
+        assert s["t"] == 1.0 and s["res"] <= RESTOL[rmode]
 
 
 def cyclic_text(n):

@@ -15,11 +15,11 @@ pytestmark = pytest.mark.gpu
 ORC = pyoracle.oracle()
 
 
-def endpoint_diff(pb, xa, xb, limbs):
-    a = xa.reshape(-1, pb.maxdim, 8)
-    b = xb.reshape(-1, pb.maxdim, 8)
+def endpoint_diff(pb, xa, xb, limbs, width=4):
+    a = xa.reshape(-1, pb.maxdim, 2 * width)
+    b = xb.reshape(-1, pb.maxdim, 2 * width)
     d = np.zeros(a.shape[:2])
-    for part in (0, 4):
+    for part in (0, width):
         acc = np.zeros(a.shape[:2])
         for l in range(limbs - 1, -1, -1):
             acc = acc + (a[..., part + l] - b[..., part + l])
@@ -52,6 +52,21 @@ def test_track_quad_double_refinement():
     ok = g.status == 0
     assert ok.all()
     assert (endpoint_diff(pb, g.xend, xo, 4)[ok] <= 1e-50).all()
+
+
+def test_track_octo_double_refinement():
+    """Octo-double refinement at t = 1 (rmode 8): the same classification as
+    the oracle, end points within 1e-110 of the oracle's, residuals
+    <= 1e-100."""
+    pb = hm.subset(hm.config4(), [3, 150, 600, 1000])
+    ipar, dpar = hm.params(restol=1e-100, refine_steps=6)
+    g = hm.track_host(pb, pmode=1, rmode=8, restol=1e-100, refine_steps=6)
+    xo, io, _ = pyoracle.track(ORC, pb, ipar, dpar, pmode=1, rmode=8)
+    assert np.array_equal(g.status, io.reshape(-1, 3)[:, 0])
+    ok = g.status == 0
+    assert ok.all()
+    assert (g.residual <= 1e-100).all()
+    assert (endpoint_diff(pb, g.xend, xo, 8, width=8)[ok] <= 1e-110).all()
 
 
 def test_one_path_per_launch_matches_batched():
