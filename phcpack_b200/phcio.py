@@ -373,17 +373,21 @@ def _eval_jac(polys, x):
 
 
 def manypaths(target, start=None, start_solutions=None, gamma=None, rmode=2, pmode=1, step_mode=0, model=None,
-              seed=0, **kw):
+              seed=0, partition=None, **kw):
     """Track all paths of (1 - t) gamma q + t p from the start solutions of
     q to p on the GPU, in PHCpack's text formats: the counterpart of
     gpumanypaths_dd (rmode 2) and gpumanypaths_qd (rmode 4), and an
-    octo-double refinement (rmode 8), with the containers replaced by text.  target, start: systems (text); without a
-    start system the total-degree start system x_i^{d_i} - 1 and all its
-    roots-of-unity solutions are used.  gamma: complex (default: random on
-    the unit circle from seed).  Returns (solution list text of the end
-    points at t = 1, the TrackResult).  err is the forward error estimate
-    |J^{-1}|_inf * res and rco the reciprocal 1-norm condition number of the
-    Jacobian at the end point (both in double)."""
+    octo-double refinement (rmode 8), with the containers replaced by text.
+    target, start: systems (text).  Without a start system the total-degree
+    start system x_i^{d_i} - 1 and all its roots-of-unity solutions are
+    used; start="linear-product" builds a random linear-product start system
+    and all its roots for a partition of the variables (partition: lists of
+    variable names; default the partition with the smallest m-homogeneous
+    Bezout number, phcpack_b200.rootcounts).  gamma: complex (default:
+    random on the unit circle from seed).  Returns (solution list text of
+    the end points at t = 1, the TrackResult).  err is the forward error
+    estimate |J^{-1}|_inf * res and rco the reciprocal 1-norm condition
+    number of the Jacobian at the end point (both in double)."""
     polys, symbols = parse_system(target)
     if len(polys) != len(symbols):
         raise ParseError("the tracker needs as many polynomials as variables")
@@ -392,6 +396,13 @@ def manypaths(target, start=None, start_solutions=None, gamma=None, rmode=2, pmo
     if start is None:
         q, degs = hm.total_degree_start(polys)
         xs = hm.total_degree_solutions(degs)
+    elif start == "linear-product":
+        from . import rootcounts
+        if partition is None:
+            part, _ = rootcounts.best_partition(polys, len(symbols))
+        else:
+            part = [[symbols.index(v) for v in st] for st in partition]
+        q, xs, _ = rootcounts.linear_product_start(polys, part, np.random.default_rng(seed + 1))
     else:
         q, _ = parse_system(start, symbols=list(symbols))
         if start_solutions is None:

@@ -2,7 +2,9 @@
 example systems (src/Demo of the PHCpack tree): every file is parsed, the
 product of the degrees is compared with the total degree the file states,
 and the solution lists that files carry are read back (by variable name)
-and the end points at t = 1 evaluated in the parsed system.  The summary goes to
+and the end points at t = 1 evaluated in the parsed system; the
+m-homogeneous Bezout numbers the files state for a partition of the
+variables are recomputed (phcpack_b200.rootcounts).  The summary goes to
 tests/golden/phcio_demo.json; tests/test_phcio.py checks it.
 
 Run from the repository root with the reference tree at hand:
@@ -16,7 +18,7 @@ import sys
 import numpy as np
 
 sys.path.insert(0, os.path.join(os.path.dirname(__file__), "..", ".."))
-from phcpack_b200 import phcio, homotopy as hm  # noqa: E402
+from phcpack_b200 import phcio, homotopy as hm, rootcounts  # noqa: E402
 
 
 def stated_total_degree(text):
@@ -58,6 +60,17 @@ def main(root):
         rec["degrees"] = [hm.degree(p) for p in polys]
         rec["total_degree"] = int(np.prod(rec["degrees"]))
         rec["stated_total_degree"] = stated_total_degree(text)
+        mh = []
+        for m in re.finditer(r"(\d+)-homogeneous Bezout number\s*:\s*([\d,]+)\s*\n\s*with partition\s*:\s*(\{.*\})",
+                             text):
+            sets = [st.split() for st in re.findall(r"\{([^{}]*)\}", m.group(3)) if st.strip()]
+            if sorted(v for st in sets for v in st) != sorted(sym):
+                continue  # a partition line that does not list every variable
+            part = [[sym.index(v) for v in st] for st in sets]
+            mh.append({"m": int(m.group(1)), "partition": sets, "stated": int(m.group(2).replace(",", "")),
+                       "computed": rootcounts.bezout_number(polys, part)})
+        if mh:
+            rec["mhom_bezout"] = mh
         k = text.find("THE SOLUTIONS")
         if k >= 0:
             body = text[k:].split("\n", 1)[1]

@@ -168,3 +168,43 @@ def test_explicit_total_degree_start_matches_builder():
     for k in ("dim", "mono_off", "mono_nvr", "mono_idx", "mono_exp", "eq_off", "term_off", "term_mono", "term_a",
               "term_b", "path_sys", "x0"):
         assert np.array_equal(getattr(a, k), getattr(b, k)), k
+
+
+def test_mhom_bezout_numbers_match_the_reference_demo_statements():
+    d = json.load(open(GOLDEN))
+    stated = [x for v in d.values() for x in v.get("mhom_bezout", [])]
+    assert len(stated) >= 60
+    assert all(x["computed"] == x["stated"] for x in stated)
+
+
+def eigen_text(A, c):
+    """(A - lam I) v = 0, c . v = 1: n + 1 equations in v1..vn, lam."""
+    n = A.shape[0]
+    rows = []
+    for i in range(n):
+        terms = [f"({float(A[i, j].real)!r} + {float(A[i, j].imag)!r}*i)*v{j + 1}" for j in range(n)]
+        rows.append(" + ".join(terms) + f" - lam*v{i + 1};")
+    rows.append(" + ".join(f"({float(c[j].real)!r} + {float(c[j].imag)!r}*i)*v{j + 1}" for j in range(n)) + " - 1;")
+    return f"{n + 1}\n" + "\n".join(rows) + "\n"
+
+
+def test_linear_product_start_system():
+    from phcpack_b200 import rootcounts
+    rng = np.random.default_rng(4)
+    n = 4
+    A = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    c = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    polys, sym = phcio.parse_system(eigen_text(A, c))
+    lam = sym.index("lam")
+    vs = [k for k in range(len(sym)) if k != lam]
+    assert rootcounts.bezout_number(polys, [list(range(len(sym)))]) == 2 ** n
+    assert rootcounts.bezout_number(polys, [[lam], vs]) == n
+    part, b = rootcounts.best_partition(polys, len(sym))
+    assert b == n and sorted(map(sorted, part)) == sorted([[lam], sorted(vs)])
+    q, roots, _ = rootcounts.linear_product_start(polys, part, np.random.default_rng(0))
+    assert len(roots) == n
+    for x in roots:
+        for poly in q:
+            v = sum(cf * np.prod([x[j] ** e for j, e in m]) for m, cf in poly)
+            assert abs(v) <= 1e-10
+    assert np.min(np.abs(np.subtract.outer(np.array(roots)[:, 0], np.array(roots)[:, 0])) + np.eye(n)) > 1e-8

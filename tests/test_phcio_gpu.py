@@ -75,3 +75,29 @@ def test_given_start_system_and_solutions_match_total_degree():
     t2, r2 = phcio.manypaths(target, start, start_sols, gamma=g)
     assert np.array_equal(r1.status, r2.status)
     assert np.abs(r1.endpoints(3) - r2.endpoints(3)).max() <= 1e-28
+
+
+def test_linear_product_start_eigenproblem():
+    """(A - lam I) v = 0, c . v = 1 has total degree 2^n but n solutions, the
+    2-homogeneous Bezout number for the partition {lam}{v}: tracked from a
+    linear-product start system, every path converges and the lam
+    coordinates are the eigenvalues of A."""
+    rng = np.random.default_rng(6)
+    n = 6
+    A = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    c = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    rows = []
+    for i in range(n):
+        terms = [f"({float(A[i, j].real)!r} + {float(A[i, j].imag)!r}*i)*v{j + 1}" for j in range(n)]
+        rows.append(" + ".join(terms) + f" - lam*v{i + 1};")
+    rows.append(" + ".join(f"({float(c[j].real)!r} + {float(c[j].imag)!r}*i)*v{j + 1}" for j in range(n)) + " - 1;")
+    target = f"{n + 1}\n" + "\n".join(rows) + "\n"
+    text, r = phcio.manypaths(target, start="linear-product")
+    assert r.status.shape == (n,) and (r.status == 0).all()
+    polys, sym = phcio.parse_system(target)
+    sols = phcio.parse_solutions(text, symbols=sym)
+    lam = sym.index("lam")
+    got = np.sort_complex(np.array([s["x"][lam] for s in sols]))
+    want = np.sort_complex(np.linalg.eigvals(A))
+    assert np.abs(got - want).max() <= 1e-10
+    assert all(s["res"] <= 1e-24 for s in sols)
