@@ -351,9 +351,67 @@ def write_solutions(sols, symbols, digits=32):
             else:
                 re_, im_ = x[j, 0], x[j, 1]
             out.append(f" {symbols[j]} : {format_number(re_, digits)}  {format_number(im_, digits)}")
+        kind = f" {s['kind']} ==" if "kind" in s else "="
         out.append("== err : " + f"{s.get('err', 0.0): .3E}" + " = rco : " + f"{s.get('rco', 1.0): .3E}" +
-                   " = res : " + f"{s.get('res', 0.0): .3E}" + " ==")
+                   " = res : " + f"{s.get('res', 0.0): .3E}" + " =" + kind)
     return "\n".join(out) + "\n"
+
+
+# ----------------------------------------------------------- root accounting
+
+def root_accounting(sols, fail, tolsing=1e-8, tolclus=1e-12, tolreal=1e-13, infinity=1e8):
+    """Classify end points as PHCpack's root refiners do (Write_Type and
+    Multiplicity of Deformations/Newton/dobldobl_root_refiners.adb:53-111,
+    At_Infinity and Is_Real of Solutions/dobldobl_solution_diagnostics.adb):
+    a coordinate above `infinity` in modulus puts the point at infinity; a
+    failed path is "no solution" (m = 0); otherwise the point is real when
+    every imaginary part is at most tolreal, singular when rco < tolsing.  A
+    singular point's multiplicity is the number of points equal to it within
+    tolclus per coordinate (0 when it stands alone); regular points that
+    coincide are marked clustered with m = -(index of the other, 1-based).
+    Sets s["kind"] and s["m"] in place; returns the counts of
+    Write_Global_Info."""
+    pts = [np.asarray(s["x"]) for s in sols]
+    pts = [p if p.ndim == 1 else p[:, 0, 0] + 1j * p[:, 1, 0] for p in pts]
+    cnt = dict(total=len(sols), regular=0, singular=0, real=0, complex=0, clustered=0, infinity=0, failures=0)
+
+    def equal(a, b):
+        return bool(np.all(np.abs(a - b) <= tolclus))
+
+    for k, s in enumerate(sols):
+        x = pts[k]
+        if np.any(~np.isfinite(x)) or np.any(np.abs(x) > infinity):
+            s["kind"] = "at infinity"
+            cnt["infinity"] += 1
+            continue
+        if fail[k]:
+            s["kind"] = "no solution"
+            s["m"] = 0
+            cnt["failures"] += 1
+            continue
+        real = bool(np.all(np.abs(x.imag) <= tolreal))
+        singular = s.get("rco", 1.0) < tolsing
+        cnt["real" if real else "complex"] += 1
+        cnt["singular" if singular else "regular"] += 1
+        s["kind"] = ("real " if real else "complex ") + ("singular" if singular else "regular")
+        others = [j for j in range(len(sols)) if j != k and not fail[j] and equal(x, pts[j])]
+        if singular:
+            s["m"] = len(others) + 1 if others else 0
+        elif others:
+            s["m"] = -(others[0] + 1)
+            cnt["clustered"] += 1
+    return cnt
+
+
+def accounting_text(cnt):
+    """The summary PHCpack writes after refining (Write_Global_Info)."""
+    bar = "=" * 75
+    rows = [("regular solutions", "regular"), ("singular solutions", "singular"), ("real solutions", "real"),
+            ("complex solutions", "complex"), ("clustered solutions", "clustered"),
+            ("solutions at infinity", "infinity"), ("failures", "failures")]
+    out = [bar, f"A list of {cnt['total']} solutions has been refined :"]
+    out += [f"Number of {name:<22}: {cnt[key]}." for name, key in rows]
+    return "\n".join(out + [bar]) + "\n"
 
 
 # ----------------------------------------------------------- the driver
@@ -385,9 +443,12 @@ def manypaths(target, start=None, start_solutions=None, gamma=None, rmode=2, pmo
     variable names; default the partition with the smallest m-homogeneous
     Bezout number, phcpack_b200.rootcounts).  gamma: complex (default:
     random on the unit circle from seed).  Returns (solution list text of
-    the end points at t = 1, the TrackResult).  err is the forward error
-    estimate |J^{-1}|_inf * res and rco the reciprocal 1-norm condition
-    number of the Jacobian at the end point (both in double)."""
+    the end points at t = 1, the TrackResult with the counts of
+    root_accounting in its `accounting` attribute).  err is the forward
+    error estimate |J^{-1}|_inf * res and rco the reciprocal 1-norm
+    condition number of the Jacobian at the end point (both in double); the
+    diagnostics line of each solution carries its kind ("complex regular",
+    "at infinity", ...)."""
     polys, symbols = parse_system(target)
     if len(polys) != len(symbols):
         raise ParseError("the tracker needs as many polynomials as variables")
@@ -426,4 +487,5 @@ def manypaths(target, start=None, start_solutions=None, gamma=None, rmode=2, pmo
         # a successful path's end point is refined at t = 1 exactly
         t_end = 1.0 if r.status[p] == 0 else float(r.t[p])
         sols.append(dict(t=complex(t_end), m=1, x=xe[p], err=err, rco=rco, res=float(r.residual[p])))
+    r.accounting = root_accounting(sols, r.status != 0)
     return write_solutions(sols, symbols, digits={2: 32, 4: 64, 8: 128}[rmode]), r

@@ -208,3 +208,28 @@ def test_linear_product_start_system():
             v = sum(cf * np.prod([x[j] ** e for j, e in m]) for m, cf in poly)
             assert abs(v) <= 1e-10
     assert np.min(np.abs(np.subtract.outer(np.array(roots)[:, 0], np.array(roots)[:, 0])) + np.eye(n)) > 1e-8
+
+
+def test_root_accounting():
+    sols = [
+        dict(x=np.array([1.0 + 0j, -2.0 + 1e-15j]), rco=0.3, res=1e-30),          # real regular
+        dict(x=np.array([1.0 + 1j, 2.0 + 0j]), rco=1e-12, res=1e-30),            # complex singular, with #3
+        dict(x=np.array([1.0 + 1j, 2.0 + 1e-14j]), rco=1e-11, res=1e-30),        # complex singular, with #2
+        dict(x=np.array([3.0 + 1j, 4.0 + 0j]), rco=0.2, res=1e-30),              # complex regular, clustered
+        dict(x=np.array([3.0 + 1j, 4.0 + 0j]), rco=0.2, res=1e-30),              # complex regular, clustered
+        dict(x=np.array([1e9 + 0j, 1.0 + 0j]), rco=0.1, res=1.0),                # at infinity
+        dict(x=np.array([0.5 + 0.5j, 0.1 + 0j]), rco=0.1, res=1e-3),             # failed path
+        dict(x=np.array([7.0 + 0j, 5.0 - 3j]), rco=1e-9, res=1e-30),             # complex singular, alone
+    ]
+    fail = np.array([0, 0, 0, 0, 0, 1, 1, 0], bool)
+    cnt = phcio.root_accounting(sols, fail)
+    kinds = [s["kind"] for s in sols]
+    assert kinds == ["real regular", "complex singular", "complex singular", "complex regular", "complex regular",
+                     "at infinity", "no solution", "complex singular"]
+    assert [s.get("m") for s in sols] == [None, 2, 2, -5, -4, None, 0, 0]
+    assert cnt == dict(total=8, regular=3, singular=3, real=1, complex=5, clustered=2, infinity=1, failures=1)
+    text = phcio.write_solutions([dict(s, t=1.0) for s in sols], ["x", "y"], digits=20)
+    assert "= res :  1.000E-30 = real regular ==" in text and "= at infinity ==" in text
+    back = phcio.parse_solutions(text, symbols=["x", "y"])
+    assert [b["m"] for b in back][:3] == [1, 2, 2]
+    assert "Number of solutions at infinity : 1." in phcio.accounting_text(cnt)

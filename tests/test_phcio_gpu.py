@@ -61,6 +61,11 @@ def test_cyclic5_endpoints():
     # distinct roots among the successes
     d = np.abs(pts[:, None, :] - pts[None, :, :]).max(axis=2) + np.eye(len(ok))
     assert (d > 1e-6).all()
+    # root accounting: the successes are regular roots, the rest diverged
+    a = r.accounting
+    assert a["regular"] == len(ok) and a["singular"] == 0 and a["clustered"] == 0
+    assert a["regular"] + a["infinity"] + a["failures"] == 120
+    assert all(sols[p]["m"] == 1 for p in ok)
 
 
 def test_given_start_system_and_solutions_match_total_degree():
