@@ -219,12 +219,16 @@ int phc_track(int nsys, const int *dim, int maxvar, int maxdim, int nmono_max, c
               const void *model, double *xend, int *info, double *dinfo, float *log, int log_cap, int *log_count,
               int *queue, int one_per_launch, void *stream);
 /* Host arrays in and out; returns the number of paths not classified as
- * success (>= 0) or an error (< 0). */
+ * success (>= 0) or an error (< 0).  The device buffer and a pinned staging
+ * buffer are kept per device between calls (grown when needed; inputs go
+ * over in one copy, outputs back in one); calls are serialised;
+ * phc_track_host_release() frees the buffers. */
 int phc_track_host(int nsys, const int *dim, int maxvar, const int *mono_off, const int *mono_nvr,
                    const int *mono_idx, const int *mono_exp, const int *eq_off, const int *term_off,
                    const int *term_mono, const double *term_a, const double *term_b, int npaths,
                    const int *path_sys, const double *x0, const int *ipar, const double *dpar, int pmode, int rmode,
                    int step_mode, const void *model, double *xend, int *info, double *dinfo, void *stream);
+void phc_track_host_release(void);
 /* ------------------------------------------------------- learned step size
  * No counterpart in the reference (its trackers use the ratio / Pade pole
  * and curvature steps only).  A 24 -> 128 -> 128 -> 1 ReLU network predicts

@@ -1,4 +1,6 @@
 // capi_track.cu -- C ABI of the path tracker (include/phc_b200.h).
+#include <cstring>
+#include <mutex>
 #include <vector>
 #include "common.cuh"
 #include "tracker.cuh"
@@ -13,6 +15,21 @@ long track_smem_bytes(int maxdim, int K, int M, int nmono_max, int maxvar, int p
 }  // namespace phc
 
 using namespace phc;
+
+namespace {
+// The device buffer and the pinned staging buffer of phc_track_host, kept
+// per device between calls and grown when a call needs more, so that a
+// call of a size seen before allocates nothing; calls are serialised by the
+// mutex (phc_track_host_release frees the buffers).
+struct HostCallBuffers {
+  void *dev = nullptr;
+  size_t dev_cap = 0;
+  void *pin = nullptr;
+  size_t pin_cap = 0;
+};
+std::mutex g_track_mu;
+HostCallBuffers g_track_buf[64];
+}  // namespace
 
 static TrackParDev make_par(const int *ipar, const double *dpar, int step_mode) {
   TrackParDev P;
@@ -127,20 +144,19 @@ int phc_track_host(int nsys, const int *dim, int maxvar, const int *mono_off, co
   const int staged = phc_track_prepare(nsys, dim, maxvar, mono_off, mono_nvr, mono_idx, mono_exp, eq_off, term_off,
                                        term_mono, maxdim, jg_off.data(), jg_term.data(), jg_slot.data());
   if (staged < 0) return staged;
-  // one device buffer for everything
+  // one device buffer for everything, staged through one pinned host buffer
   std::vector<std::pair<const void *, size_t> > ins = {
       {dim, nsys * 4ul}, {mono_off, (nsys + 1) * 4ul}, {mono_nvr, nmono * 4ul},
       {mono_idx, (size_t)nmono * maxvar * 4}, {mono_exp, (size_t)nmono * maxvar * 4}, {eq_off, (nsys + 1) * 4ul},
       {term_off, (neq + 1) * 4ul}, {term_mono, nterm * 4ul}, {term_a, nterm * 16ul}, {term_b, nterm * 16ul},
       {jg_off.data(), jg_off.size() * 4}, {jg_term.data(), jg_term.size() * 4}, {jg_slot.data(), jg_slot.size() * 4},
-      {path_sys, npaths * 4ul}, {x0, (size_t)npaths * maxdim * 16}, {model, step_mode && model ? 1ul : 0ul}};
-  const size_t model_bytes = (size_t)mlp_model_bytes();
+      {path_sys, npaths * 4ul}, {x0, (size_t)npaths * maxdim * 16},
+      {model, step_mode && model ? (size_t)mlp_model_bytes() : 0ul}};
   size_t total = 0;
   std::vector<size_t> off;
   for (size_t i = 0; i < ins.size(); ++i) {
     off.push_back(total);
-    const size_t b = (i + 1 == ins.size()) ? (ins[i].second ? model_bytes : 0) : ins[i].second;
-    total += (b + 255) & ~size_t(255);
+    total += (ins[i].second + 255) & ~size_t(255);
   }
   const size_t xbytes = (size_t)npaths * maxdim * (rmode == 8 ? 128 : 64);  // complex qd (od) per coordinate
   const size_t o_xend = total;
@@ -151,17 +167,34 @@ int phc_track_host(int nsys, const int *dim, int maxvar, const int *mono_off, co
   total += (((size_t)npaths * 16) + 255) & ~size_t(255);
   const size_t o_q = total;
   total += 256;
-  void *buf = nullptr;
-  PHC_CUDA(cudaMalloc(&buf, total));
-  char *b = (char *)buf;
+  const size_t in_bytes = o_xend, out_bytes = o_q - o_xend;
+  int devid = 0;
+  PHC_CUDA(cudaGetDevice(&devid));
+  std::lock_guard<std::mutex> lock(g_track_mu);
+  HostCallBuffers &hb = g_track_buf[devid & 63];
+  if (hb.dev_cap < total) {
+    if (hb.dev) cudaFree(hb.dev);
+    hb.dev = nullptr;
+    hb.dev_cap = 0;
+    PHC_CUDA(cudaMalloc(&hb.dev, total));
+    hb.dev_cap = total;
+  }
+  const size_t pin_need = in_bytes > out_bytes ? in_bytes : out_bytes;
+  if (hb.pin_cap < pin_need) {
+    if (hb.pin) cudaFreeHost(hb.pin);
+    hb.pin = nullptr;
+    hb.pin_cap = 0;
+    PHC_CUDA(cudaMallocHost(&hb.pin, pin_need));
+    hb.pin_cap = pin_need;
+  }
+  char *b = (char *)hb.dev, *h = (char *)hb.pin;
+  for (size_t i = 0; i < ins.size(); ++i)
+    if (ins[i].second) std::memcpy(h + off[i], ins[i].first, ins[i].second);
   cudaStream_t st = (cudaStream_t)stream;
   int out = PHC_OK;
-  for (size_t i = 0; i < ins.size() && out == PHC_OK; ++i) {
-    const size_t nb = (i + 1 == ins.size()) ? (ins[i].second ? model_bytes : 0) : ins[i].second;
-    if (nb && cudaMemcpyAsync(b + off[i], ins[i].first, nb, cudaMemcpyHostToDevice, st) != cudaSuccess) {
-      set_error("track_host: copy to the device failed");
-      out = PHC_ERR_CUDA;
-    }
+  if (cudaMemcpyAsync(b, h, in_bytes, cudaMemcpyHostToDevice, st) != cudaSuccess) {
+    set_error("track_host: copy to the device failed");
+    out = PHC_ERR_CUDA;
   }
   if (out == PHC_OK) {
     auto I = [&](int i) { return (const int *)(b + off[i]); };
@@ -172,19 +205,35 @@ int phc_track_host(int nsys, const int *dim, int maxvar, const int *mono_off, co
                     (int *)(b + o_info), (double *)(b + o_dinfo), nullptr, 0, nullptr, (int *)(b + o_q), 0, st);
   }
   if (out == PHC_OK) {
-    if (cudaMemcpyAsync(xend, b + o_xend, xbytes, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-        cudaMemcpyAsync(info, b + o_info, (size_t)npaths * 12, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-        cudaMemcpyAsync(dinfo, b + o_dinfo, (size_t)npaths * 16, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+    if (cudaMemcpyAsync(h, b + o_xend, out_bytes, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaStreamSynchronize(st) != cudaSuccess) {
       set_error("track_host: %s", cudaGetErrorString(cudaGetLastError()));
       out = PHC_ERR_CUDA;
+    } else {
+      std::memcpy(xend, h, xbytes);
+      std::memcpy(info, h + (o_info - o_xend), (size_t)npaths * 12);
+      std::memcpy(dinfo, h + (o_dinfo - o_xend), (size_t)npaths * 16);
     }
   }
-  cudaFree(buf);
   if (out < 0) return out;
   int fails = 0;
   for (int p = 0; p < npaths; ++p) fails += info[3 * p] != 0;
   return fails;
+}
+
+void phc_track_host_release(void) {
+  std::lock_guard<std::mutex> lock(g_track_mu);
+  int cur = 0;
+  cudaGetDevice(&cur);
+  for (int d = 0; d < 64; ++d) {
+    HostCallBuffers &hb = g_track_buf[d];
+    if (!hb.dev && !hb.pin) continue;
+    cudaSetDevice(d);
+    if (hb.dev) cudaFree(hb.dev);
+    if (hb.pin) cudaFreeHost(hb.pin);
+    hb = HostCallBuffers();
+  }
+  cudaSetDevice(cur);
 }
 
 }  // extern "C"
