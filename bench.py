@@ -190,10 +190,8 @@ def main():
         dist.barrier()
     total_s = t0.elapsed_time(t1) / 1e3
     kern_s = [ev[k][0].elapsed_time(ev[k][1]) / 1e3 for k in range(args.steps)]
-    ts = torch.tensor([total_s], device=dev)
-    if dist is not None:
-        dist.all_reduce(ts, op=dist.ReduceOp.MAX)
-    total_s = float(ts.item())
+    from phcpack_b200 import multirank
+    total_s = multirank.max_over_ranks(total_s, dist)
 
     if hasattr(work, "finish"):
         work.finish()
