@@ -45,7 +45,10 @@ struct wser {
 
   // z = x*y (x, y series in shared memory); returns the coefficient this
   // lane owns (m.valid) at index m.kout().  All 32 lanes must call it.
-  static __device__ __forceinline__ T conv(const double *x, const double *y, const lanemap &m) {
+  // Compiled once and called (not inlined at its many call sites): the
+  // evaluation kernel is bound by instruction fetch when every call site
+  // carries its own copy of the loop.
+  static __device__ __noinline__ T conv(const double *x, const double *y, const lanemap &m) {
     T a1 = N::zero(), a2 = N::zero();
     for (int s = 0; s < m.steps; ++s) {
       const int t = m.t0 + s;
