@@ -385,6 +385,17 @@ __device__ void block_invert_tiles(int dim, int szt, const double *U, int ldu, d
   __syncthreads();
 }
 
+// Dot products shared by aligned groups of four lanes: output o of a pass
+// is computed by the four lanes 4(o mod 8) .. +3 of warp o / 8, each summing
+// every fourth term, then two xor shuffles add the four partial sums (the
+// chains of dependent multiple-double operations are a quarter as long as
+// with one thread per output).  All lanes of a warp take part in every pass.
+template <class N>
+__device__ __forceinline__ typename N::T group4_sum(typename N::T a) {
+  a = N::add(a, md::shfl_xor(a, 1));
+  return N::add(a, md::shfl_xor(a, 2));
+}
+
 // x = U^{-1} b with the inverted diagonal tiles: for k = nbt-1..0,
 // x_k = Tinv_k b_k, then b_j -= U_jk x_k for j < k
 // (Matrices/dbl2_tabs_host.cpp:147).  b (shared or global) is overwritten.
@@ -393,57 +404,77 @@ __device__ void block_tiled_backsub(int dim, int szt, const double *U, int ldu, 
                                     double *x) {
   typedef typename N::T T;
   const int nbt = dim / szt;
+  const int grp = threadIdx.x >> 2, part = threadIdx.x & 3, ngrp = blockDim.x >> 2;
   for (int k = nbt - 1; k >= 0; --k) {
     const int off = k * szt;
     const double *inv = Tinv + (long)k * szt * szt * N::width;
-    for (int i = threadIdx.x; i < szt; i += blockDim.x) {
+    for (int base = 0; base < szt; base += ngrp) {
+      const int i = base + grp;
       T acc = N::zero();
-      for (int j = 0; j < szt; ++j) acc = N::add(acc, N::mul(ldn_at<N>(inv, (long)i * szt + j), ldn_at<N>(b, off + j)));
-      stn_at<N>(x, off + i, acc);
+      if (i < szt)
+        for (int j = part; j < szt; j += 4)
+          acc = N::add(acc, N::mul(ldn_at<N>(inv, (long)i * szt + j), ldn_at<N>(b, off + j)));
+      acc = group4_sum<N>(acc);
+      if (i < szt && part == 0) stn_at<N>(x, off + i, acc);
     }
     __syncthreads();
-    for (int r = threadIdx.x; r < off; r += blockDim.x) {
+    for (int base = 0; base < off; base += ngrp) {
+      const int r = base + grp;
       T acc = N::zero();
-      for (int j = 0; j < szt; ++j) acc = N::add(acc, N::mul(ldn_at<N>(U, (long)r * ldu + off + j), ldn_at<N>(x, off + j)));
-      stn_at<N>(b, r, N::sub(ldn_at<N>(b, r), acc));
+      if (r < off)
+        for (int j = part; j < szt; j += 4)
+          acc = N::add(acc, N::mul(ldn_at<N>(U, (long)r * ldu + off + j), ldn_at<N>(x, off + j)));
+      acc = group4_sum<N>(acc);
+      if (r < off && part == 0) stn_at<N>(b, r, N::sub(ldn_at<N>(b, r), acc));
     }
     __syncthreads();
   }
 }
 
-// w = Q^H b (Newton/dbl2_bals_kernels.cu:22 dbl2_bals_qtb)
+// w = Q^H b (Newton/dbl2_bals_kernels.cu:22 dbl2_bals_qtb), four lanes per
+// output
 template <class N>
 __device__ void block_qhb(int n, const double *Q, const double *b, double *w) {
   typedef typename N::T T;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+  const int grp = threadIdx.x >> 2, part = threadIdx.x & 3, ngrp = blockDim.x >> 2;
+  for (int base = 0; base < n; base += ngrp) {
+    const int i = base + grp;
     T acc = N::zero();
-    for (int j = 0; j < n; ++j) acc = N::add(acc, N::mul(N::conj(ldn_at<N>(Q, (long)j * n + i)), ldn_at<N>(b, j)));
-    stn_at<N>(w, i, acc);
+    if (i < n)
+      for (int j = part; j < n; j += 4)
+        acc = N::add(acc, N::mul(N::conj(ldn_at<N>(Q, (long)j * n + i)), ldn_at<N>(b, j)));
+    acc = group4_sum<N>(acc);
+    if (i < n && part == 0) stn_at<N>(w, i, acc);
   }
   __syncthreads();
 }
 
 // b_j -= A_{j-i+1} x for j = i..degp1-1 (Newton/dbl2_tail_kernels.cu:19
-// dbl2_bals_tail, all right hand sides of one stage at once): one warp per
-// matrix row, lanes along the row, shuffle reduction.
+// dbl2_bals_tail, all right hand sides of one stage at once): one thread per
+// row of the stacked matrices A_1 .. A_{degp1-i}, the row's dot product with
+// x (shared memory) in two interleaved partial sums.  The stage is a chain
+// of dependent multiple-double operations per row; a thread per row keeps
+// every thread of the CTA on its own chain instead of reducing each row
+// across a warp.
 template <class N>
 __device__ void block_tail_update(int n, int degp1, int i, const double *mat, double *rhs, const double *x) {
   typedef typename N::T T;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const long nn = (long)n * n;
   const int rows = (degp1 - i) * n;
-  for (int r = warp; r < rows; r += nw) {
+  for (int r = threadIdx.x; r < rows; r += blockDim.x) {
     const int j = i + r / n, row = r % n;
     const double *A = mat + (long)(j - i + 1) * nn * N::width + (long)row * n * N::width;
-    T acc = N::zero();
-    for (int l = lane; l < n; l += 32) acc = N::add(acc, N::mul(ldn_at<N>(A, l), ldn_at<N>(x, l)));
-    acc = warp_sum<N>(acc);
-    if (lane == 0) {
-      double *bj = rhs + ((long)j * n + row) * N::width;
-      T v;
-      md::ldn(bj, v);
-      md::stn(bj, N::sub(v, acc));
+    T a0 = N::zero(), a1 = N::zero();
+    int l = 0;
+    for (; l + 1 < n; l += 2) {
+      a0 = N::add(a0, N::mul(ldn_at<N>(A, l), ldn_at<N>(x, l)));
+      a1 = N::add(a1, N::mul(ldn_at<N>(A, l + 1), ldn_at<N>(x, l + 1)));
     }
+    if (l < n) a0 = N::add(a0, N::mul(ldn_at<N>(A, l), ldn_at<N>(x, l)));
+    double *bj = rhs + ((long)j * n + row) * N::width;
+    T v;
+    md::ldn(bj, v);
+    md::stn(bj, N::sub(v, N::add(a0, a1)));
   }
   __syncthreads();
 }
