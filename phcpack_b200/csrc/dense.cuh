@@ -130,6 +130,17 @@ __host__ __device__ inline long dense_smem_doubles(int n, int szt, int W) { retu
 // T (n x szt) and the inverted diagonal tiles of R (n x szt).
 __host__ __device__ inline long dense_work_numbers(int n, int szt) { return 5L * n * szt; }
 
+// Dot products shared by aligned groups of four lanes: output o of a pass
+// is computed by the four lanes 4(o mod 8) .. +3 of warp o / 8, each summing
+// every fourth term, then two xor shuffles add the four partial sums (the
+// chains of dependent multiple-double operations are a quarter as long as
+// with one thread per output).  All lanes of a warp take part in every pass.
+template <class N>
+__device__ __forceinline__ typename N::T group4_sum(typename N::T a) {
+  a = N::add(a, md::shfl_xor(a, 1));
+  return N::add(a, md::shfl_xor(a, 2));
+}
+
 // ------------------------------------------------------------- Householder
 // Reflector of x = R[c.., c], m = n - c entries, in PHCpack's convention
 // (Matrices/dbl2_factorizations.cpp:374 real, :436 complex): v[0] = 1,
@@ -205,15 +216,17 @@ __device__ void block_apply_reflector(int n, int ncols, int c, int e, double *Rm
   typedef typename N::T T;
   typedef typename N::real R;
   typedef md::num<R, false> RN;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int grp = threadIdx.x >> 2, part = threadIdx.x & 3, ngrp = blockDim.x >> 2;
   const R beta = ldn_at<RN>(S.misc, 0);
   if (md::is_zero(beta)) return;
-  for (int j = c + warp; j < e; j += nw) {
+  for (int base = c; base < e; base += ngrp) {  // four lanes per column
+    const int j = base + grp;
     T acc = N::zero();
-    for (int i = c + lane; i < n; i += 32)
-      acc = N::add(acc, N::mul(N::conj(ldn_at<N>(Rm, (long)i * ncols + j)), ldn_at<N>(S.v, i - c)));
-    acc = warp_sum<N>(acc);
-    if (lane == 0) stn_at<N>(S.w, j - c, N::scale(acc, beta));
+    if (j < e)
+      for (int i = c + part; i < n; i += 4)
+        acc = N::add(acc, N::mul(N::conj(ldn_at<N>(Rm, (long)i * ncols + j)), ldn_at<N>(S.v, i - c)));
+    acc = group4_sum<N>(acc);
+    if (j < e && part == 0) stn_at<N>(S.w, j - c, N::scale(acc, beta));
   }
   __syncthreads();
   const int nc = e - c;
@@ -270,14 +283,16 @@ __device__ void block_houseqr(int n, int ncols, int szt, double *Q, double *Rm, 
       for (int i = threadIdx.x; i < m; i += blockDim.x)
         stn_at<N>(Wm, i, N::neg(N::scale(ldn_at<N>(Y, i), b0)));
       __syncthreads();
-      const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+      const int grp = threadIdx.x >> 2, part = threadIdx.x & 3, ngrp = blockDim.x >> 2;
       for (int j = 1; j < szt; ++j) {
-        for (int kk = warp; kk < j; kk += nw) {
+        for (int base = 0; base < j; base += ngrp) {  // four lanes per inner product
+          const int kk = base + grp;
           T acc = N::zero();
-          for (int i = lane; i < m; i += 32)
-            acc = N::add(acc, N::mul(N::conj(ldn_at<N>(Y, (long)kk * m + i)), ldn_at<N>(Y, (long)j * m + i)));
-          acc = warp_sum<N>(acc);
-          if (lane == 0) stn_at<N>(S.w, kk, acc);
+          if (kk < j)
+            for (int i = part; i < m; i += 4)
+              acc = N::add(acc, N::mul(N::conj(ldn_at<N>(Y, (long)kk * m + i)), ldn_at<N>(Y, (long)j * m + i)));
+          acc = group4_sum<N>(acc);
+          if (kk < j && part == 0) stn_at<N>(S.w, kk, acc);
         }
         __syncthreads();
         const R bj = ldn_at<RN>(S.beta, j);
@@ -383,17 +398,6 @@ __device__ void block_invert_tiles(int dim, int szt, const double *U, int ldu, d
     }
   }
   __syncthreads();
-}
-
-// Dot products shared by aligned groups of four lanes: output o of a pass
-// is computed by the four lanes 4(o mod 8) .. +3 of warp o / 8, each summing
-// every fourth term, then two xor shuffles add the four partial sums (the
-// chains of dependent multiple-double operations are a quarter as long as
-// with one thread per output).  All lanes of a warp take part in every pass.
-template <class N>
-__device__ __forceinline__ typename N::T group4_sum(typename N::T a) {
-  a = N::add(a, md::shfl_xor(a, 1));
-  return N::add(a, md::shfl_xor(a, 2));
 }
 
 // x = U^{-1} b with the inverted diagonal tiles: for k = nbt-1..0,
