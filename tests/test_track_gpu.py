@@ -108,3 +108,38 @@ def test_track_device_entry_matches_host_entry():
     torch.cuda.synchronize()
     d = dt.result()
     assert np.array_equal(h.xend, d.xend) and np.array_equal(h.status, d.status)
+
+
+@pytest.mark.parametrize("n", [1, 2, 24, 32])
+def test_track_dimension_extremes_vs_oracle(n):
+    """The smallest and largest dimensions the kernel takes (n = 1 and the
+    32 of one warp per LU): a seeded weakly coupled quadratic system, a
+    sample of its total-degree paths, same classification as the oracle and
+    end points within 1e-26 (relative to their size)."""
+    rng = np.random.default_rng(100 + n)
+    # x_i^2 - a_i plus a weak coupling to three other variables: 2^n regular
+    # roots near the (+-) square roots of a_i, all reached from x_i^2 - 1
+    target = []
+    for i in range(n):
+        poly = [(((i, 2),), 1.0 + 0j), ((), complex(-rng.uniform(1.0, 3.0)))]
+        if n > 1:
+            for j in rng.choice([k for k in range(n) if k != i], size=min(3, n - 1), replace=False):
+                poly.append((((int(j), 1),), complex(0.1 * hm.unit(rng))))
+        target.append(poly)
+    gamma = complex(hm.unit(rng))
+    cap = min(8, 2 ** n)
+    pb = hm.total_degree_problem([target], gamma, max_paths_per_system=cap, rng=rng)
+    ipar, dpar = hm.params()
+    g = hm.track_host(pb, pmode=1, rmode=2)
+    xo, io, _ = pyoracle.track(ORC, pb, ipar, dpar, pmode=1, rmode=2)
+    io = io.reshape(-1, 3)
+    assert np.array_equal(g.status == 0, io[:, 0] == 0)
+    ok = (g.status == 0) & (io[:, 0] == 0)
+    assert ok.any()
+    assert (g.residual[ok] <= 1e-24).all()
+    scale = np.maximum(1.0, np.abs(g.endpoints(pb.maxdim)).max(axis=1))
+    assert (endpoint_diff(pb, g.xend, xo, 2)[ok] <= 1e-26 * scale[ok]).all()
+    if n == 1:
+        a = -target[0][1][1].real
+        x = g.endpoints(pb.maxdim)[:, 0]
+        assert np.allclose(np.sort(x.real), [-np.sqrt(a), np.sqrt(a)], atol=1e-14)
