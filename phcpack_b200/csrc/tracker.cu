@@ -327,9 +327,11 @@ __global__ void __launch_bounds__(kTrackThreads, (track_min_blocks<PN, RN>::valu
       }
       __syncthreads();
       hom_eval_cta<PN>(S, s, 0, t, xs, K + 1, sm + L.V, sm + L.G, sm + L.hs, sm + L.J0);
-      if (ctid() < 32) warp_lufac<PN>(n, sm + L.J0, piv, dinv);
+      if (ctid() < 32) {
+        warp_lufac<PN>(n, sm + L.J0, piv, dinv);
+        warp_luinverse<PN>(n, sm + L.J0, piv, dinv, sm + L.M);
+      }
       __syncthreads();
-      cta_luinverse<PN>(n, sm + L.J0, piv, dinv, sm + L.M);
       for (int k = 1; k <= K; ++k) {
         hom_coef_cta<PN>(S, s, k, t, xs, K + 1, sm + L.V, sm + L.r);
         for (int i = ctid(); i < n; i += blockDim.x) {

@@ -404,8 +404,9 @@ __device__ TRACK_FN void hom_coef_cta(const TrackDev &S, int s, int k, double t0
 // limbs), rows k and ell swap in columns k..n-1, and the multipliers
 // -a_ik / a_kk overwrite column k below the diagonal.  Besides ipvt the
 // reciprocals dinv[k] = 1 / u_kk are kept for the back substitution (NaN
-// for a zero pivot).  One warp alone, lane i owning row i: no CTA barrier,
-// the other warps of the CTA stay free.  Called by all lanes of the warp;
+// for a zero pivot).  One warp alone (lanes over the rows for the pivot and
+// the multipliers, over the entries for the trailing update): no CTA
+// barrier, the other warps of the CTA stay free.  Called by all lanes of the warp;
 // returns info to every lane: 0, or k + 1 for the first column k without a
 // nonzero pivot.
 template <class N>
@@ -442,13 +443,14 @@ __device__ TRACK_FN int warp_lufac(int n, double *A, int *ipvt, double *dinv) {
     __syncwarp();
     const T inv = N::div(N::one(), ldn_at<N>(A, (long)k * n + k));
     if (lane == 0) stn_at<N>(dinv, k, inv);
-    if (lane > k && lane < n) {
-      const T m = N::mul(N::neg(inv), ldn_at<N>(A, (long)lane * n + k));
-      stn_at<N>(A, (long)lane * n + k, m);
-      for (int j = k + 1; j < n; ++j) {
-        const long o = (long)lane * n + j;
-        stn_at<N>(A, o, N::add(ldn_at<N>(A, o), N::mul(ldn_at<N>(A, (long)k * n + j), m)));
-      }
+    if (lane > k && lane < n) stn_at<N>(A, (long)lane * n + k, N::mul(N::neg(inv), ldn_at<N>(A, (long)lane * n + k)));
+    __syncwarp();
+    // trailing update, the (n-k-1)^2 entries spread over the lanes
+    const int m = n - k - 1;
+    for (int e = lane; e < m * m; e += 32) {
+      const int i = k + 1 + e / m, j = k + 1 + e % m;
+      const long o = (long)i * n + j;
+      stn_at<N>(A, o, N::add(ldn_at<N>(A, o), N::mul(ldn_at<N>(A, (long)k * n + j), ldn_at<N>(A, (long)i * n + k))));
     }
     __syncwarp();
   }
@@ -482,36 +484,45 @@ __device__ typename N::T warp_lusolve(int n, const double *A, const int *ipvt, c
   return v;
 }
 
-// M = A^{-1} from the factors of warp_lufac, one thread per column c: the
-// column of M is the work vector of lusolve applied to e_c (same order of
-// operations as warp_lusolve).
+// M = A^{-1} from the factors of warp_lufac by one warp: lusolve applied to
+// the columns e_c of the identity, all columns at once, each substitution
+// step spread over the lanes (every entry sees the same operations in the
+// same order as a column-by-column solve).  Called by all lanes of one
+// warp; the caller synchronises before M is read by other warps.
 template <class N>
-__device__ TRACK_FN void cta_luinverse(int n, const double *A, const int *ipvt, const double *dinv, double *M) {
+__device__ TRACK_FN void warp_luinverse(int n, const double *A, const int *ipvt, const double *dinv, double *M) {
   typedef typename N::T T;
-  for (int c = ctid(); c < n; c += blockDim.x) {
-    for (int i = 0; i < n; ++i) stn_at<N>(M, (long)i * n + c, i == c ? N::one() : N::zero());
-    for (int k = 0; k < n - 1; ++k) {
-      const int ell = ipvt[k];
-      const T t = ldn_at<N>(M, (long)ell * n + c);
-      if (ell != k) {
+  const int lane = threadIdx.x & 31;
+  for (int e = lane; e < n * n; e += 32) stn_at<N>(M, e, (e / n == e % n) ? N::one() : N::zero());
+  __syncwarp();
+  for (int k = 0; k < n - 1; ++k) {  // L y = P e_c
+    const int ell = ipvt[k];
+    if (ell != k)
+      for (int c = lane; c < n; c += 32) {
+        const T t = ldn_at<N>(M, (long)ell * n + c);
         stn_at<N>(M, (long)ell * n + c, ldn_at<N>(M, (long)k * n + c));
         stn_at<N>(M, (long)k * n + c, t);
       }
-      for (int i = k + 1; i < n; ++i) {
-        const long o = (long)i * n + c;
-        stn_at<N>(M, o, N::add(ldn_at<N>(M, o), N::mul(t, ldn_at<N>(A, (long)i * n + k))));
-      }
+    __syncwarp();
+    const int m = n - k - 1;
+    for (int e = lane; e < m * n; e += 32) {
+      const int i = k + 1 + e / n, c = e % n;
+      const long o = (long)i * n + c;
+      stn_at<N>(M, o, N::add(ldn_at<N>(M, o), N::mul(ldn_at<N>(M, (long)k * n + c), ldn_at<N>(A, (long)i * n + k))));
     }
-    for (int kb = n - 1; kb >= 0; --kb) {
-      const T x = N::mul(ldn_at<N>(M, (long)kb * n + c), ldn_at<N>(dinv, kb));
-      stn_at<N>(M, (long)kb * n + c, x);
-      for (int j = 0; j < kb; ++j) {
-        const long o = (long)j * n + c;
-        stn_at<N>(M, o, N::sub(ldn_at<N>(M, o), N::mul(x, ldn_at<N>(A, (long)j * n + kb))));
-      }
-    }
+    __syncwarp();
   }
-  __syncthreads();
+  for (int kb = n - 1; kb >= 0; --kb) {  // U x = y
+    for (int c = lane; c < n; c += 32)
+      stn_at<N>(M, (long)kb * n + c, N::mul(ldn_at<N>(M, (long)kb * n + c), ldn_at<N>(dinv, kb)));
+    __syncwarp();
+    for (int e = lane; e < kb * n; e += 32) {
+      const int j = e / n, c = e % n;
+      const long o = (long)j * n + c;
+      stn_at<N>(M, o, N::sub(ldn_at<N>(M, o), N::mul(ldn_at<N>(M, (long)kb * n + c), ldn_at<N>(A, (long)j * n + kb))));
+    }
+    __syncwarp();
+  }
 }
 
 // y = M b, M n x n, one thread per row
