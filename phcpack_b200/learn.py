@@ -10,7 +10,7 @@ much further than the conservative pole step the predictor can be trusted.
 At run time the corrector judges every proposal; a rejected one is redone
 with the plain step, so the learned step never changes which paths succeed.
 
-    python -m phcpack_b200.learn --out gpurun_out/step_mlp.npz
+    python -m phcpack_b200.learn --out step_mlp.npz
 """
 from __future__ import annotations
 
@@ -151,7 +151,7 @@ def train_default(seed=0, epochs=30, device="cuda"):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--out", default="gpurun_out/step_mlp.npz")
+    ap.add_argument("--out", default="step_mlp.npz")
     ap.add_argument("--epochs", type=int, default=30)
     a = ap.parse_args()
     tr, X, y, hist = train_default(epochs=a.epochs)
