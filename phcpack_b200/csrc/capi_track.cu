@@ -12,6 +12,7 @@ int track(const TrackDev &S, const TrackParDev &P, int nmono_max, int npaths, co
           int pmode, int rmode, const void *model, double *xend, int *info, double *dinfo, float *log, int log_cap,
           int *log_count, int *queue, int one_per_launch, cudaStream_t st);
 long track_smem_bytes(int maxdim, int K, int M, int nmono_max, int maxvar, int pmode, int rmode, int gst);
+int track_check(const TrackParDev &P, int pmode, int rmode, int maxdim);
 }  // namespace phc
 
 using namespace phc;
@@ -135,6 +136,12 @@ int phc_track_host(int nsys, const int *dim, int maxvar, const int *mono_off, co
   for (int s = 0; s < nsys; ++s) {
     maxdim = dim[s] > maxdim ? dim[s] : maxdim;
     nmono_max = (mono_off[s + 1] - mono_off[s]) > nmono_max ? (mono_off[s + 1] - mono_off[s]) : nmono_max;
+  }
+  // the checks of phc_track, made here before any device work
+  {
+    const TrackParDev P = make_par(ipar, dpar, step_mode);
+    const int rc = track_check(P, pmode, rmode, maxdim);
+    if (rc) return rc;
   }
   const int neq = eq_off[nsys];
   const int nterm = term_off[neq];

@@ -557,14 +557,21 @@ static int track_launch(const TrackDev &S, const TrackParDev &P, int nmono_max, 
   return PHC_OK;
 }
 
+// The checks of the modes, the dimension and the series and Pade degrees.
+int track_check(const TrackParDev &P, int pmode, int rmode, int maxdim) {
+  PHC_REQUIRE(pmode == 1 || pmode == 2, "track: predictor precision %d not in {1,2}", pmode);
+  PHC_REQUIRE(rmode == 2 || rmode == 4 || rmode == 8, "track: refinement precision %d not in {2,4,8}", rmode);
+  PHC_REQUIRE(maxdim >= 1 && maxdim <= 32, "track: dimension %d not in [1,32]", maxdim);
+  PHC_REQUIRE(P.deg >= 3 && P.deg <= kTrackKmax && P.numdeg + P.dendeg == P.deg && P.dendeg <= 8 && P.nit >= 1,
+              "track: need 3 <= deg = numdeg + dendeg <= %d, dendeg <= 8", kTrackKmax);
+  return PHC_OK;
+}
+
 int track(const TrackDev &S, const TrackParDev &P, int nmono_max, int npaths, const int *path_sys, const double *x0,
           int pmode, int rmode, const void *model, double *xend, int *info, double *dinfo, float *log, int log_cap,
           int *log_count, int *queue, int one_per_launch, cudaStream_t st) {
-  PHC_REQUIRE(pmode == 1 || pmode == 2, "track: predictor precision %d not in {1,2}", pmode);
-  PHC_REQUIRE(rmode == 2 || rmode == 4 || rmode == 8, "track: refinement precision %d not in {2,4,8}", rmode);
-  PHC_REQUIRE(S.maxdim >= 1 && S.maxdim <= 32, "track: dimension %d not in [1,32]", S.maxdim);
-  PHC_REQUIRE(P.deg >= 3 && P.deg <= kTrackKmax && P.numdeg + P.dendeg == P.deg && P.dendeg <= 8 && P.nit >= 1,
-              "track: need 3 <= deg = numdeg + dendeg <= %d, dendeg <= 8", kTrackKmax);
+  const int bad = track_check(P, pmode, rmode, S.maxdim);
+  if (bad) return bad;
   PHC_REQUIRE(queue != nullptr || one_per_launch, "track: the batched launch needs a queue counter");
   PHC_REQUIRE(model == nullptr || (reinterpret_cast<unsigned long long>(model) & 15) == 0, "track: the model buffer is not 16-byte aligned");
   if (npaths == 0) return PHC_OK;
