@@ -120,9 +120,10 @@ int phc_bals_solve_wy(int prec, int cplx, int ninst, int dim, int degp1, int szt
 
 /* phc_bals_solve without any allocation.  No counterpart in the reference:
  * this entry point is for callers that cannot let a library call cudaMalloc
- * or cudaFree (work recorded into a CUDA graph under stream capture,
- * latency-critical callers that cannot afford cudaFree's device-wide
- * synchronisation, frameworks whose own allocator owns all device memory).
+ * or cudaFree (latency-critical callers that cannot afford cudaFree's
+ * device-wide synchronisation, frameworks whose own allocator owns and
+ * accounts for all device memory, code that must not allocate once it has
+ * been set up).
  * Same arguments and results as phc_bals_solve minus the workspace, which
  * is a static device array of phc_bals_solve_static_capacity_bytes() bytes
  * (8 MiB, held by every GPU that loads the library until exit); larger

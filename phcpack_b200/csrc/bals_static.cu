@@ -3,10 +3,10 @@
 // library owns for the lifetime of the process.
 //
 // Who needs this: callers that cannot let a library call cudaMalloc or
-// cudaFree, namely code that records its work into a CUDA graph while a
-// stream is being captured, latency-critical callers that cannot afford the
-// device-wide synchronisation cudaFree implies, and frameworks that hand all
-// device memory to their own allocator and account for every byte.  They
+// cudaFree, namely latency-critical callers that cannot afford the
+// device-wide synchronisation cudaFree implies, frameworks that hand all
+// device memory to their own allocator and account for every byte, and code
+// that must not allocate at all once it has been set up.  They
 // pass inputs and outputs (device memory they own) and get the workspace
 // from here.
 //

@@ -1,8 +1,8 @@
 """The allocation-free block-Toeplitz solve (phc_bals_solve_static).
 
-Callers that record work into CUDA graphs, cannot afford cudaFree's
-device-wide synchronisation, or hand all device memory to their own
-allocator cannot let the library allocate; this entry point takes its
+Callers that cannot afford cudaFree's device-wide synchronisation, hand all
+device memory to their own allocator, or must not allocate once set up
+cannot let the library allocate; this entry point takes its
 workspace from a static device array instead.  Checked through the C ABI
 against phc_bals_solve with a caller-provided workspace, on two calls in a
 row with different shapes and precisions (the shared array keeps the first
