@@ -22,12 +22,19 @@ _D = ctypes.POINTER(ctypes.c_double)
 _I = ctypes.POINTER(ctypes.c_int)
 
 
+SHIM_BIN = os.path.join(HERE, "_ref", "test_dbl2_polynomials")
+
+
 def build(ref: bool = True) -> None:
-    """Compile liboracle.so, and _ref/libphcref.so where the reference tree
-    exists."""
+    """Compile liboracle.so and, where the reference tree exists,
+    _ref/libphcref.so and _ref/test_dbl2_polynomials (the reference's
+    polynomial test program on this library through ref_shim_polynomials.cu;
+    needs phcpack_b200/libphcb200.so built first)."""
     targets = ["liboracle.so"]
     if ref and os.path.isdir(REF_TREE):
         targets.append("_ref/libphcref.so")
+        if os.path.exists(os.path.join(HERE, "..", "phcpack_b200", "libphcb200.so")):
+            targets.append("_ref/test_dbl2_polynomials")
     subprocess.run(["make", "-s", "-C", HERE, f"REF={REF_TREE}"] + targets, check=True)
 
 

@@ -59,9 +59,15 @@ static int launch_system(int nsys, int dim, int deg, int maxvar, const int *mon_
                          cudaStream_t stream) {
   const int W = N::width;
   const int S = (deg + 1) * W;
-  const int wpb = dim < kMaxWarpsPerBlock ? dim : kMaxWarpsPerBlock;
-  const long scr = (long)wpb * warp_slots(maxvar) * S * sizeof(double);
+  // one warp per polynomial, up to 8 per CTA; monomials with many variables
+  // need many scratch series per warp, so fewer warps share a CTA when the
+  // shared memory would not hold the scratch of 8; the inputs are staged in
+  // shared memory when they fit beside the scratch
+  const long per_warp = (long)warp_slots(maxvar) * S * sizeof(double);
   const long xs = (long)((dim * S + 1) & ~1) * sizeof(double);
+  int wpb = dim < kMaxWarpsPerBlock ? dim : kMaxWarpsPerBlock;
+  while (wpb > 1 && (long)wpb * per_warp > kMaxSmem) --wpb;
+  const long scr = (long)wpb * per_warp;
   int stage = (scr + xs) <= 200 * 1024;
   const long smem = scr + (stage ? xs : 0);
   if (smem > kMaxSmem) {

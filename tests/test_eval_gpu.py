@@ -47,6 +47,18 @@ def test_eval_gpu_vs_oracle_config2_shape(prec, cplx):
     assert check_scaled(out, ref, scale, prec, cplx, RTOL[prec]) <= 1.0
 
 
+@pytest.mark.parametrize("prec,cplx", [(2, False), (2, True), (4, True)])
+def test_eval_gpu_long_monomials(prec, cplx):
+    # monomials of 20..32 distinct variables at degree 31: the scratch of a
+    # warp (2*32-1 series) no longer fits 8 warps per CTA, so fewer
+    # polynomials share a CTA
+    b = wl.eval_batch(40 + prec, 1, 32, 31, 6, 32, prec, cplx, expmax=1, minvar=20)
+    out = run_device(b)
+    ref = ORC.system_evaldiff(b)
+    scale = ORC.system_evaldiff(abs_batch(b))
+    assert check_scaled(out, ref, scale, prec, cplx, RTOL[prec]) <= 1.0
+
+
 @pytest.mark.parametrize("deg", [0, 1, 2, 7, 8, 15, 30])
 def test_eval_gpu_degrees(deg):
     b = wl.eval_batch(100 + deg, 5, 6, deg, 5, 4, 2, True, expmax=3)
