@@ -230,6 +230,58 @@ int phc_track_host(int nsys, const int *dim, int maxvar, const int *mono_off, co
                    const int *path_sys, const double *x0, const int *ipar, const double *dpar, int pmode, int rmode,
                    int step_mode, const void *model, double *xend, int *info, double *dinfo, void *stream);
 void phc_track_host_release(void);
+
+/* End-game diagnostics at points (x, t) of the homotopies of phc_track: the
+ * Newton-Fabry convergence radius of the path's series and the Hessian
+ * distance to the nearest singular solution, with the curvature step of the
+ * Pade predictor.  Replaces, batched over points:
+ *   Newton_Fabry      Ada Deformations/Curves/dobldobl_fabry_on_homotopy.adb:30-83
+ *   Fabry             Ada Math_Lib/Circuits/convergence_radius_estimates.adb:138-163,392-425
+ *   Distance          Ada Deformations/Curves/singular_values_of_hessians.adb:190-211
+ *   Hesse_Pade        Ada Deformations/Curves/dobldobl_predictor_convolutions.adb:368-406
+ *   Step_Distance     Ada Deformations/Curves/series_and_predictors.adb:813-825
+ * Systems: the device arrays of phc_track (gather lists from
+ *   phc_track_prepare).  Point p lies on system path_sys[p] at t = tpt[p]
+ *   with x at xpt: maxdim complex numbers per point, xlimbs doubles per part
+ *   (the real limbs, then the imaginary limbs; xlimbs 1, 2, 4 or 8, so that
+ *   start points (1) and the end points of phc_track (4, or 8 after an
+ *   octo-double refinement) are read as they are).
+ * ipar: deg K (3..16, the degree of the series), numdeg L and dendeg M
+ *   (L + M <= K, M <= 8: the Pade approximant of the curvature step),
+ *   offset (0..K-2: the Fabry ratio is c_{K-1-offset} / c_{K-offset}; 1 in
+ *   Newton_Fabry), newton_steps (0..64 Newton steps at t before the series;
+ *   0 = none).
+ * dpar: tolres (Newton's bound on max |dx|), beta2 (factor of the curvature
+ *   step; 0.005 in the reference's defaults).
+ * pmode: 1, 2 or 4: double, double-double or quad-double for Newton, the
+ *   series, Fabry and Pade; the Jacobian and the Hessians are rounded to
+ *   double for their singular values (one-sided Jacobi).
+ * Outputs per point: series (may be NULL): maxdim x (K+1) complex numbers
+ *   in the working precision (2 * pmode doubles each: real limbs, then
+ *   imaginary limbs); dout (10 doubles): z (real, imaginary; the singular
+ *   point is at t + z), the radius |z|, Fabry's error estimate,
+ *   sigma_min(J), the 2-norm of the Hessians' largest singular values, eta =
+ *   2 sigma_min(J) / that norm (+inf when every Hessian is zero), the 2-norm
+ *   of the Pade error estimates, the curvature step (beta2 eta / that
+ *   norm)^(1/K), Newton's last max |dx|; iout (2 ints): 1 when Fabry fails
+ *   (every component's c_{K-offset} is negligible, or no series), and the
+ *   status: 0, 1 (singular Jacobian at the point: no series) or 2 (Newton did
+ *   not reach tolres).  Device pointers; no counterpart of this batching in
+ *   the reference, which runs these one solution at a time on the host. */
+int phc_series_diagnostics(int nsys, const int *dim, int maxvar, int maxdim, int nmono_max, const int *mono_off,
+                           const int *mono_nvr, const int *mono_idx, const int *mono_exp, const int *eq_off,
+                           const int *term_off, const int *term_mono, const double *term_a, const double *term_b,
+                           const int *jg_off, const int *jg_term, const int *jg_slot, int gstaged, int npaths,
+                           const int *path_sys, const double *xpt, int xlimbs, const double *tpt, const int *ipar,
+                           const double *dpar, int pmode, double *series, double *dout, int *iout, void *stream);
+/* Host arrays in and out (the same arguments; the gather lists are built
+ * here); allocates and frees its device memory per call. */
+int phc_series_diagnostics_host(int nsys, const int *dim, int maxvar, const int *mono_off, const int *mono_nvr,
+                                const int *mono_idx, const int *mono_exp, const int *eq_off, const int *term_off,
+                                const int *term_mono, const double *term_a, const double *term_b, int npaths,
+                                const int *path_sys, const double *xpt, int xlimbs, const double *tpt,
+                                const int *ipar, const double *dpar, int pmode, double *series, double *dout,
+                                int *iout);
 /* ------------------------------------------------------- learned step size
  * No counterpart in the reference (its trackers use the ratio / Pade pole
  * and curvature steps only).  A 24 -> 128 -> 128 -> 1 ReLU network predicts

@@ -182,3 +182,34 @@ def track(lib: Lib, pb, ipar, dpar, pmode=1, rmode=2, nthreads=1):
            _ip(info), _dp(dinfo))
     assert rc == 0
     return xend, info, dinfo
+
+
+def series_diagnostics(lib: Lib, pb, xpt, xlimbs, tpt, ipar, dpar, pmode=2):
+    """End-game diagnostics of tracker_oracle.cpp at the points (xpt, tpt)
+    of a TrackProblem's homotopies: the series, Fabry's ratio, the Pade error
+    norm, and the Jacobian and Hessians in complex double (their singular
+    values are left to the caller).  Returns a dict of arrays."""
+    K = int(ipar[0])
+    W = 2 * pmode
+    n = pb.maxdim
+    series = np.zeros(pb.npaths * n * (K + 1) * W)
+    dout = np.zeros(pb.npaths * 6)
+    iout = np.zeros(pb.npaths * 2, np.int32)
+    J = np.zeros(pb.npaths * n * n * 2)
+    H = np.zeros(pb.npaths * n * n * n * 2)
+    xpt = np.ascontiguousarray(xpt, dtype=np.float64)
+    tpt = np.ascontiguousarray(tpt, dtype=np.float64)
+    ipar = np.ascontiguousarray(ipar, dtype=np.int32)
+    dpar = np.ascontiguousarray(dpar, dtype=np.float64)
+    f = lib._fn("series_diagnostics")
+    rc = f(pb.nsys, _ip(pb.dim), pb.maxvar, _ip(pb.mono_off), _ip(pb.mono_nvr), _ip(pb.mono_idx), _ip(pb.mono_exp),
+           _ip(pb.eq_off), _ip(pb.term_off), _ip(pb.term_mono), _dp(pb.term_a), _dp(pb.term_b), pb.npaths,
+           _ip(pb.path_sys), n, _dp(xpt), int(xlimbs), _dp(tpt), _ip(ipar), _dp(dpar), pmode, _dp(series),
+           _dp(dout), _ip(iout), _dp(J), _dp(H))
+    assert rc == 0
+    d = dout.reshape(-1, 6)
+    Jc = J.reshape(pb.npaths, n, n, 2)
+    Hc = H.reshape(pb.npaths, n, n, n, 2)
+    return dict(series=series.reshape(pb.npaths, n, K + 1, W), z=d[:, 0] + 1j * d[:, 1], radius=d[:, 2],
+                err=d[:, 3], padenorm=d[:, 4], lastdx=d[:, 5], fail=iout[0::2].copy(), status=iout[1::2].copy(),
+                J=Jc[..., 0] + 1j * Jc[..., 1], H=Hc[..., 0] + 1j * Hc[..., 1])

@@ -343,6 +343,7 @@ template <class T> static T horner(const std::vector<T> &a, int deg, const T &z)
 template <class PT, class CT> static void convert(const CT &a, PT &b);
 template <> void convert(const cx<dd> &a, cx<double> &b) { b = cx<double>(a.re.hi + a.re.lo, a.im.hi + a.im.lo); }
 template <> void convert(const cx<dd> &a, cx<dd> &b) { b = a; }
+template <> void convert(const cx<double> &a, cx<double> &b) { b = a; }
 template <> void convert(const cx<double> &a, cx<dd> &b) { b = cx<dd>(dd(a.re), dd(a.im)); }
 template <> void convert(const cx<dd> &a, cx<qd> &b) { b = cx<qd>(qd(a.re), qd(a.im)); }
 template <> void convert(const cx<qd> &a, cx<qd> &b) { b = a; }
@@ -522,6 +523,193 @@ static PathOut track_path(const TrackSys &S, int s, const TrackPar &P, const dou
   return o;
 }
 
+// ---------------------------------------------------------------- end game
+// The end-game diagnostics at a point (x, t) of the homotopy, restated:
+// Newton at the point, the Taylor series of the path to degree K, Fabry's
+// ratio over the components (Newton_Fabry,
+// Curves/dobldobl_fabry_on_homotopy.adb:30-83; Fabry,
+// Circuits/convergence_radius_estimates.adb:138-163,392-425), the Pade error
+// estimates (Solution_Error_Estimate, Threshold_Index,
+// Curves/homotopy_pade_approximants.adb:558-568,717-754), and the Jacobian
+// and the Hessians in complex double, whose singular values the caller
+// computes (Distance, Curves/singular_values_of_hessians.adb:190-211).
+
+// a + 1 == 1 in the working precision (Is_Zero,
+// Circuits/convergence_radius_estimates.adb:8-20)
+template <class R> static bool negligible(const R &a) {
+  double u[8], v[8];
+  store(u, R(1.0) + a);
+  store(v, R(1.0));
+  for (int l = 0; l < limbs<R>::n; ++l)
+    if (u[l] != v[l]) return false;
+  return true;
+}
+template <class R> static bool negligible(const cx<R> &z) { return negligible(z.re) && negligible(z.im); }
+
+template <class R> static bool less_limbs(const R &a, const R &b) {
+  double u[8], v[8];
+  store(u, a);
+  store(v, b);
+  for (int l = 0; l < limbs<R>::n; ++l)
+    if (u[l] != v[l]) return u[l] < v[l];
+  return false;
+}
+
+template <class T>
+static void fabry_one(const std::vector<T> &c, int K, int off, T &z, double &e, bool &fail) {
+  fail = negligible(c[K - off]);
+  if (fail) return;
+  const double nm1 = (double)(K - 1);
+  if (off == 0) {
+    z = c[K - 1] / c[K];
+    e = negligible(c[K - 1]) ? 1.0 : cabs(z - c[K - 2] / c[K - 1]) * nm1;
+  } else {
+    z = c[K - 1 - off] / c[K - off];
+    e = negligible(c[K]) ? 1.0 : cabs(z - c[K - 1] / c[K]) * nm1;
+  }
+}
+
+template <class T>
+static double pade_error(const std::vector<T> &c, int K, const std::vector<T> &p, int pdeg, const std::vector<T> &q,
+                         int qdeg) {
+  typedef typename real_of<T>::type R;
+  const int endidx = std::min(pdeg + qdeg + 2, K);
+  int top = -1;
+  for (int i = endidx; i >= 0; --i)
+    if (cabs(c[i]) > 1e-5) { top = i; break; }
+  T res = T(R(1.0));
+  if (top >= 0) {
+    res = c[top];
+    for (int i = 1; i <= qdeg && i <= top; ++i) res = res + q[i] * c[top - i];
+    if (top <= pdeg) res = p[top] - res;
+  }
+  const double a = cabs(res);
+  return a < 1e-5 ? 1.0 : a;
+}
+
+template <class R> static double lead_of(const R &a) { double u[8]; store(u, a); return u[0]; }
+
+// J[i][j] = dh_i/dx_j and H[i][j][k] = d^2 h_i / dx_j dx_k at (x, t), complex
+// double, row-major (real, imaginary) pairs with ld numbers per row
+static void jacobian_hessians(const TrackSys &S, int s, double t, const std::vector<cx<double> > &x, int ld,
+                              double *J, double *H) {
+  const int n = S.dim[s];
+  std::fill(J, J + 2L * ld * ld, 0.0);
+  std::fill(H, H + 2L * ld * ld * ld, 0.0);
+  for (int i = 0; i < n; ++i) {
+    const int eq = S.eq_off[s] + i;
+    for (int tr = S.term_off[eq]; tr < S.term_off[eq + 1]; ++tr) {
+      const int gm = S.term_mono[tr];
+      const int nv = S.mono_nvr[gm];
+      const int *ix = S.mono_idx + (long)gm * S.maxvar, *ex = S.mono_exp + (long)gm * S.maxvar;
+      const cx<double> c(std::fma(S.term_b[2 * tr] - S.term_a[2 * tr], t, S.term_a[2 * tr]),
+                         std::fma(S.term_b[2 * tr + 1] - S.term_a[2 * tr + 1], t, S.term_a[2 * tr + 1]));
+      for (int u = 0; u < nv; ++u) {
+        // first partial
+        cx<double> a = mul_d(c, (double)ex[u]);
+        for (int w = 0; w < nv; ++w)
+          for (int e = ex[w] - (w == u); e > 0; --e) a = a * x[ix[w]];
+        J[2 * ((long)i * ld + ix[u])] += a.re;
+        J[2 * ((long)i * ld + ix[u]) + 1] += a.im;
+        for (int v = 0; v < nv; ++v) {
+          const double mult = u == v ? (double)ex[u] * (ex[u] - 1) : (double)ex[u] * ex[v];
+          if (mult == 0.0) continue;
+          cx<double> b = mul_d(c, mult);
+          for (int w = 0; w < nv; ++w)
+            for (int e = ex[w] - (w == u) - (w == v); e > 0; --e) b = b * x[ix[w]];
+          const long o = 2 * (((long)i * ld + ix[u]) * ld + ix[v]);
+          H[o] += b.re;
+          H[o + 1] += b.im;
+        }
+      }
+    }
+  }
+}
+
+struct DiagOut {
+  int fail, status;
+  double zre, zim, radius, err, padenorm, lastdx;
+};
+
+template <class T>
+static DiagOut diag_point(const TrackSys &S, int s, const int *ipar, const double *dpar, const double *xp, int xlimbs,
+                          double t, int ld, double *series, double *J, double *H) {
+  typedef typename real_of<T>::type R;
+  const int n = S.dim[s];
+  const int K = ipar[0], L = ipar[1], M = ipar[2], off = ipar[3], nsteps = ipar[4];
+  const int LP = limbs<R>::n;
+  DiagOut o{1, 0, 0.0, 0.0, INFINITY, 0.0, 0.0, 0.0};
+  std::vector<T> x(n);
+  for (int i = 0; i < n; ++i) {
+    double re[8] = {0}, im[8] = {0};
+    for (int l = 0; l < LP && l < xlimbs; ++l) {
+      re[l] = xp[(long)i * 2 * xlimbs + l];
+      im[l] = xp[(long)i * 2 * xlimbs + xlimbs + l];
+    }
+    load(re, x[i].re);
+    load(im, x[i].im);
+  }
+  bool conv = true;
+  if (nsteps > 0) conv = point_newton<T, T>(S, s, t, x, nsteps, dpar[0], 1, &o.lastdx);
+  std::vector<cx<double> > xd(n);
+  for (int i = 0; i < n; ++i) xd[i] = cx<double>(lead_of(x[i].re), lead_of(x[i].im));
+  jacobian_hessians(S, s, t, xd, ld, J, H);
+  std::vector<std::vector<T> > xs(n, std::vector<T>(K + 1));
+  for (int i = 0; i < n; ++i) xs[i][0] = x[i];
+  {
+    std::vector<std::vector<T> > x0(n, std::vector<T>(1)), h;
+    std::vector<T> jac;
+    for (int i = 0; i < n; ++i) x0[i][0] = x[i];
+    hom_eval(S, s, 0, t, x0, h, &jac);
+    lu_solver<T> lu;
+    lu.factor(n, jac);
+    if (lu.info != 0) {
+      o.status = 1;
+      o.padenorm = std::sqrt((double)n);
+    }
+  }
+  if (o.status == 0) {
+    TrackPar P{};
+    P.deg = K;
+    taylor_series(S, s, P, t, xs);
+    int best = -1;
+    R rbest = R(0.0);
+    double pn = 0.0;
+    for (int i = 0; i < n; ++i) {
+      T z;
+      double e = 0.0;
+      bool fail = true;
+      fabry_one(xs[i], K, off, z, e, fail);
+      if (!fail) {
+        const R ri = norm2(z);
+        if (best < 0 || less_limbs(ri, rbest)) {
+          best = i;
+          rbest = ri;
+          o.zre = lead_of(z.re);
+          o.zim = lead_of(z.im);
+          o.radius = cabs(z);
+          o.err = e;
+        }
+      }
+      std::vector<T> p, q;
+      int pd = L, qd = M;
+      if (!pade(L, M, xs[i], p, q)) {  // the fallback: the Taylor polynomial of degree K
+        p = xs[i];
+        pd = K;
+        qd = 0;
+      }
+      const double pe = pade_error(xs[i], K, p, pd, q, qd);
+      pn += pe * pe;
+    }
+    o.padenorm = std::sqrt(pn);
+    o.fail = best < 0 ? 1 : 0;
+    o.status = conv ? 0 : 2;
+  }
+  for (int i = 0; i < n; ++i)
+    for (int k = 0; k <= K; ++k) store(series + ((long)i * (K + 1) + k) * 2 * LP, xs[i][k]);
+  return o;
+}
+
 }  // namespace
 
 extern "C" {
@@ -574,6 +762,42 @@ int orc_track(int nsys, const int *dim, int maxvar, const int *mono_off, const i
     std::vector<std::thread> th;
     for (int i = 0; i < nthreads; ++i) th.emplace_back(work);
     for (auto &x : th) x.join();
+  }
+  return 0;
+}
+
+
+// End-game diagnostics of npaths points (restating phc_series_diagnostics
+// but for the singular values): per point x at xpt (maxdim complex numbers of
+// xlimbs limbs per part) and t = tpt[p]; ipar: deg, numdeg, dendeg, offset,
+// newton_steps; dpar: tolres; pmode 1, 2 or 4.  Out per point: series
+// (maxdim x (deg+1) complex numbers in the working precision), dout (z re,
+// z im, radius, Fabry error, Pade error norm, last Newton |dx|), iout (fail,
+// status), J (maxdim^2 complex doubles, row-major) and H (maxdim^3 complex
+// doubles: equation, row, column).
+int orc_series_diagnostics(int nsys, const int *dim, int maxvar, const int *mono_off, const int *mono_nvr,
+                           const int *mono_idx, const int *mono_exp, const int *eq_off, const int *term_off,
+                           const int *term_mono, const double *term_a, const double *term_b, int npaths,
+                           const int *path_sys, int maxdim, const double *xpt, int xlimbs, const double *tpt,
+                           const int *ipar, const double *dpar, int pmode, double *series, double *dout, int *iout,
+                           double *J, double *H) {
+  TrackSys S{nsys, maxvar, dim, mono_off, mono_nvr, mono_idx, mono_exp, eq_off, term_off, term_mono, term_a, term_b};
+  const int K = ipar[0];
+  if (pmode != 1 && pmode != 2 && pmode != 4) return -1;
+  if (K < 3 || ipar[1] + ipar[2] > K || ipar[3] < 0 || ipar[3] > K - 2) return -1;
+  for (int p = 0; p < npaths; ++p) {
+    const int s = path_sys[p];
+    const double *xp = xpt + (long)p * maxdim * 2 * xlimbs;
+    double *se = series + (long)p * maxdim * (K + 1) * 2 * pmode;
+    double *Jp = J + 2L * p * maxdim * maxdim, *Hp = H + 2L * p * maxdim * maxdim * maxdim;
+    DiagOut o;
+    if (pmode == 1) o = diag_point<cx<double> >(S, s, ipar, dpar, xp, xlimbs, tpt[p], maxdim, se, Jp, Hp);
+    else if (pmode == 2) o = diag_point<cx<dd> >(S, s, ipar, dpar, xp, xlimbs, tpt[p], maxdim, se, Jp, Hp);
+    else o = diag_point<cx<qd> >(S, s, ipar, dpar, xp, xlimbs, tpt[p], maxdim, se, Jp, Hp);
+    double *d = dout + 6L * p;
+    d[0] = o.zre; d[1] = o.zim; d[2] = o.radius; d[3] = o.err; d[4] = o.padenorm; d[5] = o.lastdx;
+    iout[2 * p] = o.fail;
+    iout[2 * p + 1] = o.status;
   }
   return 0;
 }

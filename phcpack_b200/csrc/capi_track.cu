@@ -13,6 +13,10 @@ int track(const TrackDev &S, const TrackParDev &P, int nmono_max, int npaths, co
           int *log_count, int *queue, int one_per_launch, cudaStream_t st);
 long track_smem_bytes(int maxdim, int K, int M, int nmono_max, int maxvar, int pmode, int rmode, int gst);
 int track_check(const TrackParDev &P, int pmode, int rmode, int maxdim);
+int series_diag(const TrackDev &S, const DiagParDev &D, int nmono_max, int npaths, const int *path_sys,
+                const double *xpt, int xlimbs, const double *tpt, int pmode, double *series, double *dout, int *iout,
+                cudaStream_t st);
+int diag_check(const DiagParDev &D, int pmode, int maxdim, int xlimbs);
 }  // namespace phc
 
 using namespace phc;
@@ -51,6 +55,18 @@ static TrackParDev make_par(const int *ipar, const double *dpar, int step_mode) 
   P.restol = dpar[6];
   P.learn_scale = dpar[7] > 0.0 ? dpar[7] : 1.0;
   return P;
+}
+
+static DiagParDev make_diag_par(const int *ipar, const double *dpar) {
+  DiagParDev D;
+  D.deg = ipar[0];
+  D.numdeg = ipar[1];
+  D.dendeg = ipar[2];
+  D.offset = ipar[3];
+  D.newton_steps = ipar[4];
+  D.tolres = dpar[0];
+  D.beta2 = dpar[1];
+  return D;
 }
 
 extern "C" {
@@ -241,6 +257,96 @@ void phc_track_host_release(void) {
     hb = HostCallBuffers();
   }
   cudaSetDevice(cur);
+}
+
+int phc_series_diagnostics(int nsys, const int *dim, int maxvar, int maxdim, int nmono_max, const int *mono_off,
+                           const int *mono_nvr, const int *mono_idx, const int *mono_exp, const int *eq_off,
+                           const int *term_off, const int *term_mono, const double *term_a, const double *term_b,
+                           const int *jg_off, const int *jg_term, const int *jg_slot, int gstaged, int npaths,
+                           const int *path_sys, const double *xpt, int xlimbs, const double *tpt, const int *ipar,
+                           const double *dpar, int pmode, double *series, double *dout, int *iout, void *stream) {
+  PHC_REQUIRE(nsys >= 1 && npaths >= 0, "series_diagnostics: bad sizes");
+  TrackDev S{nsys,      maxvar, maxdim, dim,    mono_off, mono_nvr, mono_idx, mono_exp,    eq_off,
+             term_off,  term_mono, term_a, term_b, jg_off,  jg_term,  jg_slot,  gstaged != 0};
+  return series_diag(S, make_diag_par(ipar, dpar), nmono_max, npaths, path_sys, xpt, xlimbs, tpt, pmode, series,
+                     dout, iout, (cudaStream_t)stream);
+}
+
+int phc_series_diagnostics_host(int nsys, const int *dim, int maxvar, const int *mono_off, const int *mono_nvr,
+                                const int *mono_idx, const int *mono_exp, const int *eq_off, const int *term_off,
+                                const int *term_mono, const double *term_a, const double *term_b, int npaths,
+                                const int *path_sys, const double *xpt, int xlimbs, const double *tpt,
+                                const int *ipar, const double *dpar, int pmode, double *series, double *dout,
+                                int *iout) {
+  PHC_REQUIRE(nsys >= 1 && npaths >= 0, "series_diagnostics_host: bad sizes");
+  int maxdim = 0, nmono_max = 0;
+  for (int s = 0; s < nsys; ++s) {
+    maxdim = dim[s] > maxdim ? dim[s] : maxdim;
+    nmono_max = (mono_off[s + 1] - mono_off[s]) > nmono_max ? (mono_off[s + 1] - mono_off[s]) : nmono_max;
+  }
+  const DiagParDev D = make_diag_par(ipar, dpar);
+  {
+    const int rc = diag_check(D, pmode, maxdim, xlimbs);
+    if (rc) return rc;
+  }
+  if (npaths == 0) return PHC_OK;
+  const int neq = eq_off[nsys];
+  const int nterm = term_off[neq];
+  const int nmono = mono_off[nsys];
+  const long long njg = phc_track_gather_count(nsys, mono_off, mono_nvr, eq_off, term_off, term_mono);
+  std::vector<int> jg_off((size_t)neq * maxdim + 1), jg_term(njg > 0 ? njg : 1), jg_slot(njg > 0 ? njg : 1);
+  const int staged = phc_track_prepare(nsys, dim, maxvar, mono_off, mono_nvr, mono_idx, mono_exp, eq_off, term_off,
+                                       term_mono, maxdim, jg_off.data(), jg_term.data(), jg_slot.data());
+  if (staged < 0) return staged;
+  const size_t sbytes = (size_t)npaths * maxdim * (D.deg + 1) * 2 * pmode * sizeof(double);
+  std::vector<std::pair<const void *, size_t> > ins = {
+      {dim, nsys * 4ul}, {mono_off, (nsys + 1) * 4ul}, {mono_nvr, nmono * 4ul},
+      {mono_idx, (size_t)nmono * maxvar * 4}, {mono_exp, (size_t)nmono * maxvar * 4}, {eq_off, (nsys + 1) * 4ul},
+      {term_off, (neq + 1) * 4ul}, {term_mono, nterm * 4ul}, {term_a, nterm * 16ul}, {term_b, nterm * 16ul},
+      {jg_off.data(), jg_off.size() * 4}, {jg_term.data(), jg_term.size() * 4}, {jg_slot.data(), jg_slot.size() * 4},
+      {path_sys, npaths * 4ul}, {xpt, (size_t)npaths * maxdim * 2 * xlimbs * 8}, {tpt, npaths * 8ul}};
+  std::vector<size_t> off;
+  size_t total = 0;
+  for (auto &in : ins) {
+    off.push_back(total);
+    total += (in.second + 255) & ~size_t(255);
+  }
+  const size_t o_series = total;
+  total += (sbytes + 255) & ~size_t(255);
+  const size_t o_dout = total;
+  total += ((size_t)npaths * kDiagOut * 8 + 255) & ~size_t(255);
+  const size_t o_iout = total;
+  total += ((size_t)npaths * 8 + 255) & ~size_t(255);
+  char *b = nullptr;
+  PHC_CUDA(cudaMalloc((void **)&b, total));
+  int out = PHC_OK;
+  for (size_t i = 0; i < ins.size() && out == PHC_OK; ++i)
+    if (ins[i].second && cudaMemcpy(b + off[i], ins[i].first, ins[i].second, cudaMemcpyHostToDevice) != cudaSuccess) {
+      set_error("series_diagnostics_host: copy to the device failed");
+      out = PHC_ERR_CUDA;
+    }
+  if (out == PHC_OK && series && cudaMemset(b + o_series, 0, sbytes) != cudaSuccess) {
+    set_error("series_diagnostics_host: memset failed");
+    out = PHC_ERR_CUDA;
+  }
+  if (out == PHC_OK) {
+    auto I = [&](int i) { return (const int *)(b + off[i]); };
+    auto Dp = [&](int i) { return (const double *)(b + off[i]); };
+    out = phc_series_diagnostics(nsys, I(0), maxvar, maxdim, nmono_max, I(1), I(2), I(3), I(4), I(5), I(6), I(7),
+                                 Dp(8), Dp(9), I(10), I(11), I(12), staged, npaths, I(13), Dp(14), xlimbs, Dp(15),
+                                 ipar, dpar, pmode, series ? (double *)(b + o_series) : nullptr,
+                                 (double *)(b + o_dout), (int *)(b + o_iout), nullptr);
+  }
+  if (out == PHC_OK) {
+    if (cudaMemcpy(dout, b + o_dout, (size_t)npaths * kDiagOut * 8, cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(iout, b + o_iout, (size_t)npaths * 8, cudaMemcpyDeviceToHost) != cudaSuccess ||
+        (series && cudaMemcpy(series, b + o_series, sbytes, cudaMemcpyDeviceToHost) != cudaSuccess)) {
+      set_error("series_diagnostics_host: %s", cudaGetErrorString(cudaGetLastError()));
+      out = PHC_ERR_CUDA;
+    }
+  }
+  cudaFree(b);
+  return out;
 }
 
 }  // extern "C"

@@ -34,53 +34,6 @@
 namespace phc {
 
 
-struct TrackLayout {
-  long xs, V, G, hs, J0, M, r, num, den, xp, xc, hc, Jc, Vc, Gc, red, piv, dinv, feat, mag, degs, hbuf, total;
-};
-
-__host__ __device__ inline TrackLayout track_layout(int n, int K, int M, int nm, int mv, int Wp, int Wr, int gst) {
-  TrackLayout L;
-  long o = 0;
-  auto take = [&](long doubles) {
-    long r = o;
-    o += (doubles + 1) & ~1L;  // keep 16-byte alignment
-    return r;
-  };
-  const long K1 = K + 1;
-  // state that lives through a whole step
-  L.xs = take(n * K1 * Wp);
-  L.xc = take(n * Wr);
-  L.num = take(n * K1 * Wp);
-  L.den = take(n * (M + 1) * Wp);
-  L.xp = take(n * Wp);
-  const int Wm = Wp > Wr ? Wp : Wr;
-  L.red = take(32 * Wm);
-  L.piv = take(24);  // 32 pivot rows and the info word, as ints
-  L.dinv = take(n * Wm);
-  L.feat = take(32);
-  L.mag = take(n * K1);
-  L.degs = take(n);
-  L.hbuf = take(2 * 128 + 8);
-  // scratch of the Taylor series and the predictor feedback ...
-  const long ov = o;
-  L.V = take(nm * 2 * Wp);  // two coefficients per monomial (point evaluations use one)
-  L.G = take(gst ? nm * mv * Wp : 0);  // only monomials of degree >= 3 stage partials
-  L.hs = take(n * Wp);
-  L.J0 = take(n * n * Wp);
-  L.M = take(n * n * Wp);
-  L.r = take(n * Wp);
-  const long pend = o;
-  // ... overlaid by the scratch of the corrector and the refinement, which
-  // run after the Pade approximants are formed
-  o = ov;
-  L.hc = take(n * Wr);
-  L.Jc = take(n * n * Wr);
-  L.Vc = take(nm * Wr);
-  L.Gc = take(gst ? nm * mv * Wr : 0);
-  L.total = o > pend ? o : pend;
-  return L;
-}
-
 template <class N>
 __device__ double cta_maxmag(int n, const double *v, double *red) {
   double a = 0.0;
@@ -91,116 +44,12 @@ __device__ double cta_maxmag(int n, const double *v, double *red) {
   return block_max(a, red);
 }
 
-// Newton at a point in precision N (the corrector and the refinement):
-// LU_Newton_Steps of Curves/corrector_convolutions.adb:1193-1224 restated:
-// each step evaluates h(x) in precision N and J(x) in precision JN (N, or
-// double in the precision-split tracker: Newton with a double Jacobian and
-// a residual in N still converges to the accuracy of N, each step gaining
-// about 16 digits near the solution), factors J by warp_lufac and solves
-// J dx = -h(x) (a singular Jacobian ends the steps unconverged, x
-// unchanged); converged when max |dx| <= tol, then extra more steps.  x
-// (shared, n numbers of precision N) is updated in place; lastdx: the last
-// max |dx|.
-template <class N, class JN>
-__device__ TRACK_FN bool point_newton(const TrackDev &S, int s, int n, double t, double *x, double *h, double *Jm, double *Vc,
-                             double *Gc, int *piv, double *dinv, double *red, int maxit, double tol, int extra,
-                             double *lastdx) {
-  bool conv = false;
-  int extra_left = extra;
-  *lastdx = 1e300;
-  for (int it = 0; it < maxit + extra; ++it) {
-    if (it >= maxit && !conv) break;
-    hom_eval_cta<N, 1, JN>(S, s, 0, t, x, 1, Vc, Gc, h, Jm);
-    if (ctid() < 32) {
-      const int lane = ctid();
-      const int info = warp_lufac<JN>(n, Jm, piv, dinv);
-      typename JN::T b = JN::zero();
-      if (lane < n) b = JN::neg(conv_num<N, JN>::go(ldn_at<N>(h, lane)));
-      const typename JN::T v = warp_lusolve<JN>(n, Jm, piv, dinv, b);
-      double m = 0.0;
-      if (lane < n) {
-        m = JN::mag(v);
-        if (!(m == m)) m = INFINITY;
-        if (info == 0) stn_at<N>(x, lane, N::add(ldn_at<N>(x, lane), conv_num<JN, N>::go(v)));
-      }
-      m = warp_max(m);
-      if (lane == 0) red[0] = info ? INFINITY : m;
-    }
-    __syncthreads();
-    const double m = red[0];
-    __syncthreads();
-    *lastdx = m;
-    if (!(m <= 1e300)) return false;
-    if (conv) {
-      if (--extra_left <= 0) break;
-    } else if (m <= tol) {
-      conv = true;
-      if (extra_left <= 0) break;
-    }
-  }
-  return conv;
-}
-
 // max_i |h_i(x, t)| at a point, in precision N
 template <class N>
 __device__ double point_residual(const TrackDev &S, int s, int n, double t, const double *x, double *h, double *Vc,
                                  double *Gc, double *red) {
   hom_eval_cta<N>(S, s, 0, t, x, 1, Vc, Gc, h, nullptr);
   return cta_maxmag<N>(n, h, red);
-}
-
-// Pade [L/M] of component i's series c (K+1 numbers), Gaussian elimination
-// with partial pivoting on the M x M system; Taylor fallback when singular.
-// Curves/standard_rational_approximations.ads:67-100.  Returns the numerator
-// degree used (L, or K for the fallback); the denominator degree is M or 0.
-template <class N>
-__device__ TRACK_FN int pade_one(int L, int M, int K, const double *c, double *num, double *den) {
-  typedef typename N::T T;
-  T A[kTrackKmax * kTrackKmax / 4 + 16], b[kTrackKmax / 2 + 8], q[kTrackKmax / 2 + 9];
-  bool ok = true;
-  for (int i = 1; i <= M; ++i) {
-    for (int j = 1; j <= M; ++j) {
-      const int k = L + i - j;
-      A[(i - 1) * M + (j - 1)] = k >= 0 ? ldn_at<N>(c, k) : N::zero();
-    }
-    b[i - 1] = N::neg(ldn_at<N>(c, L + i));
-  }
-  for (int col = 0; col < M && ok; ++col) {
-    int piv = col;
-    double best = N::mag(A[col * M + col]);
-    for (int r = col + 1; r < M; ++r) {
-      const double m = N::mag(A[r * M + col]);
-      if (m > best) { best = m; piv = r; }
-    }
-    if (!(best > 0.0)) { ok = false; break; }
-    if (piv != col) {
-      for (int j = 0; j < M; ++j) { T tt = A[piv * M + j]; A[piv * M + j] = A[col * M + j]; A[col * M + j] = tt; }
-      T tt = b[piv]; b[piv] = b[col]; b[col] = tt;
-    }
-    for (int r = col + 1; r < M; ++r) {
-      const T f = N::div(A[r * M + col], A[col * M + col]);
-      for (int j = col; j < M; ++j) A[r * M + j] = N::sub(A[r * M + j], N::mul(f, A[col * M + j]));
-      b[r] = N::sub(b[r], N::mul(f, b[col]));
-    }
-  }
-  q[0] = N::one();
-  if (ok) {
-    for (int i = M - 1; i >= 0; --i) {
-      T acc = b[i];
-      for (int j = i + 1; j < M; ++j) acc = N::sub(acc, N::mul(A[i * M + j], q[j + 1]));
-      q[i + 1] = N::div(acc, A[i * M + i]);
-    }
-    for (int i = 0; i <= M; ++i) stn_at<N>(den, i, q[i]);
-    for (int i = 0; i <= L; ++i) {
-      T acc = N::zero();
-      for (int j = 0; j <= (i < M ? i : M); ++j) acc = N::add(acc, N::mul(q[j], ldn_at<N>(c, i - j)));
-      stn_at<N>(num, i, acc);
-    }
-    return L;
-  }
-  stn_at<N>(den, 0, N::one());
-  for (int i = 0; i <= K; ++i) stn_at<N>(num, i, ldn_at<N>(c, i));
-  return K;
 }
 
 template <class N>
@@ -510,6 +359,7 @@ __global__ void __launch_bounds__(kTrackThreads, (track_min_blocks<PN, RN>::valu
     __syncthreads();
   }
 }
+
 
 }  // namespace phc
 
