@@ -231,6 +231,20 @@ int phc_track_host(int nsys, const int *dim, int maxvar, const int *mono_off, co
                    int step_mode, const void *model, double *xend, int *info, double *dinfo, void *stream);
 void phc_track_host_release(void);
 
+/* The mixed volume of the Newton polytopes of a square system in n
+ * variables (the BKK bound on its isolated roots with nonzero coordinates):
+ * the method of MixedVol, Ada Root_Counts/MixedVol/mixedvol_algorithm.adb
+ * (mv, the C code mixed_volume1.c, relation_table1.c, one_level_lp1.c):
+ * random lifting from seed, the mixed cells of the induced subdivision by a
+ * depth-first search with LP feasibility tests, the volume the sum of
+ * |det| over the cells.  Support i has counts[i] exponent vectors of n ints,
+ * stored support after support in pts.  cells (may be NULL): up to
+ * max_cells cells, each n pairs (p_i, q_i) of point indices within the
+ * supports; *ncells (may be NULL): the number of mixed cells.  Host code
+ * only (no device work).  Returns the mixed volume (>= 0) or an error. */
+long long phc_mixed_volume(int n, const int *counts, const int *pts, unsigned long long seed, int max_cells,
+                           int *cells, long long *ncells);
+
 /* End-game diagnostics at points (x, t) of the homotopies of phc_track: the
  * Newton-Fabry convergence radius of the path's series and the Hessian
  * distance to the nearest singular solution, with the curvature step of the

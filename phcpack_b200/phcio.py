@@ -441,7 +441,10 @@ def manypaths(target, start=None, start_solutions=None, gamma=None, rmode=2, pmo
     used; start="linear-product" builds a random linear-product start system
     and all its roots for a partition of the variables (partition: lists of
     variable names; default the partition with the smallest m-homogeneous
-    Bezout number, phcpack_b200.rootcounts).  gamma: complex (default:
+    Bezout number, phcpack_b200.rootcounts); start="mixed-volume" a system
+    with the target's supports and random coefficients whose roots with
+    nonzero coordinates, as many as the mixed volume, are found first on the
+    GPU (rootcounts.mixed_volume_start).  gamma: complex (default:
     random on the unit circle from seed).  Returns (solution list text of
     the end points at t = 1, the TrackResult with the counts of
     root_accounting in its `accounting` attribute).  err is the forward
@@ -464,6 +467,9 @@ def manypaths(target, start=None, start_solutions=None, gamma=None, rmode=2, pmo
         else:
             part = [[symbols.index(v) for v in st] for st in partition]
         q, xs, _ = rootcounts.linear_product_start(polys, part, np.random.default_rng(seed + 1))
+    elif start == "mixed-volume":
+        from . import rootcounts
+        q, xs, _ = rootcounts.mixed_volume_start(polys, len(symbols), np.random.default_rng(seed + 1))
     else:
         q, _ = parse_system(start, symbols=list(symbols))
         if start_solutions is None:

@@ -155,3 +155,86 @@ def linear_product_problem(polys, partition, gamma, rng) -> hm.TrackProblem:
     q for the partition, with all of q's roots as start points."""
     q, roots, _ = linear_product_start(polys, partition, rng)
     return hm.homotopy_problem([(polys, q)], gamma, [(0, x) for x in roots])
+
+
+# ------------------------------------------------------------ mixed volume
+# The BKK bound: the number of isolated roots with nonzero coordinates of a
+# system with generic coefficients is the mixed volume of its Newton
+# polytopes, computed natively by phc_mixed_volume (include/phc_b200.h; the
+# method of MixedVol, Root_Counts/MixedVol/mixedvol_algorithm.adb: random
+# lifting, lower edges, relation table, depth-first search of the mixed
+# cells with LP feasibility tests).
+
+def _supports(polys, nvar):
+    out = []
+    for p in polys:
+        pts = set()
+        for m, c in p:
+            if c == 0:
+                continue
+            e = [0] * nvar
+            for v, k in m:
+                e[v] += k
+            pts.add(tuple(e))
+        out.append(np.array(sorted(pts), dtype=np.int64).reshape(-1, nvar))
+    return out
+
+
+def mixed_cells(supports, seed=0, max_cells=1 << 16):
+    """Mixed volume and mixed cells of a random lifting of n supports (arrays
+    of exponent vectors in n variables).  Returns (mixed volume, cells): a
+    cell is an n x 2 array of point indices, one edge per support."""
+    from . import _lib
+    n = len(supports)
+    if any(np.asarray(a).reshape(-1, n).shape[1] != n for a in supports):
+        raise ValueError("mixed_cells: need n supports in n variables")
+    counts = np.array([len(a) for a in supports], np.int32)
+    pts = np.ascontiguousarray(np.concatenate([np.asarray(a, np.int64).reshape(-1, n) for a in supports])
+                               .astype(np.int32).reshape(-1))
+    cells = np.zeros(max(1, max_cells) * 2 * n, np.int32)
+    nc = np.zeros(1, np.int64)
+    lib = _lib.lib()
+    f = lib.phc_mixed_volume
+    f.restype = _lib.ctypes.c_longlong
+    mv = int(f(n, _lib.ptr(counts), _lib.ptr(pts), _lib.ctypes.c_ulonglong(seed), int(max_cells), _lib.ptr(cells),
+               _lib.ptr(nc)))
+    if mv < 0:
+        raise _lib.PhcError(lib.phc_last_error().decode())
+    k = int(min(nc[0], max_cells))
+    return mv, cells[:k * 2 * n].reshape(k, n, 2)
+
+
+def mixed_volume(polys, nvar=None, seed=0):
+    """The mixed volume of the Newton polytopes of a square system (a list
+    of polynomials as lists of (monomial, coefficient))."""
+    nvar = len(polys) if nvar is None else nvar
+    mv, _ = mixed_cells(_supports(polys, nvar), seed, max_cells=0)
+    return mv
+
+
+def _monomial(e):
+    return tuple((v, int(k)) for v, k in enumerate(e) if k > 0)
+
+
+def mixed_volume_start(polys, nvar, rng, pmode=1, rmode=2, **kw):
+    """A start system with as many paths as the mixed volume: q has the
+    supports of polys and random coefficients on the unit circle, and its
+    roots with nonzero coordinates (as many as the mixed volume, for generic
+    coefficients) are found once by the total-degree homotopy on the GPU.
+    q then starts the linear homotopy (1 - t) gamma q + t p to polys, or to
+    any system with the same supports (a cheater's homotopy), with one path
+    per root instead of one per total-degree start point.  Returns (q, the
+    distinct roots of q with nonzero coordinates, the mixed volume)."""
+    S = _supports(polys, nvar)
+    mv = mixed_volume(polys, nvar)
+    q = [[(_monomial(e), complex(hm.unit(rng))) for e in S[i]] for i in range(len(polys))]
+    qq, degs = hm.total_degree_start(q)
+    pb = hm.homotopy_problem([(q, qq)], complex(hm.unit(rng)), [(0, x) for x in hm.total_degree_solutions(degs)])
+    r = hm.track_host(pb, pmode=pmode, rmode=rmode, **kw)
+    x = r.endpoints(pb.maxdim)[r.status == 0, :nvar]
+    x = x[np.abs(x).min(axis=1) > 1e-8] if len(x) else x
+    roots = []
+    for v in x:
+        if all(np.abs(v - w).max() > 1e-8 * max(1.0, np.abs(v).max()) for w in roots):
+            roots.append(v)
+    return q, roots, mv

@@ -106,3 +106,19 @@ def test_linear_product_start_eigenproblem():
     want = np.sort_complex(np.linalg.eigvals(A))
     assert np.abs(got - want).max() <= 1e-10
     assert all(s["res"] <= 1e-24 for s in sols)
+
+
+def test_mixed_volume_start_cyclic5():
+    """cyclic 5-roots from a start system with its supports: the mixed
+    volume, 70, is the number of paths (against 120 total-degree paths),
+    and every path ends at a distinct root."""
+    from phcpack_b200 import rootcounts
+    polys, sym = phcio.parse_system(cyclic_text(5))
+    assert rootcounts.mixed_volume(polys, len(sym)) == 70
+    text, r = phcio.manypaths(cyclic_text(5), start="mixed-volume", seed=3, maxsteps=2000)
+    assert r.status.shape == (70,) and (r.status == 0).all()
+    sols = phcio.parse_solutions(text, symbols=sym)
+    pts = np.array([s["x"] for s in sols])
+    d = np.abs(pts[:, None, :] - pts[None, :, :]).max(axis=2) + np.eye(len(pts))
+    assert (d > 1e-6).all()
+    assert all(s["res"] <= 1e-24 for s in sols)
