@@ -124,3 +124,28 @@ def classify(t, diag: Diagnostics, near=0.5):
         else:
             out.append("regular")
     return out
+
+
+def series_diagnostics_device(dt, xpt, tpt, xlimbs=1, pmode=2, dout=None, iout=None, stream=None, **kw):
+    """phc_series_diagnostics on a problem resident on the device
+    (homotopy.DeviceTracker dt) with device tensors xpt and tpt; dout
+    (points x 10 doubles) and iout (points x 2 ints) are device tensors,
+    allocated when not given.  Returns (dout, iout); does not synchronise."""
+    import torch
+    pb = dt.pb
+    ipar, dpar = params(pmode, **kw)
+    a = dt.arr
+    dev = a["x0"].device
+    if dout is None:
+        dout = torch.zeros(pb.npaths * len(FIELDS), dtype=torch.float64, device=dev)
+    if iout is None:
+        iout = torch.zeros(pb.npaths * 2, dtype=torch.int32, device=dev)
+    s = 0 if stream is None else stream.cuda_stream
+    _lib.call("phc_series_diagnostics", pb.nsys, _lib.ptr(a["dim"]), pb.maxvar, pb.maxdim, pb.nmono_max,
+              _lib.ptr(a["mono_off"]), _lib.ptr(a["mono_nvr"]), _lib.ptr(a["mono_idx"]), _lib.ptr(a["mono_exp"]),
+              _lib.ptr(a["eq_off"]), _lib.ptr(a["term_off"]), _lib.ptr(a["term_mono"]), _lib.ptr(a["term_a"]),
+              _lib.ptr(a["term_b"]), _lib.ptr(a["jg_off"]), _lib.ptr(a["jg_term"]), _lib.ptr(a["jg_slot"]),
+              dt.gstaged, pb.npaths, _lib.ptr(a["path_sys"]), _lib.ptr(xpt), int(xlimbs), _lib.ptr(tpt),
+              _lib.ptr(ipar), _lib.ptr(dpar), pmode, _lib.c_void_p(0), _lib.ptr(dout), _lib.ptr(iout),
+              _lib.c_void_p(s))
+    return dout, iout

@@ -152,3 +152,19 @@ def test_dimension_extremes(n):
         polys.append(poly)
     pb = hm.total_degree_problem([polys], complex(hm.unit(rng)), max_paths_per_system=4, rng=rng)
     check_against_oracle(pb, pb.x0, 1, np.zeros(pb.npaths), 2)
+
+
+def test_device_entry_point_matches_host_entry_point():
+    import torch
+    rng = np.random.default_rng(15)
+    pb = hm.total_degree_problem([hm.dense_quadratic(rng, 5)], complex(hm.unit(rng)))
+    pb = hm.subset(pb, np.arange(16))
+    dt = hm.DeviceTracker(pb)
+    tpt = torch.zeros(pb.npaths, dtype=torch.float64, device="cuda")
+    dout, iout = eg.series_diagnostics_device(dt, dt.arr["x0"], tpt, 1, 2)
+    torch.cuda.synchronize()
+    dev = eg.Diagnostics.from_arrays(dout.cpu().numpy(), iout.cpu().numpy())
+    host = eg.series_diagnostics(pb, pb.x0, np.zeros(pb.npaths), pmode=2)
+    assert np.array_equal(dev.status, host.status) and np.array_equal(dev.fail, host.fail)
+    for f in ("z", "radius", "err", "sigma_min", "hessian_norm", "eta", "pade_norm", "curv_step"):
+        assert np.array_equal(getattr(dev, f), getattr(host, f)), f
