@@ -133,3 +133,18 @@ def test_diagnostics_host_rejects_bad_arguments(change, match):
     rc = f(*_host_args(pb, ipar, dpar, change.get("pmode", 2), change.get("xlimbs", 1)))
     msg = _lib.lib().phc_last_error().decode()
     assert rc < 0 and match in msg, msg
+
+
+def test_diagnostics_refuses_shared_memory_beyond_the_limit():
+    """n = 32 in quad-double needs more than 227 KB of shared memory per
+    point: refused before any device work (null device pointers suffice)."""
+    f = _lib.lib().phc_series_diagnostics
+    f.restype = ctypes.c_int
+    dim = np.array([32], np.int32)
+    ipar = np.array([8, 5, 1, 1, 4], np.int32)
+    dpar = np.array([1e-48, 0.005])
+    N = ctypes.c_void_p(0)
+    rc = f(1, _lib.ptr(dim), 2, 32, 600, N, N, N, N, N, N, N, N, N, N, N, N, 0, 1, N, N, 1, N, _lib.ptr(ipar),
+           _lib.ptr(dpar), 4, N, N, N, N)
+    msg = _lib.lib().phc_last_error().decode()
+    assert rc < 0 and "shared memory" in msg, msg
