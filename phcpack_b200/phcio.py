@@ -431,7 +431,7 @@ def _eval_jac(polys, x):
 
 
 def manypaths(target, start=None, start_solutions=None, gamma=None, rmode=2, pmode=1, step_mode=0, model=None,
-              seed=0, partition=None, **kw):
+              seed=0, partition=None, endgame=True, **kw):
     """Track all paths of (1 - t) gamma q + t p from the start solutions of
     q to p on the GPU, in PHCpack's text formats: the counterpart of
     gpumanypaths_dd (rmode 2) and gpumanypaths_qd (rmode 4), and an
@@ -451,7 +451,11 @@ def manypaths(target, start=None, start_solutions=None, gamma=None, rmode=2, pmo
     error estimate |J^{-1}|_inf * res and rco the reciprocal 1-norm
     condition number of the Jacobian at the end point (both in double); the
     diagnostics line of each solution carries its kind ("complex regular",
-    "at infinity", ...)."""
+    "at infinity", ...).  endgame: the paths that failed get the end-game
+    diagnostics at their last point (phcpack_b200.endgame): the result's
+    `endgame` maps each to "singular at t = 1" (diverging, or ending at a
+    singular solution), "interior singularity", "regular" or "no series",
+    and the accounting counts them under "endgame"."""
     polys, symbols = parse_system(target)
     if len(polys) != len(symbols):
         raise ParseError("the tracker needs as many polynomials as variables")
@@ -494,4 +498,16 @@ def manypaths(target, start=None, start_solutions=None, gamma=None, rmode=2, pmo
         t_end = 1.0 if r.status[p] == 0 else float(r.t[p])
         sols.append(dict(t=complex(t_end), m=1, x=xe[p], err=err, rco=rco, res=float(r.residual[p])))
     r.accounting = root_accounting(sols, r.status != 0)
+    # the end game of the failed paths: where is the nearest singular point?
+    r.endgame = {}
+    bad = np.flatnonzero(r.status != 0)
+    if endgame and len(bad):
+        from . import endgame as eg
+        xe = r.xend.reshape(pb.npaths, -1)[bad]
+        d = eg.series_diagnostics(hm.subset(pb, bad), xe, r.t[bad], xlimbs=r.limbs, pmode=2)
+        r.endgame = {int(p): c for p, c in zip(bad, eg.classify(r.t[bad], d))}
+        counts = {}
+        for c in r.endgame.values():
+            counts[c] = counts.get(c, 0) + 1
+        r.accounting["endgame"] = counts
     return write_solutions(sols, symbols, digits={2: 32, 4: 64, 8: 128}[rmode]), r

@@ -66,6 +66,9 @@ def test_cyclic5_endpoints():
     assert a["regular"] == len(ok) and a["singular"] == 0 and a["clustered"] == 0
     assert a["regular"] + a["infinity"] + a["failures"] == 120
     assert all(sols[p]["m"] == 1 for p in ok)
+    # the end game places the singular point of the failed paths at t = 1
+    assert len(r.endgame) == 120 - len(ok)
+    assert list(r.endgame.values()).count("singular at t = 1") >= 0.8 * len(r.endgame)
 
 
 def test_given_start_system_and_solutions_match_total_degree():
