@@ -199,7 +199,7 @@ def mixed_cells(supports, seed=0, max_cells=1 << 16):
     mv = int(f(n, _lib.ptr(counts), _lib.ptr(pts), _lib.ctypes.c_ulonglong(seed), int(max_cells), _lib.ptr(cells),
                _lib.ptr(nc)))
     if mv < 0:
-        raise _lib.PhcError(lib.phc_last_error().decode())
+        raise _lib.PhcError("phc_mixed_volume", mv, lib.phc_last_error().decode(errors="replace"))
     k = int(min(nc[0], max_cells))
     return mv, cells[:k * 2 * n].reshape(k, n, 2)
 

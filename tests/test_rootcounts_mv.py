@@ -64,3 +64,8 @@ def test_rejects_bad_sizes():
     assert f(0, _lib.ptr(counts), _lib.ptr(pts), ctypes.c_ulonglong(0), 0, ctypes.c_void_p(0),
              ctypes.c_void_p(0)) < 0
     assert "bad sizes" in _lib.lib().phc_last_error().decode()
+
+
+def test_error_is_raised_as_phc_error():
+    with pytest.raises(_lib.PhcError, match="phc_mixed_volume"):
+        rc.mixed_cells([np.zeros((2, 65), np.int64)] * 65)
