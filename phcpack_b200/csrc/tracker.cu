@@ -1,425 +1,18 @@
-// tracker.cu -- batched series-Pade path tracking on the GPU.
-//
-// A persistent kernel: each CTA repeatedly takes the next path from an
-// on-device work queue (one atomicAdd; no waiting on other CTAs) and tracks
-// it from t = 0 to t = 1, so paths of uneven length balance across the SMs.
-// Per step (the Ada Predictor_Corrector_Loop, predictor_corrector_loops.adb
-// :37-85, restated):
-//   predictor, in PN precision (double or double-double):
-//     the Taylor series of the path in s = t - t0 to degree K, one
-//     coefficient at a time with the LU of J_0 (factored and J_0^{-1}
-//     formed once per predictor step);
-//     [L/M] Pade approximant per component; pole step pbeta * r, r the
-//     smallest Fabry radius |c_{K-3}/c_{K-2}|; step <= maxsize, cut at t = 1;
-//     predictor feedback: halve until the mixed residual < alpha;
-//   corrector: at most corsteps LU Newton steps with residuals and updates
-//     in double-double and the Jacobian and its solve in PN precision,
-//     converged when max |dx| <= tolres, plus one extra step; on failure
-//     halve the step;
-//   the step size comes from a learned model when one is given (step_mode
-//     1): a proposal whose corrector fails is rejected and the step is
-//     redone with the plain pole step;
-//   at t = 1: refinement in RN precision (double-, quad- or octo-double) and
-//     classification by the max-norm residual.
-// Every loop is bounded (maxsteps, halvings down to minsize); nothing waits.
-#include "common.cuh"
-#include "tracker.cuh"
-#include "mlp.cuh"
-#include "../../include/phc_b200.h"
-
-#ifndef TRACK_MINB
-#define TRACK_MINB 8
-#endif
+// tracker.cu -- the path tracker's entry (the checks and the dispatch over
+// the precisions) and the launches with the double-double predictor; the
+// kernel is in tracker_kernel.cuh, the double-predictor launches in
+// tracker_fp64.cu.
+#include "tracker_kernel.cuh"
 
 namespace phc {
 
-
-template <class N>
-__device__ double cta_maxmag(int n, const double *v, double *red) {
-  double a = 0.0;
-  for (int i = ctid(); i < n; i += blockDim.x) {
-    const double m = N::mag(ldn_at<N>(v, i));
-    a = (m != m) ? INFINITY : fmax(a, m);  // a NaN reads as infinity
-  }
-  return block_max(a, red);
-}
-
-// max_i |h_i(x, t)| at a point, in precision N
-template <class N>
-__device__ double point_residual(const TrackDev &S, int s, int n, double t, const double *x, double *h, double *Vc,
-                                 double *Gc, double *red) {
-  hom_eval_cta<N>(S, s, 0, t, x, 1, Vc, Gc, h, nullptr);
-  return cta_maxmag<N>(n, h, red);
-}
-
-template <class N>
-__device__ typename N::T horner(const double *a, int deg, const typename N::T &z) {
-  typename N::T acc = ldn_at<N>(a, deg);
-  for (int i = deg - 1; i >= 0; --i) acc = N::add(N::mul(acc, z), ldn_at<N>(a, i));
-  return acc;
-}
-
-// Evaluate the Pade approximants at step st into xp, and return the mixed
-// residual (1/n) sum_i |h_i(xp, t+st)| / (|h|_i(|xp|, t+st) + 1) of
-// Solutions/standard_mixed_residuals.adb:472, where |h| has the moduli of
-// the coefficients at t+st.  Predictor_Feedback,
-// Curves/standard_predictor_convolutions.adb:958-993.
-template <class PN>
-__device__ TRACK_FN double pade_mixres(const TrackDev &S, int s, int n, int K, int dendeg, double t, double st,
-                              const double *num, const double *den, const int *degs, double *xp, double *V,
-                              double *G, double *hs, double *red) {
-  const int Wp = PN::width;
-  for (int i = ctid(); i < n; i += blockDim.x) {
-    const typename PN::T z = PN::from(st);
-    const typename PN::T nv = horner<PN>(num + (long)i * (K + 1) * Wp, degs[2 * i], z);
-    const typename PN::T dv = horner<PN>(den + (long)i * (dendeg + 1) * Wp, degs[2 * i + 1], z);
-    stn_at<PN>(xp, i, PN::div(nv, dv));
-  }
-  __syncthreads();
-  hom_eval_cta<PN>(S, s, 0, t + st, xp, 1, V, G, hs, nullptr);
-  // one warp per equation, lanes over its terms
-  const int lane = ctid() & 31, warp = ctid() >> 5, nw = blockDim.x >> 5;
-  double part = 0.0;
-  for (int i = warp; i < n; i += nw) {
-    double ab = 0.0;
-    const int eq = S.eq_off[s] + i;
-    for (int tr = S.term_off[eq] + lane; tr < S.term_off[eq + 1]; tr += 32) {
-      const int gm = S.term_mono[tr];
-      // |(1 - t') a + t' b| at t' = t + st
-      double v = hypot(fma(S.term_b[2 * tr] - S.term_a[2 * tr], t + st, S.term_a[2 * tr]),
-                       fma(S.term_b[2 * tr + 1] - S.term_a[2 * tr + 1], t + st, S.term_a[2 * tr + 1]));
-      for (int u = 0; u < S.mono_nvr[gm]; ++u) {
-        const double xa = PN::mag(ldn_at<PN>(xp, S.mono_idx[(long)gm * S.maxvar + u]));
-        for (int e = 0; e < S.mono_exp[(long)gm * S.maxvar + u]; ++e) v *= xa;
-      }
-      ab += v;
-    }
-    for (int o = 16; o > 0; o >>= 1) ab += __shfl_xor_sync(0xffffffffu, ab, o);
-    if (lane == 0) part += PN::mag(ldn_at<PN>(hs, i)) / (ab + 1.0);
-  }
-  return block_sum<md::num<double, false> >(part, red) / n;
-}
-
-// Track the paths of one CTA.  PN: predictor numbers, CN: corrector
-// (double-double), RN: refinement.  Output per path: xend (maxdim complex
-// quad-doubles), info (status, steps, rejected), dinfo (t, residual).
-// Resident CTAs per SM asked of the compiler (a register budget): 8 for the
-// precision-split tracker (double predictor, double-double refinement), whose
-// shared memory per path is small enough for 8 paths per SM; 1 otherwise.
-// The WIDE variant of the split tracker asks for one CTA fewer (72 registers
-// per thread instead of 64: fewer spills, each step a little faster); a batch
-// that fits on the GPU in one wave at that occupancy is launched with it.
-template <class PN, class RN, bool WIDE>
-struct track_min_blocks {
-  static const bool split = PN::width <= 2 && RN::width <= 4;
-  static const int value = split ? (WIDE ? TRACK_MINB - 1 : TRACK_MINB) : 1;
-};
-
-template <class PN, class CN, class RN, bool WIDE>
-__global__ void __launch_bounds__(kTrackThreads, (track_min_blocks<PN, RN, WIDE>::value))
-    k_track(TrackDev S, TrackParDev P, int npaths, int path_begin, const int *__restrict__ path_sys,
-            const double *__restrict__ x0, int *queue, const float *__restrict__ model, double *__restrict__ xend,
-            int *__restrict__ info, double *__restrict__ dinfo, float *__restrict__ log, int log_cap,
-            int *__restrict__ log_count) {
-  extern __shared__ __align__(16) double sm[];
-  __shared__ int cur;
-  const int K = P.deg;
-  const int Wp = PN::width, Wr = RN::width;
-  const int n_max = S.maxdim;
-  int nm_max = 0;
-  for (int s = 0; s < S.nsys; ++s) nm_max = max(nm_max, S.mono_off[s + 1] - S.mono_off[s]);
-  const TrackLayout L = track_layout(n_max, K, P.dendeg, nm_max, S.maxvar, Wp, Wr, S.gstaged);
-  double *red = sm + L.red;
-  int *piv = reinterpret_cast<int *>(sm + L.piv);
-  double *dinv = sm + L.dinv;
-  track_pick_lead();
-  int next_static = blockIdx.x;
-  for (;;) {
-    if (queue) {
-      if (ctid() == 0) cur = atomicAdd(queue, 1);
-      __syncthreads();
-    } else {
-      if (ctid() == 0) cur = next_static;
-      __syncthreads();
-      next_static += gridDim.x;
-    }
-    const int p = cur;
-    __syncthreads();
-    if (p >= npaths) break;
-    const int path = path_begin + p;
-    const int s = path_sys[path];
-    const int n = S.dim[s];
-    double *xc = sm + L.xc;
-    // start point, refined at t = 0
-    for (int i = ctid(); i < n; i += blockDim.x) {
-      const double *z = x0 + ((long)path * n_max + i) * 2;
-      stn_at<CN>(xc, i, cnum<CN>(z[0], z[1]));
-    }
-    __syncthreads();
-    double t = 0.0, dxn;
-    point_newton<CN, PN>(S, s, n, 0.0, xc, sm + L.hc, sm + L.Jc, sm + L.Vc, sm + L.Gc, piv, dinv, red, P.corsteps,
-                     P.tolres, 1, &dxn);
-    int status = 2, nsteps = 0, nrej = 0;
-    bool failed = false;
-    for (int step_it = 0; step_it < P.maxsteps; ++step_it) {
-      // ---------------- predictor: the Taylor series of the path in PN
-      // x(s) = x_0 + x_1 s + ... + x_K s^K solves h(x(s), t + s) = 0 to
-      // degree K.  Its coefficients follow one degree at a time from the
-      // LU of J_0 = dh/dx at the point: x_k = -J_0^{-1} [h(x_0 + ... +
-      // x_{k-1} s^{k-1}, t + s)]_k.  This is the fixed point that Newton's
-      // method on power series (LU_Prediction,
-      // Curves/standard_predictor_convolutions.adb:1142-1185, J_0 factored
-      // once by lufac) converges to, computed without the Jacobian series:
-      // K coefficient evaluations and K products with J_0^{-1}.
-      double *xs = sm + L.xs;
-      for (int t2 = ctid(); t2 < n * (K + 1); t2 += blockDim.x) {
-        const int i = t2 / (K + 1), k = t2 % (K + 1);
-        typename PN::T v = PN::zero();
-        if (k == 0) v = conv_num<CN, PN>::go(ldn_at<CN>(xc, i));
-        stn_at<PN>(xs, t2, v);
-      }
-      __syncthreads();
-      hom_eval_cta<PN>(S, s, 0, t, xs, K + 1, sm + L.V, sm + L.G, sm + L.hs, sm + L.J0);
-      if (ctid() < 32) {
-        warp_lufac<PN>(n, sm + L.J0, piv, dinv);
-        warp_luinverse<PN>(n, sm + L.J0, piv, dinv, sm + L.M);
-      }
-      __syncthreads();
-      for (int k = 1; k <= K; ++k) {
-        hom_coef_cta<PN>(S, s, k, t, xs, K + 1, sm + L.V, sm + L.r);
-        for (int i = ctid(); i < n; i += blockDim.x) {
-          typename PN::T acc = PN::zero();
-          for (int j = 0; j < n; ++j)
-            acc = PN::add(acc, PN::mul(ldn_at<PN>(sm + L.M, (long)i * n + j), ldn_at<PN>(sm + L.r, j)));
-          stn_at<PN>(xs, (long)i * (K + 1) + k, PN::neg(acc));
-        }
-        __syncthreads();
-      }
-      // ---------------- Pade and the pole step
-      int pdeg_i = 0, qdeg_i = 0;
-      double rmin = 1e300;
-      double *num = sm + L.num, *den = sm + L.den;
-      for (int i = ctid(); i < n; i += blockDim.x) {
-        const double *ci = xs + (long)i * (K + 1) * Wp;
-        pdeg_i = pade_one<PN>(P.numdeg, P.dendeg, K, ci, num + (long)i * (K + 1) * Wp, den + (long)i * (P.dendeg + 1) * Wp);
-        qdeg_i = (pdeg_i == P.numdeg) ? P.dendeg : 0;
-        const double cd = PN::mag(ldn_at<PN>(ci, K - 2));
-        if (cd != 0.0) rmin = fmin(rmin, PN::mag(ldn_at<PN>(ci, K - 3)) / cd);
-        double *mg = sm + L.mag + (long)i * (K + 1);
-        for (int k = 0; k <= K; ++k) mg[k] = PN::mag(ldn_at<PN>(ci, k));
-      }
-      // per-component Pade degrees go to shared memory for the evaluations
-      int *degs = reinterpret_cast<int *>(sm + L.degs);
-      if (ctid() < n) {
-        degs[2 * ctid()] = pdeg_i;
-        degs[2 * ctid() + 1] = qdeg_i;
-      }
-      const double r = block_min(rmin, red);
-      const bool rfail = !(r < 1e299);
-      double pole_step = rfail ? P.maxsize : P.pbeta * r;
-      if (pole_step > P.maxsize) pole_step = P.maxsize;
-      double step = pole_step;
-      bool learned = false;
-      float *feat = reinterpret_cast<float *>(sm + L.feat);
-      if ((P.step_mode == 1 && model != nullptr) || log != nullptr) {
-        track_features(ctid(), n, K, t, pole_step, sm + L.mag, feat);
-        __syncthreads();
-      }
-      if (P.step_mode == 1 && model != nullptr) {
-        const float lr = mlp_forward_cta(model, feat, reinterpret_cast<float *>(sm + L.hbuf));
-        const double prop = pole_step * exp((double)lr) * P.learn_scale;
-        if (prop > P.minsize && prop == prop) {
-          step = fmin(prop, P.maxsize);
-          learned = true;
-        }
-      }
-      const double step0 = step;
-      bool accepted = false;
-      for (int attempt = 0; attempt < 2 && !accepted; ++attempt) {
-        if (attempt == 1) {
-          // the learned proposal was rejected: redo the step with the plain one
-          if (!learned) break;
-          learned = false;
-          step = pole_step;
-        }
-        if (t + step > 1.0) step = 1.0 - t;
-        // predictor feedback on the mixed residual
-        double *xp = sm + L.xp;
-        bool ok = false;
-        for (int h = 0; h < 64; ++h) {
-          const double mixres = pade_mixres<PN>(S, s, n, K, P.dendeg, t, step, num, den, degs, xp, sm + L.V,
-                                                sm + L.G, sm + L.hs, red);
-          if (mixres < P.alpha) { ok = true; break; }
-          step *= 0.5;
-          ++nrej;
-          if (step < P.minsize) break;
-        }
-        if (!ok) {
-          if (learned) continue;  // the plain step gets its own feedback
-          failed = true;
-          break;
-        }
-        // corrector with step halving
-        bool cok = false;
-        for (int h = 0; h < 64; ++h) {
-          for (int i = ctid(); i < n; i += blockDim.x)
-            stn_at<CN>(xc, i, conv_num<PN, CN>::go(ldn_at<PN>(xp, i)));
-          __syncthreads();
-          if (point_newton<CN, PN>(S, s, n, t + step, xc, sm + L.hc, sm + L.Jc, sm + L.Vc, sm + L.Gc, piv, dinv, red,
-                               P.corsteps, P.tolres, 1, &dxn)) {
-            cok = true;
-            break;
-          }
-          ++nrej;
-          if (learned) break;  // rejected proposal: retry with the plain step
-          step *= 0.5;
-          if (step < P.minsize) break;
-          for (int i = ctid(); i < n; i += blockDim.x) {
-            const typename PN::T z = PN::from(step);
-            const int pd = degs[2 * i], qd = degs[2 * i + 1];
-            stn_at<PN>(xp, i, PN::div(horner<PN>(num + (long)i * (K + 1) * Wp, pd, z),
-                                      horner<PN>(den + (long)i * (P.dendeg + 1) * Wp, qd, z)));
-          }
-          __syncthreads();
-        }
-        if (cok) { accepted = true; break; }
-        if (learned) continue;  // rejected proposal: redo with the plain step
-        failed = true;
-        break;
-      }
-      if (failed || !accepted) { failed = true; break; }
-      // training log: features, accepted step, plain step, proposal, t and
-      // the largest probed step (pole step times 1.5, 2, 3, 4, 6, at most
-      // maxsize and 1 - t) whose Pade prediction still passes the feedback
-      if (log != nullptr) {
-        double best = step;
-        const double mults[5] = {1.5, 2.0, 3.0, 4.0, 6.0};
-        for (int q = 0; q < 5; ++q) {
-          double sp = fmin(pole_step * mults[q], P.maxsize);
-          if (t + sp > 1.0) sp = 1.0 - t;
-          if (sp <= best) continue;
-          const double mr = pade_mixres<PN>(S, s, n, K, P.dendeg, t, sp, num, den, degs, sm + L.xp, sm + L.V,
-                                            sm + L.G, sm + L.hs, red);
-          if (mr < P.alpha) best = sp;
-        }
-        if (ctid() == 0) {
-          const int slot = atomicAdd(log_count, 1);
-          if (slot < log_cap) {
-            float *f = log + (long)slot * 32;
-            for (int q = 0; q < 24; ++q) f[q] = feat[q];
-            f[24] = (float)step;
-            f[25] = (float)pole_step;
-            f[26] = (float)step0;
-            f[27] = (float)t;
-            f[28] = (float)best;
-            for (int q = 29; q < 32; ++q) f[q] = 0.0f;
-          }
-        }
-      }
-      t += step;
-      ++nsteps;
-      if (fabs(1.0 - t) < P.epsilon) { status = 0; break; }
-    }
-    // ---------------- refinement and classification
-    double *xr = sm + L.xc;  // reuse the corrector slots at the refinement width
-    // xc holds CN numbers: widen in place from the top (RN width >= CN width)
-    if (RN::width != CN::width) {  // n <= blockDim.x: one number per thread
-      typename CN::T v = CN::zero();
-      if (ctid() < n) v = ldn_at<CN>(xc, ctid());
-      __syncthreads();
-      if (ctid() < n) stn_at<RN>(xr, ctid(), conv_num<CN, RN>::go(v));
-      __syncthreads();
-    }
-    double res;
-    if (!failed && status == 0) {
-      point_newton<RN, RN>(S, s, n, 1.0, xr, sm + L.hc, sm + L.Jc, sm + L.Vc, sm + L.Gc, piv, dinv, red, P.refine_steps,
-                       0.0, 0, &dxn);
-      res = point_residual<RN>(S, s, n, 1.0, xr, sm + L.hc, sm + L.Vc, sm + L.Gc, red);
-      status = (res <= P.restol) ? 0 : 3;
-    } else {
-      res = point_residual<RN>(S, s, n, t, xr, sm + L.hc, sm + L.Vc, sm + L.Gc, red);
-      status = failed ? 1 : 2;
-    }
-    // end points as complex quad-doubles (octo-doubles for an octo-double
-    // refinement), lower limbs zero below the refinement precision
-    const int XL = RN::tr::limbs > 4 ? 8 : 4;
-    for (int q = ctid(); q < n_max * 2 * XL; q += blockDim.x) {
-      const int i = q / (2 * XL), c = q % (2 * XL);
-      double v = 0.0;
-      if (i < n) {
-        const int lim = RN::tr::limbs;
-        const int part = c / XL, limb = c % XL;
-        if (limb < lim) v = xr[(long)i * RN::width + part * lim + limb];
-      }
-      xend[((long)path * n_max) * 2 * XL + q] = v;
-    }
-    if (ctid() == 0) {
-      info[3 * path] = status;
-      info[3 * path + 1] = nsteps;
-      info[3 * path + 2] = nrej;
-      dinfo[2 * path] = t;
-      dinfo[2 * path + 1] = res;
-    }
-    __syncthreads();
-  }
-}
-
-
-}  // namespace phc
-
-namespace phc {
+int track_fp64(const TrackDev &S, const TrackParDev &P, int nmono_max, int npaths, const int *path_sys,
+               const double *x0, int rmode, const void *model, double *xend, int *info, double *dinfo, float *log,
+               int log_cap, int *log_count, int *queue, int one_per_launch, cudaStream_t st);
 
 long track_smem_bytes(int maxdim, int K, int M, int nmono_max, int maxvar, int pmode, int rmode, int gst) {
   const int Wp = 2 * pmode, Wr = 2 * rmode;
   return track_layout(maxdim, K, M, nmono_max, maxvar, Wp, Wr, gst).total * (long)sizeof(double);
-}
-
-template <class PN, class CN, class RN>
-static int track_launch(const TrackDev &S, const TrackParDev &P, int nmono_max, int npaths, const int *path_sys,
-                        const double *x0, const void *model, double *xend, int *info, double *dinfo, float *log,
-                        int log_cap, int *log_count, int *queue, int one_per_launch, cudaStream_t st) {
-  const long smem = track_smem_bytes(S.maxdim, P.deg, P.dendeg, nmono_max, S.maxvar, PN::tr::limbs, RN::tr::limbs, S.gstaged);
-  if (smem > 227 * 1024) {
-    set_error("track: %ld bytes of shared memory needed (dim %d, degree %d, %d monomials)", smem, S.maxdim, P.deg,
-              nmono_max);
-    return PHC_ERR_LIMIT;
-  }
-  auto kern = k_track<PN, CN, RN, false>;
-  PHC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  const float *mdl = reinterpret_cast<const float *>(model);
-  if (one_per_launch) {
-    // the plain arrangement: one launch (one CTA) per path, back to back
-    for (int p = 0; p < npaths; ++p) {
-      kern<<<1, kTrackThreads, smem, st>>>(S, P, 1, p, path_sys, x0, nullptr, mdl, xend, info, dinfo, log, log_cap,
-                                           log_count);
-      PHC_CHECK_LAUNCH();
-    }
-    return PHC_OK;
-  }
-  int dev = 0, nsm = 148, per = 1;
-  PHC_CUDA(cudaGetDevice(&dev));
-  PHC_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-  PHC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, kTrackThreads, smem));
-  if (per < 1) per = 1;
-  if constexpr (track_min_blocks<PN, RN, true>::split) {
-    // one wave at the lower occupancy: take the variant with more registers
-    auto wide = k_track<PN, CN, RN, true>;
-    PHC_CUDA(cudaFuncSetAttribute(wide, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    int per_w = 0;
-    PHC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_w, wide, kTrackThreads, smem));
-    if (per_w >= 1 && (long)npaths <= (long)nsm * per_w) {
-      kern = wide;
-      per = per_w;
-    }
-  }
-  long grid = (long)nsm * per;
-  if (grid > npaths) grid = npaths;
-  if (grid < 1) return PHC_OK;
-  PHC_CUDA(cudaMemsetAsync(queue, 0, sizeof(int), st));
-  kern<<<(unsigned)grid, kTrackThreads, smem, st>>>(S, P, npaths, 0, path_sys, x0, queue, mdl, xend, info, dinfo, log,
-                                                     log_cap, log_count);
-  PHC_CHECK_LAUNCH();
-  return PHC_OK;
 }
 
 // The checks of the modes, the dimension and the series and Pade degrees.
@@ -440,20 +33,14 @@ int track(const TrackDev &S, const TrackParDev &P, int nmono_max, int npaths, co
   PHC_REQUIRE(queue != nullptr || one_per_launch, "track: the batched launch needs a queue counter");
   PHC_REQUIRE(model == nullptr || (reinterpret_cast<unsigned long long>(model) & 15) == 0, "track: the model buffer is not 16-byte aligned");
   if (npaths == 0) return PHC_OK;
-  typedef md::num<double, true> Z1;
+  if (pmode == 1)
+    return track_fp64(S, P, nmono_max, npaths, path_sys, x0, rmode, model, xend, info, dinfo, log, log_cap, log_count,
+                      queue, one_per_launch, st);
   typedef md::num<md::dd, true> Z2;
   typedef md::num<md::qd, true> Z4;
   typedef md::num<md::od, true> Z8;
   if (rmode == 8)
-    return pmode == 1 ? track_launch<Z1, Z2, Z8>(S, P, nmono_max, npaths, path_sys, x0, model, xend, info, dinfo, log,
-                                                 log_cap, log_count, queue, one_per_launch, st)
-                      : track_launch<Z2, Z2, Z8>(S, P, nmono_max, npaths, path_sys, x0, model, xend, info, dinfo, log,
-                                                 log_cap, log_count, queue, one_per_launch, st);
-  if (pmode == 1 && rmode == 2)
-    return track_launch<Z1, Z2, Z2>(S, P, nmono_max, npaths, path_sys, x0, model, xend, info, dinfo, log, log_cap,
-                                    log_count, queue, one_per_launch, st);
-  if (pmode == 1)
-    return track_launch<Z1, Z2, Z4>(S, P, nmono_max, npaths, path_sys, x0, model, xend, info, dinfo, log, log_cap,
+    return track_launch<Z2, Z2, Z8>(S, P, nmono_max, npaths, path_sys, x0, model, xend, info, dinfo, log, log_cap,
                                     log_count, queue, one_per_launch, st);
   if (rmode == 2)
     return track_launch<Z2, Z2, Z2>(S, P, nmono_max, npaths, path_sys, x0, model, xend, info, dinfo, log, log_cap,
