@@ -143,3 +143,22 @@ def test_track_dimension_extremes_vs_oracle(n):
         a = -target[0][1][1].real
         x = g.endpoints(pb.maxdim)[:, 0]
         assert np.allclose(np.sort(x.real), [-np.sqrt(a), np.sqrt(a)], atol=1e-14)
+
+
+def test_track_batch_beyond_one_wave_matches_smaller_batches():
+    """1,200 paths are more than the GPU holds at 7 paths per SM, so they run
+    in the 8-paths-per-SM (64-register) variant; two batches of 600 fit and run
+    in the 72-register variant.  Both give the same classification and end
+    points."""
+    pb5 = hm.config5()
+    pb = hm.subset(pb5, np.arange(1200))
+    whole = hm.track_host(pb, pmode=1, rmode=2)
+    a = hm.track_host(hm.subset(pb5, np.arange(600)), pmode=1, rmode=2)
+    b = hm.track_host(hm.subset(pb5, np.arange(600, 1200)), pmode=1, rmode=2)
+    status = np.concatenate([a.status, b.status])
+    assert np.array_equal(whole.status, status)
+    ok = whole.status == 0
+    assert ok.sum() >= 200  # most paths of these sparse systems diverge
+    d = endpoint_diff(pb, whole.xend, np.concatenate([a.xend, b.xend]), 2)
+    scale = np.maximum(1.0, np.abs(whole.endpoints(pb.maxdim)).max(axis=1))
+    assert (d[ok] <= 1e-26 * scale[ok]).all()
