@@ -41,6 +41,43 @@ int newton_step(int prec, int cplx, int nsys, int dim, int deg, int maxdeg, int 
                 double *series, double *Q, double *R, int *flags, double *work, cudaStream_t st);
 
 // device scratch owned for the duration of one host call
+// Two streams that start after the work already on a caller's stream and
+// that the caller's stream waits for at the end (join); without pipelining
+// the caller's stream is used alone.
+struct StreamPair {
+  cudaStream_t q[2] = {nullptr, nullptr};
+  cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+  cudaStream_t base = nullptr;
+  bool two = false;
+  ~StreamPair() {
+    for (auto &e : ev)
+      if (e) cudaEventDestroy(e);
+    for (auto &s : q)
+      if (s) cudaStreamDestroy(s);
+  }
+  int make(cudaStream_t st, bool pipelined) {
+    base = st;
+    two = pipelined;
+    if (!two) return PHC_OK;
+    for (auto &e : ev) PHC_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    PHC_CUDA(cudaEventRecord(ev[0], st));
+    for (auto &s : q) {
+      PHC_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+      PHC_CUDA(cudaStreamWaitEvent(s, ev[0], 0));
+    }
+    return PHC_OK;
+  }
+  cudaStream_t get(int c) const { return two ? q[c & 1] : base; }
+  int join(cudaStream_t st) {
+    if (!two) return PHC_OK;
+    for (int i = 0; i < 2; ++i) {
+      PHC_CUDA(cudaEventRecord(ev[1 + i], q[i]));
+      PHC_CUDA(cudaStreamWaitEvent(st, ev[1 + i], 0));
+    }
+    return PHC_OK;
+  }
+};
+
 struct dbuf {
   void *p = nullptr;
   ~dbuf() {
@@ -106,12 +143,31 @@ int phc_system_evaldiff_host(int prec, int cplx, int nsys, int dim, int deg, int
   PHC_CUDA(cudaMemcpyAsync(d_nvr, nvr, b_nvr, cudaMemcpyHostToDevice, st));
   PHC_CUDA(cudaMemcpyAsync(d_idx, idx, b_idx, cudaMemcpyHostToDevice, st));
   PHC_CUDA(cudaMemcpyAsync(d_exp, exps, b_idx, cudaMemcpyHostToDevice, st));
-  PHC_CUDA(cudaMemcpyAsync(d_cst, cst, b_cst, cudaMemcpyHostToDevice, st));
-  PHC_CUDA(cudaMemcpyAsync(d_cff, cff, b_cff, cudaMemcpyHostToDevice, st));
-  PHC_CUDA(cudaMemcpyAsync(d_in, input, b_in, cudaMemcpyHostToDevice, st));
-  rc = system_evaldiff(prec, cplx, nsys, dim, deg, maxvar, d_off, d_nvr, d_idx, d_exp, d_cst, d_cff, d_in, d_out, st);
+  // The systems in chunks on two streams: the copies of one chunk in and
+  // of another out overlap the evaluation of a third.  A chunk's
+  // coefficients are the contiguous rows of its monomials; the kernel
+  // indexes monomials globally and everything else from the chunk's start.
+  const int nchunk = nsys >= 64 ? 8 : 1;
+  StreamPair sp;
+  rc = sp.make(st, nchunk > 1);
   if (rc) return rc;
-  PHC_CUDA(cudaMemcpyAsync(output, d_out, b_out, cudaMemcpyDeviceToHost, st));
+  for (int c = 0; c < nchunk; ++c) {
+    cudaStream_t q = sp.get(c);
+    const long s0 = (long)nsys * c / nchunk, s1 = (long)nsys * (c + 1) / nchunk;
+    if (s1 == s0) continue;
+    const long r0 = s0 * dim, r1 = s1 * dim;
+    const long m0 = mon_off[r0], m1 = mon_off[r1];
+    PHC_CUDA(cudaMemcpyAsync(d_cst + r0 * S, cst + r0 * S, (r1 - r0) * S * sizeof(double), cudaMemcpyHostToDevice, q));
+    PHC_CUDA(cudaMemcpyAsync(d_cff + m0 * S, cff + m0 * S, (m1 - m0) * S * sizeof(double), cudaMemcpyHostToDevice, q));
+    PHC_CUDA(cudaMemcpyAsync(d_in + r0 * S, input + r0 * S, (r1 - r0) * S * sizeof(double), cudaMemcpyHostToDevice, q));
+    rc = system_evaldiff(prec, cplx, (int)(s1 - s0), dim, deg, maxvar, d_off + r0, d_nvr, d_idx, d_exp, d_cst + r0 * S,
+                         d_cff, d_in + r0 * S, d_out + r0 * (dim + 1) * S, q);
+    if (rc) return rc;
+    PHC_CUDA(cudaMemcpyAsync(output + r0 * (dim + 1) * S, d_out + r0 * (dim + 1) * S,
+                             (r1 - r0) * (dim + 1) * S * sizeof(double), cudaMemcpyDeviceToHost, q));
+  }
+  rc = sp.join(st);
+  if (rc) return rc;
   PHC_CUDA(cudaStreamSynchronize(st));
   return PHC_OK;
 }

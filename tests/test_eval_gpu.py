@@ -100,6 +100,15 @@ def test_eval_host_entry_point_matches_device():
     assert np.array_equal(a, c)
 
 
+def test_eval_host_entry_point_pipelined_chunks():
+    # 70 systems: the host entry copies and evaluates them in 8 uneven
+    # chunks on two streams; the result equals one device launch bit for bit
+    b = wl.eval_batch(6, 70, 6, 7, 5, 3, 2, True, expmax=2)
+    a = series.system_evaldiff_host(b)
+    c = run_device(b)
+    assert np.array_equal(a, c)
+
+
 def test_eval_reference_shaped_single_polynomial():
     d = golden_io.load("eval_dd_real")
     b = golden_io.batch(d)
