@@ -116,3 +116,16 @@ def test_bals_skip_rules():
                                         flags=(0, 0, 0, 0, 1), Q=Qo, R=Ro)
     assert fl2[1] == 1 and np.array_equal(fl2, flo2)
     assert check_bals(sol2, so2, prec, cplx, degp1, n)
+
+
+def test_bals_host_entry_matches_device_entry():
+    # 70 instances through the host entry and through the device entry:
+    # solutions and flags equal bit for bit
+    prec, cplx, n, szt, degp1, ninst = 2, True, 8, 4, 4, 70
+    rng = np.random.default_rng(70)
+    mat = batch_of([wl.random_numbers(rng, (degp1, n, n), prec, cplx, "normal") for _ in range(ninst)])
+    rhs = batch_of([wl.random_numbers(rng, (degp1, n), prec, cplx, "normal") for _ in range(ninst)])
+    sol, _, _, _, fl = dense.bals_solve_host(prec, cplx, mat.copy(), rhs.copy(), ninst, n, degp1, szt)
+    sol2, fl2 = dense.bals_solve_wy(prec, cplx, mat, rhs, ninst, n, degp1, szt, wy=0)
+    assert np.array_equal(fl, fl2)
+    assert np.array_equal(sol, sol2)
