@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define PHC_ABI_VERSION 1
+#define PHC_ABI_VERSION 2
 
 const char *phc_last_error(void);
 int phc_abi_version(void);
@@ -54,6 +54,11 @@ int phc_abi_version(void);
 int phc_system_evaldiff(int prec, int cplx, int nsys, int dim, int deg, int maxvar, const int *mon_off,
                         const int *nvr, const int *idx, const int *exps, const double *cst, const double *cff,
                         const double *input, double *output, void *stream);
+/* The host entry copies the systems in, evaluates and copies out in chunks
+ * on two streams; the copies overlap the evaluation only when the host
+ * arrays are pinned (cudaHostAlloc / cudaHostRegister): with pageable
+ * memory each copy out blocks the issuing thread and the chunks run one
+ * after another. */
 int phc_system_evaldiff_host(int prec, int cplx, int nsys, int dim, int deg, int maxvar, const int *mon_off,
                              const int *nvr, const int *idx, const int *exps, const double *cst,
                              const double *cff, const double *input, double *output, void *stream);
@@ -129,7 +134,9 @@ int phc_bals_solve_wy(int prec, int cplx, int ninst, int dim, int degp1, int szt
  * (8 MiB, held by every GPU that loads the library until exit); larger
  * requests fail with -3.  All calls share that array: calls that overlap on
  * the GPU race and must be serialised.  The first call on a device looks up
- * the array's address and should come before any stream capture. */
+ * the array's address and should come before any stream capture; the
+ * address is kept for the process, so do not use the library across a
+ * device reset (cudaDeviceReset). */
 long long phc_bals_solve_static_capacity_bytes(void);
 int phc_bals_solve_static(int prec, int cplx, int ninst, int dim, int degp1, int szt, int tailidx, const double *mat,
                           double *rhs, double *sol, double *Q, double *R, int *flags, void *stream);
@@ -189,7 +196,17 @@ int phc_newton_host(int prec, int cplx, int nsys, int dim, int deg, int szt, int
  *   coefficients are computed one degree at a time, the fixed point those
  *   steps approach), corsteps, maxsteps, refine_steps.
  * dpar: pbeta, alpha, maxsize, minsize, tolres, epsilon, restol (endpoint
- *   residual bound), learn_scale (multiplies learned proposals; 0 = 1).
+ *   residual bound), learn_scale (multiplies learned proposals; 0 = 1),
+ *   cbeta (the curvature step's factor, beta2; 0.005 in the reference's
+ *   defaults, Curves/homotopy_continuation_parameters.adb:13).
+ * Step rule per predictor step (LU_Prediction,
+ *   Curves/standard_predictor_convolutions.adb:1170-1184, with Hesse_Pade as
+ *   in Curves/dobldobl_predictor_convolutions.adb:383-406): the smallest of
+ *   the pole step pbeta * r (r the smallest Fabry radius |c_{K-3}/c_{K-2}|;
+ *   maxsize when no component has a radius), the curvature step
+ *   (cbeta eta / |Pade errors|_2)^(1/K) with eta = 2 sigma_min(J) /
+ *   |(sigma_max(H_1), ..., sigma_max(H_n))|_2 at the current point, and
+ *   maxsize; a step that reaches 1 - minsize goes to t = 1 (Bounded_Update).
  * pmode: 1 (double) or 2 (double-double), the precision of the predictor
  *   and of the corrector's Jacobian and linear solves; the corrector's
  *   residuals and updates are double-double; rmode: refinement precision 2,
@@ -197,11 +214,14 @@ int phc_newton_host(int prec, int cplx, int nsys, int dim, int deg, int szt, int
  * step_mode 1 with a model (phc_mlp_*) uses the learned step proposer; a
  *   proposal whose feedback or corrector fails is redone with the plain step.
  * Output per path: xend maxdim complex quad-doubles, octo-doubles for rmode
- *   8 (lower limbs zero below rmode), info[3p..3p+2] = status (0 success, 1 step below minsize,
- *   2 maxsteps reached, 3 endpoint residual above restol), steps, rejected
- *   steps; dinfo[2p..2p+1] = final t, endpoint residual.
+ *   8 (lower limbs zero below rmode), info[6p..6p+5] = status (0 success,
+ *   1 step below minsize, 2 maxsteps reached, 3 endpoint residual above
+ *   restol), steps, rejected steps, and how often the step was the pole
+ *   step, the curvature step and maxsize (the reference's nbpole, nbhess,
+ *   nbmaxm); dinfo[2p..2p+1] = final t, endpoint residual.
  * log: when not NULL, each accepted step appends 32 floats (24 features,
- *   accepted step, plain step, proposed step, t) up to log_cap records;
+ *   accepted step, plain step, proposed step, t, largest probed step that
+ *   passes the feedback) up to log_cap records;
  *   *log_count counts them.  queue: one device int (the work-queue counter).
  * one_per_launch != 0 tracks one path per launch (one CTA), back to back:
  *   the plain arrangement the batched kernel is measured against. */
@@ -230,6 +250,51 @@ int phc_track_host(int nsys, const int *dim, int maxvar, const int *mono_off, co
                    const int *path_sys, const double *x0, const int *ipar, const double *dpar, int pmode, int rmode,
                    int step_mode, const void *model, double *xend, int *info, double *dinfo, void *stream);
 void phc_track_host_release(void);
+
+/* ------------------------------------------- the tracker's drop-in entry
+ * gpumanypaths_d, gpumanypaths_dd, gpumanypaths_qd replace the functions of
+ * the same names and signatures in Ada/PHCtoC/gpumanypaths_d.h,
+ * gpumanypaths_dd.h:27 and gpumanypaths_qd.h (bodies gpumanypaths_dd.cpp
+ * :18-62), which phcpy calls as py2c_gpu_manypaths_dd(mode, verbose,
+ * regamma, imgamma) (Mod/phcpy2cpath_dd.cpp:4593).  Like them, they read
+ * the target system p, the start system q and the start solutions from the
+ * containers, track every path of (1 - t) gamma q + t p with gamma =
+ * regamma + i imgamma, and write the end points back into the solution
+ * container.  mode: 0 (CPU and GPU in the reference; here the GPU, whose
+ * end points the reference writes back in this mode too), 1 (CPU only:
+ * refused, -1, as this library tracks on the GPU), 2 (GPU); verbose > 0
+ * prints what the reference prints.  Returns 0 when the paths were tracked
+ * (per-path status in the container), < 0 on an error.  End points are
+ * refined in double-double (_d, _dd) or quad-double (_qd); the tracker is
+ * phc_track_host with the parameters of phc_container_set_parameters
+ * (default: degree 8, [4/4] Pade, the reference's step rules).
+ *
+ * The containers: PHCpack keeps the systems and solutions in its Ada
+ * containers (syscon, solcon), which need the Ada runtime; this library
+ * keeps its own with the same content.  A system of neq polynomials in
+ * nvar variables: polynomial i has nterms[i] terms; term r (the terms of
+ * all polynomials in order) has the exponents exps[r*nvar .. r*nvar+nvar-1]
+ * and the complex coefficient cff[2r] + i cff[2r+1] (rounded to double, as
+ * the tracker's coefficients are doubles).  Solutions: coordinate j of
+ * solution s has the limbs doubles per part (1, 2 or 4) at
+ * sols[((s*nvar + j)*2 + part)*limbs + l], part 0 real and 1 imaginary; start
+ * solutions are rounded to double.  After tracking, get_solutions gives the
+ * end points with t, the status (0 success, 1 step below minsize, 2
+ * maxsteps, 3 residual above restol) and the endpoint residual per
+ * solution (any of its output pointers may be NULL). */
+int phc_container_set_target(int neq, int nvar, const int *nterms, const int *exps, const double *cff);
+int phc_container_set_start(int neq, int nvar, const int *nterms, const int *exps, const double *cff);
+int phc_container_set_solutions(int nsols, int nvar, int limbs, const double *sols);
+int phc_container_number_of_solutions(int *nsols);
+/* the number of variables of the solutions (else of the target), 0 when empty */
+int phc_container_dimension(int *nvar);
+int phc_container_get_solutions(int limbs, double *sols, double *t, int *status, double *res);
+/* ipar[7] and dpar[9] as in phc_track */
+int phc_container_set_parameters(const int *ipar, const double *dpar);
+void phc_container_clear(void);
+int gpumanypaths_d(int mode, int verbose, double regamma, double imgamma);
+int gpumanypaths_dd(int mode, int verbose, double regamma, double imgamma);
+int gpumanypaths_qd(int mode, int verbose, double regamma, double imgamma);
 
 /* The mixed volume of the Newton polytopes of a square system in n
  * variables (the BKK bound on its isolated roots with nonzero coordinates):

@@ -16,7 +16,9 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libphcref.so")
-REF_TREE = os.environ.get("PHC_REFERENCE_GPU", "/root/reference/src/GPU")
+# the reference's src/GPU tree, where the reference is present (unset: the
+# reference-backed library is not built)
+REF_TREE = os.environ.get("PHC_REFERENCE_GPU", "")
 
 _D = ctypes.POINTER(ctypes.c_double)
 _I = ctypes.POINTER(ctypes.c_int)
@@ -31,7 +33,7 @@ def build(ref: bool = True) -> None:
     polynomial test program on this library through ref_shim_polynomials.cu;
     needs phcpack_b200/libphcb200.so built first)."""
     targets = ["liboracle.so"]
-    if ref and os.path.isdir(REF_TREE):
+    if ref and REF_TREE and os.path.isdir(REF_TREE):
         targets.append("_ref/libphcref.so")
         if os.path.exists(os.path.join(HERE, "..", "phcpack_b200", "libphcb200.so")):
             targets.append("_ref/test_dbl2_polynomials")
@@ -124,7 +126,7 @@ def reference() -> Lib | None:
     """PHCpack's own host code, or None where it was never built."""
     global _ref
     if _ref is None:
-        if not os.path.exists(REF_SO) and os.path.isdir(REF_TREE):
+        if not os.path.exists(REF_SO) and REF_TREE and os.path.isdir(REF_TREE):
             build(ref=True)
         if not os.path.exists(REF_SO):
             return None
@@ -167,19 +169,22 @@ def newton_steps(lib: Lib, b, deg, nsteps, schedule=0):
     return out, np.concatenate(flags_all)
 
 
-def track(lib: Lib, pb, ipar, dpar, pmode=1, rmode=2, nthreads=1):
+def track(lib: Lib, pb, ipar, dpar, pmode=1, rmode=2, nthreads=1, step_mode=0, model=None):
     """Track the paths of a homotopy TrackProblem on the CPU (the tracker
-    restatement of tracker_oracle.cpp).  Returns (xend, info, dinfo) with
-    the layout of the C ABI (16 doubles per complex end point coordinate for
-    rmode 8, 8 otherwise)."""
+    restatement of tracker_oracle.cpp); step_mode 1 with a model buffer
+    (uint8 array, the device layout) uses the learned step.  Returns (xend,
+    info, dinfo) with the layout of the C ABI (16 doubles per complex end
+    point coordinate for rmode 8, 8 otherwise; 6 ints of info per path)."""
     xend = np.zeros(pb.npaths * pb.maxdim * (16 if rmode == 8 else 8))
-    info = np.zeros(pb.npaths * 3, np.int32)
+    info = np.zeros(pb.npaths * 6, np.int32)
+    m = None if model is None else np.ascontiguousarray(model)
     dinfo = np.zeros(pb.npaths * 2)
     f = lib._fn("track")
     rc = f(pb.nsys, _ip(pb.dim), pb.maxvar, _ip(pb.mono_off), _ip(pb.mono_nvr), _ip(pb.mono_idx), _ip(pb.mono_exp),
            _ip(pb.eq_off), _ip(pb.term_off), _ip(pb.term_mono), _dp(pb.term_a), _dp(pb.term_b), pb.npaths,
-           _ip(pb.path_sys), pb.maxdim, _dp(pb.x0), _ip(ipar), _dp(dpar), pmode, rmode, nthreads, _dp(xend),
-           _ip(info), _dp(dinfo))
+           _ip(pb.path_sys), pb.maxdim, _dp(pb.x0), _ip(ipar), _dp(dpar), pmode, rmode, int(step_mode),
+           None if m is None else m.ctypes.data_as(ctypes.c_void_p), nthreads,
+           _dp(xend), _ip(info), _dp(dinfo))
     assert rc == 0
     return xend, info, dinfo
 

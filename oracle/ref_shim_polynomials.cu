@@ -12,7 +12,7 @@
 // test program Polynomials/test_dbl2_polynomials.cpp and its host sources
 // (read in place, output into oracle/_ref).  The reference's own tester then
 // compares this library's results with its CPU code.  The same file is the
-// binding a maintainer would add to PHCpack.
+// binding a maintainer would add to PHCpack in place of its own kernels.
 //
 // The reference's per-limb arrays (hi, lo; re, im) become the library's
 // limb-interleaved numbers; the polynomial is polynomial 0 of a one-system

@@ -20,9 +20,23 @@
 //    J_0 factored once and applied as its inverse); [L/M] Pade approximant
 //    per component; pole step
 //    pbeta * r with r the smallest Fabry radius |c_{K-3}/c_{K-2}| (offset 2
-//    as in Newton_Fabry); step = min(pole step, maxsize), cut at t = 1;
-//  * the Hessian curvature step (Hesse_Pade, singular values of Hessians)
-//    is left out: the predictor feedback and the corrector bound the step;
+//    as in Newton_Fabry);
+//  * the curvature step (Hesse_Pade, Curves/dobldobl_predictor_convolutions
+//    .adb:383-406): eta = 2 sigma_min(J) / |(sigma_max(H_1), ...,
+//    sigma_max(H_n))|_2 at the current point (Distance,
+//    Curves/singular_values_of_hessians.adb:190-211), the step
+//    (cbeta eta / |Pade error estimates|_2)^(1/K) (Step_Distance,
+//    Curves/series_and_predictors.adb:813-825; Solution_Error,
+//    Curves/homotopy_pade_approximants.adb:687-754); the singular values in
+//    complex double by one-sided Jacobi rotations to convergence;
+//  * step = the smallest of the pole step, the curvature step and maxsize,
+//    counted as pole, curvature or maxsize step (Minimum,
+//    Curves/three_way_minima.adb:48-62); a step reaching 1 - minsize goes to
+//    t = 1 (Bounded_Update, three_way_minima.adb:96-109);
+//  * step_mode 1: the learned proposal plain step * exp(network(features))
+//    (the BF16 network of the model buffer, evaluated in float in the
+//    device's order of operations); a proposal whose feedback or corrector
+//    fails is redone with the plain step;
 //  * predictor feedback: halve the step until the mixed residual of the
 //    Pade prediction is below alpha (fail below minsize);
 //  * corrector: at most corsteps LU Newton steps at the new t (LU_Newton_Steps,
@@ -40,6 +54,8 @@
 #include <atomic>
 #include <cmath>
 #include <algorithm>
+#include <cstring>
+#include <utility>
 #include "oracle_core.hpp"
 
 using namespace orc;
@@ -61,8 +77,9 @@ struct TrackSys {
 };
 
 struct TrackPar {
-  int deg, numdeg, dendeg, nit, corsteps, maxsteps, refine_steps;
-  double pbeta, alpha, maxsize, minsize, tolres, epsilon, restol;
+  int deg, numdeg, dendeg, nit, corsteps, maxsteps, refine_steps, step_mode;
+  double pbeta, alpha, maxsize, minsize, tolres, epsilon, restol, learn_scale, cbeta;
+  const unsigned char *model;  // the learned step's model buffer (step_mode 1)
 };
 
 template <class R> static cx<R> cplx(double re, double im) { return cx<R>(R(re), R(im)); }
@@ -419,9 +436,132 @@ template <class T> static double maxres(const TrackSys &S, int s, double t, cons
 
 
 struct PathOut {
-  int status, nsteps, nreject;
+  int status, nsteps, nreject, nbpole, nbhess, nbmaxm;
   double t, residual;
 };
+
+// ------------------------------------------------------ curvature step
+// Extreme singular values (smallest, largest) of the n x n complex matrix A
+// (row-major, real and imaginary parts) by one-sided Jacobi rotations of
+// its columns (Hestenes) until every pair is orthogonal to 1e-15 relative.
+static std::pair<double, double> singular_extremes(int n, std::vector<cx<double> > A) {
+  for (int sweep = 0; sweep < 80; ++sweep) {
+    bool rotated = false;
+    for (int p = 0; p + 1 < n; ++p)
+      for (int q = p + 1; q < n; ++q) {
+        double al = 0.0, be = 0.0, gr = 0.0, gi = 0.0;
+        for (int r = 0; r < n; ++r) {
+          const cx<double> &ap = A[(long)r * n + p], &aq = A[(long)r * n + q];
+          al += ap.re * ap.re + ap.im * ap.im;
+          be += aq.re * aq.re + aq.im * aq.im;
+          gr += ap.re * aq.re + ap.im * aq.im;
+          gi += ap.re * aq.im - ap.im * aq.re;
+        }
+        const double g = std::hypot(gr, gi);
+        if (!(g > 1e-15 * std::sqrt(al) * std::sqrt(be))) continue;
+        rotated = true;
+        const double zeta = (be - al) / (2.0 * g);
+        const double tt = (zeta < 0.0 ? -1.0 : 1.0) / (std::fabs(zeta) + std::sqrt(1.0 + zeta * zeta));
+        const double c = 1.0 / std::sqrt(1.0 + tt * tt), sn = c * tt;
+        const double pr = gr / g, pi = gi / g;
+        for (int r = 0; r < n; ++r) {
+          const cx<double> ap = A[(long)r * n + p], aq = A[(long)r * n + q];
+          const cx<double> aqt(pr * aq.re + pi * aq.im, pr * aq.im - pi * aq.re);
+          A[(long)r * n + p] = cx<double>(c * ap.re - sn * aqt.re, c * ap.im - sn * aqt.im);
+          A[(long)r * n + q] = cx<double>(sn * ap.re + c * aqt.re, sn * ap.im + c * aqt.im);
+        }
+      }
+    if (!rotated) break;
+  }
+  double smin = INFINITY, smax = 0.0;
+  for (int j = 0; j < n; ++j) {
+    double s2 = 0.0;
+    for (int r = 0; r < n; ++r) s2 += A[(long)r * n + j].re * A[(long)r * n + j].re + A[(long)r * n + j].im * A[(long)r * n + j].im;
+    smin = std::min(smin, std::sqrt(s2));
+    smax = std::max(smax, std::sqrt(s2));
+  }
+  return std::make_pair(smin, smax);
+}
+
+// ------------------------------------------------------ learned step
+// Features of a predictor step and the network's forward pass, in the
+// operations and order of the device (phcpack_b200/csrc/mlp.cuh:
+// track_features, mlp_forward_cta).
+static void step_features(int n, int K, double t, double plain_step, const std::vector<double> &mag, float *f) {
+  const double tiny = 1e-300;
+  for (int q = 0; q < 8; ++q) {
+    const int k = (q + 1 <= K) ? q + 1 : K;
+    double mx = 0.0, rmin = 1e300;
+    for (int i = 0; i < n; ++i) {
+      const double a = mag[(long)i * (K + 1) + k], b = mag[(long)i * (K + 1) + k - 1];
+      mx = std::fmax(mx, a);
+      if (a > 0.0) rmin = std::fmin(rmin, b / a);
+    }
+    const double rt = (mx > 0.0) ? -std::log(mx + tiny) / k : 30.0;
+    const double rr = (rmin < 1e299) ? std::log(rmin + tiny) : 30.0;
+    f[q] = (float)std::fmin(std::fmax(rt, -30.0), 30.0);
+    f[8 + q] = (float)std::fmin(std::fmax(rr, -30.0), 30.0);
+  }
+  for (int q = 0; q < 4; ++q) {
+    const int k = q <= K ? q : K;
+    double mx = 0.0;
+    for (int i = 0; i < n; ++i) mx = std::fmax(mx, mag[(long)i * (K + 1) + k]);
+    f[20 + q] = (float)std::fmin(std::fmax(std::log(mx + tiny), -60.0), 60.0);
+  }
+  f[16] = (float)std::log(plain_step + tiny);
+  f[17] = (float)t;
+  f[18] = (float)std::log(std::fmax(1.0 - t, 1e-16));
+  f[19] = (float)std::log((double)n);
+}
+
+static float bf16_to_float(unsigned short h) {
+  const unsigned int u = (unsigned int)h << 16;
+  float f;
+  std::memcpy(&f, &u, 4);
+  return f;
+}
+
+// The network 24 -> 128 -> 128 -> 1 of a model buffer (float mean[24],
+// inv_std[24], b1[128], b2[128], b3[4], pad[4], then BF16 W1[128][24],
+// W2[128][128], W3[128]); the output clipped to [-3, 3].
+static float mlp_forward(const unsigned char *model, const float *feat) {
+  const float *fl = reinterpret_cast<const float *>(model);
+  const float *mean = fl, *inv_std = fl + 24, *b1 = fl + 48, *b2 = fl + 176, *b3 = fl + 304;
+  const unsigned short *h = reinterpret_cast<const unsigned short *>(fl + 312);
+  const unsigned short *W1 = h, *W2 = h + 128 * 24, *W3 = h + 128 * 24 + 128 * 128;
+  float h1[128], c[128];
+  for (int j = 0; j < 128; ++j) {
+    float a = b1[j];
+    for (int i = 0; i < 24; ++i) a = std::fmaf(bf16_to_float(W1[j * 24 + i]), (feat[i] - mean[i]) * inv_std[i], a);
+    h1[j] = std::fmax(a, 0.0f);
+  }
+  for (int j = 0; j < 128; ++j) {
+    float a = b2[j];
+    for (int i = 0; i < 128; ++i) a = std::fmaf(bf16_to_float(W2[j * 128 + i]), h1[i], a);
+    c[j] = bf16_to_float(W3[j]) * std::fmax(a, 0.0f);
+  }
+  float red[4];
+  for (int w = 0; w < 4; ++w) {  // the butterfly of __shfl_xor_sync within each warp
+    float v[32];
+    for (int l = 0; l < 32; ++l) v[l] = c[32 * w + l];
+    for (int o = 16; o > 0; o >>= 1) {
+      float u[32];
+      for (int l = 0; l < 32; ++l) u[l] = v[l] + v[l ^ o];
+      for (int l = 0; l < 32; ++l) v[l] = u[l];
+    }
+    red[w] = v[0];
+  }
+  const float out = b3[0] + red[0] + red[1] + red[2] + red[3];
+  return std::fmin(std::fmax(out, -3.0f), 3.0f);
+}
+
+// The pieces of the step size that need the point's Hessians, Jacobian and
+// Pade error estimates (defined after the end-game helpers below).
+template <class T>
+static double curvature_step(const TrackSys &S, int s, const TrackPar &P, double t,
+                             const std::vector<std::vector<T> > &xs, const std::vector<std::vector<T> > &num,
+                             const std::vector<std::vector<T> > &den, const std::vector<int> &pdeg,
+                             const std::vector<int> &qdeg);
 
 // Track one path.  PT: predictor numbers, CT: corrector numbers, RT:
 // refinement numbers.
@@ -429,7 +569,7 @@ template <class PT, class CT, class RT>
 static PathOut track_path(const TrackSys &S, int s, const TrackPar &P, const double *x0, double *xend) {
   const int n = S.dim[s];
   const int K = P.deg;
-  PathOut o{0, 0, 0, 0.0, 0.0};
+  PathOut o{0, 0, 0, 0, 0, 0, 0.0, 0.0};
   std::vector<CT> x(n);
   for (int i = 0; i < n; ++i) convert(cx<double>(x0[2 * i], x0[2 * i + 1]), x[i]);
   double t = 0.0, dxn;
@@ -438,8 +578,9 @@ static PathOut track_path(const TrackSys &S, int s, const TrackPar &P, const dou
   std::vector<std::vector<PT> > num(n), den(n);
   std::vector<CT> xc(n);
   std::vector<PT> xp(n);
-  std::vector<double> ax(n), rabs;
+  std::vector<double> ax(n), rabs, mag((size_t)n * (K + 1));
   std::vector<int> pdeg(n), qdeg(n);
+  const bool use_model = P.step_mode == 1 && P.model != nullptr;
   bool failed = false;
   int k;
   for (k = 0; k < P.maxsteps; ++k) {
@@ -460,44 +601,89 @@ static PathOut track_path(const TrackSys &S, int s, const TrackPar &P, const dou
         if (ri < r) r = ri;
         rfail = false;
       }
+      for (int q = 0; q <= K; ++q) mag[(size_t)i * (K + 1) + q] = cabs(xs[i][q]);
     }
-    double step = rfail ? P.maxsize : P.pbeta * r;
-    if (step > P.maxsize) step = P.maxsize;
-    if (t + step > 1.0) step = 1.0 - t;
-    // predictor feedback on the mixed residual
+    const double pole_step = rfail ? P.maxsize : P.pbeta * r;
+    const double curv_step = curvature_step(S, s, P, t, xs, num, den, pdeg, qdeg);
+    double plain_step;
+    if (pole_step < curv_step) {
+      if (pole_step < P.maxsize) { plain_step = pole_step; ++o.nbpole; }
+      else { plain_step = P.maxsize; ++o.nbmaxm; }
+    } else {
+      if (curv_step < P.maxsize) { plain_step = curv_step; ++o.nbhess; }
+      else { plain_step = P.maxsize; ++o.nbmaxm; }
+    }
+    if (std::isnan(plain_step)) plain_step = 0.0;
+    double step = plain_step;
+    bool learned = false;
+    if (use_model) {
+      float feat[24];
+      step_features(n, K, t, plain_step, mag, feat);
+      const float lr = mlp_forward(P.model, feat);
+      const double prop = plain_step * std::exp((double)lr) * P.learn_scale;
+      if (prop > P.minsize && prop == prop) {
+        step = std::fmin(prop, P.maxsize);
+        learned = true;
+      }
+    }
     auto predict = [&](double st) {
       const PT z = PT(typename real_of<PT>::type(st));
       for (int i = 0; i < n; ++i) xp[i] = horner(num[i], pdeg[i], z) / horner(den[i], qdeg[i], z);
     };
-    double mixres;
-    for (;;) {
-      predict(step);
-      std::vector<std::vector<PT> > xs0(n, std::vector<PT>(1)), hv;
-      for (int i = 0; i < n; ++i) {
-        xs0[i][0] = xp[i];
-        ax[i] = cabs(xp[i]);
+    bool accepted = false;
+    for (int attempt = 0; attempt < 2 && !accepted; ++attempt) {
+      if (attempt == 1) {  // the learned proposal was rejected: the plain step
+        if (!learned) break;
+        learned = false;
+        step = plain_step;
       }
-      hom_eval<PT>(S, s, 0, t + step, xs0, hv, nullptr);
-      hom_abs_eval<PT>(S, s, t + step, ax, rabs);
-      mixres = 0.0;
-      for (int i = 0; i < n; ++i) mixres += cabs(hv[i][0]) / (rabs[i] + 1.0);
-      mixres /= n;
-      if (mixres < P.alpha) break;
-      step *= 0.5;
-      ++o.nreject;
-      if (step < P.minsize) break;
+      if (t + step >= 1.0 - P.minsize) step = 1.0 - t;  // Bounded_Update
+      if (!(step > 0.0)) {
+        if (learned) continue;
+        failed = true;
+        break;
+      }
+      // predictor feedback on the mixed residual
+      bool ok = false;
+      for (int h = 0; h < 64; ++h) {
+        predict(step);
+        std::vector<std::vector<PT> > xs0(n, std::vector<PT>(1)), hv;
+        for (int i = 0; i < n; ++i) {
+          xs0[i][0] = xp[i];
+          ax[i] = cabs(xp[i]);
+        }
+        hom_eval<PT>(S, s, 0, t + step, xs0, hv, nullptr);
+        hom_abs_eval<PT>(S, s, t + step, ax, rabs);
+        double mixres = 0.0;
+        for (int i = 0; i < n; ++i) mixres += cabs(hv[i][0]) / (rabs[i] + 1.0);
+        mixres /= n;
+        if (mixres < P.alpha) { ok = true; break; }
+        step *= 0.5;
+        ++o.nreject;
+        if (step < P.minsize) break;
+      }
+      if (!ok) {
+        if (learned) continue;
+        failed = true;
+        break;
+      }
+      // corrector with step halving
+      bool cok = false;
+      for (int h = 0; h < 64; ++h) {
+        for (int i = 0; i < n; ++i) convert(xp[i], xc[i]);
+        if (point_newton<CT, PT>(S, s, t + step, xc, P.corsteps, P.tolres, 1, &dxn)) { cok = true; break; }
+        ++o.nreject;
+        if (learned) break;
+        step *= 0.5;
+        if (step < P.minsize) break;
+        predict(step);
+      }
+      if (cok) { accepted = true; break; }
+      if (learned) continue;
+      failed = true;
+      break;
     }
-    if (step < P.minsize) { failed = true; break; }
-    // corrector with step halving
-    for (;;) {
-      for (int i = 0; i < n; ++i) convert(xp[i], xc[i]);
-      if (point_newton<CT, PT>(S, s, t + step, xc, P.corsteps, P.tolres, 1, &dxn)) break;
-      step *= 0.5;
-      ++o.nreject;
-      if (step < P.minsize) break;
-      predict(step);
-    }
-    if (step < P.minsize) { failed = true; break; }
+    if (failed || !accepted) { failed = true; break; }
     x = xc;
     t += step;
     if (std::fabs(1.0 - t) < P.epsilon) { ++k; break; }
@@ -626,6 +812,39 @@ static void jacobian_hessians(const TrackSys &S, int s, double t, const std::vec
   }
 }
 
+// The curvature step at the predictor's point (Hesse_Pade): the Jacobian
+// and the Hessians of the equations at (x_0, t) in complex double, eta =
+// 2 sigma_min(J) / |(sigma_max(H_1), ..., sigma_max(H_n))|_2, and
+// (cbeta eta / |Pade error estimates|_2)^(1/K).
+template <class T>
+static double curvature_step(const TrackSys &S, int s, const TrackPar &P, double t,
+                             const std::vector<std::vector<T> > &xs, const std::vector<std::vector<T> > &num,
+                             const std::vector<std::vector<T> > &den, const std::vector<int> &pdeg,
+                             const std::vector<int> &qdeg) {
+  const int n = S.dim[s];
+  const int K = P.deg;
+  std::vector<cx<double> > xd(n);
+  for (int i = 0; i < n; ++i) xd[i] = cx<double>(lead_of(xs[i][0].re), lead_of(xs[i][0].im));
+  std::vector<double> J(2L * n * n), H(2L * n * n * n);
+  jacobian_hessians(S, s, t, xd, n, J.data(), H.data());
+  std::vector<cx<double> > A((size_t)n * n);
+  for (long q = 0; q < (long)n * n; ++q) A[q] = cx<double>(J[2 * q], J[2 * q + 1]);
+  const double smin = singular_extremes(n, A).first;
+  double hsum = 0.0;
+  for (int i = 0; i < n; ++i) {
+    for (long q = 0; q < (long)n * n; ++q) A[q] = cx<double>(H[2 * ((long)i * n * n + q)], H[2 * ((long)i * n * n + q) + 1]);
+    const double sm = singular_extremes(n, A).second;
+    hsum += sm * sm;
+  }
+  const double eta = hsum > 0.0 ? 2.0 * smin / std::sqrt(hsum) : INFINITY;
+  double perr = 0.0;
+  for (int i = 0; i < n; ++i) {
+    const double pe = pade_error(xs[i], K, num[i], pdeg[i], den[i], qdeg[i]);
+    perr += pe * pe;
+  }
+  return std::pow(P.cbeta * eta / std::sqrt(perr), 1.0 / K);
+}
+
 struct DiagOut {
   int fail, status;
   double zre, zim, radius, err, padenorm, lastdx;
@@ -716,23 +935,28 @@ extern "C" {
 
 // Track npaths paths with nthreads host threads.  pmode: predictor
 // precision (1 double, 2 double-double); rmode: refinement precision
-// (2 dd, 4 qd, 8 od); the corrector is double-double.  x0: start points,
-// maxdim complex doubles per path; xend: maxdim complex quad-doubles per
-// path (octo-doubles for rmode 8; lower limbs zero below the refinement
-// precision); info: per path
-// status, nsteps, nreject; dinfo: per path t, residual.
+// (2 dd, 4 qd, 8 od); the corrector is double-double; step_mode 1 with a
+// model buffer: the learned step.  ipar and dpar as in phc_track (dpar[8]
+// = cbeta).  x0: start points, maxdim complex doubles per path; xend:
+// maxdim complex quad-doubles per path (octo-doubles for rmode 8; lower
+// limbs zero below the refinement precision); info: per path status,
+// nsteps, nreject, nbpole, nbhess, nbmaxm; dinfo: per path t, residual.
 int orc_track(int nsys, const int *dim, int maxvar, const int *mono_off, const int *mono_nvr, const int *mono_idx,
               const int *mono_exp, const int *eq_off, const int *term_off, const int *term_mono,
               const double *term_a, const double *term_b, int npaths, const int *path_sys, int maxdim,
-              const double *x0, const int *ipar, const double *dpar, int pmode, int rmode, int nthreads,
-              double *xend, int *info, double *dinfo) {
+              const double *x0, const int *ipar, const double *dpar, int pmode, int rmode, int step_mode,
+              const void *model, int nthreads, double *xend, int *info, double *dinfo) {
   TrackSys S{nsys, maxvar, dim, mono_off, mono_nvr, mono_idx, mono_exp, eq_off, term_off, term_mono, term_a, term_b};
   TrackPar P;
   P.deg = ipar[0]; P.numdeg = ipar[1]; P.dendeg = ipar[2]; P.nit = ipar[3];
   P.corsteps = ipar[4]; P.maxsteps = ipar[5]; P.refine_steps = ipar[6];
   P.pbeta = dpar[0]; P.alpha = dpar[1]; P.maxsize = dpar[2]; P.minsize = dpar[3];
   P.tolres = dpar[4]; P.epsilon = dpar[5]; P.restol = dpar[6];
-  if (P.numdeg + P.dendeg != P.deg || P.deg < 3) return -1;
+  P.learn_scale = dpar[7] > 0.0 ? dpar[7] : 1.0;
+  P.cbeta = dpar[8];
+  P.step_mode = step_mode;
+  P.model = step_mode == 1 ? static_cast<const unsigned char *>(model) : nullptr;
+  if (P.numdeg + P.dendeg != P.deg || P.deg < 3 || !(P.cbeta > 0.0)) return -1;
   if ((pmode != 1 && pmode != 2) || (rmode != 2 && rmode != 4 && rmode != 8)) return -1;
   std::atomic<int> next(0);
   auto work = [&]() {
@@ -749,9 +973,13 @@ int orc_track(int nsys, const int *dim, int maxvar, const int *mono_off, const i
       else if (rmode == 2) o = track_path<cx<dd>, cx<dd>, cx<dd> >(S, s, P, xs, xe);
       else if (rmode == 4) o = track_path<cx<dd>, cx<dd>, cx<qd> >(S, s, P, xs, xe);
       else o = track_path<cx<dd>, cx<dd>, cx<od> >(S, s, P, xs, xe);
-      info[3 * p] = o.status;
-      info[3 * p + 1] = o.nsteps;
-      info[3 * p + 2] = o.nreject;
+      int *io = info + 6L * p;
+      io[0] = o.status;
+      io[1] = o.nsteps;
+      io[2] = o.nreject;
+      io[3] = o.nbpole;
+      io[4] = o.nbhess;
+      io[5] = o.nbmaxm;
       dinfo[2 * p] = o.t;
       dinfo[2 * p + 1] = o.residual;
     }

@@ -42,7 +42,10 @@ static double *g_bals_scratch_ptr[kMaxDevices] = {nullptr};
 static std::mutex g_bals_scratch_lock;
 
 // Device address of this device's array (host code must not use the
-// symbol itself: on the host it names a stand-in, not device memory).
+// symbol itself: on the host it names a stand-in, not device memory).  The
+// address is looked up once per device and kept for the life of the
+// process, so the library must not be used across a reset of the device
+// (cudaDeviceReset or a new primary context), which would leave it stale.
 static int bals_scratch_address(double **out) {
   int dev = 0;
   PHC_CUDA(cudaGetDevice(&dev));

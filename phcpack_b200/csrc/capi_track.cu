@@ -54,6 +54,7 @@ static TrackParDev make_par(const int *ipar, const double *dpar, int step_mode) 
   P.epsilon = dpar[5];
   P.restol = dpar[6];
   P.learn_scale = dpar[7] > 0.0 ? dpar[7] : 1.0;
+  P.cbeta = dpar[8];
   return P;
 }
 
@@ -185,7 +186,7 @@ int phc_track_host(int nsys, const int *dim, int maxvar, const int *mono_off, co
   const size_t o_xend = total;
   total += (xbytes + 255) & ~size_t(255);
   const size_t o_info = total;
-  total += (((size_t)npaths * 12) + 255) & ~size_t(255);
+  total += (((size_t)npaths * 4 * kTrackInfo) + 255) & ~size_t(255);
   const size_t o_dinfo = total;
   total += (((size_t)npaths * 16) + 255) & ~size_t(255);
   const size_t o_q = total;
@@ -193,8 +194,12 @@ int phc_track_host(int nsys, const int *dim, int maxvar, const int *mono_off, co
   const size_t in_bytes = o_xend, out_bytes = o_q - o_xend;
   int devid = 0;
   PHC_CUDA(cudaGetDevice(&devid));
+  if (devid < 0 || devid >= 64) {
+    set_error("track_host: device %d beyond the 64 whose buffers are kept", devid);
+    return PHC_ERR_LIMIT;
+  }
   std::lock_guard<std::mutex> lock(g_track_mu);
-  HostCallBuffers &hb = g_track_buf[devid & 63];
+  HostCallBuffers &hb = g_track_buf[devid];
   if (hb.dev_cap < total) {
     if (hb.dev) cudaFree(hb.dev);
     hb.dev = nullptr;
@@ -234,13 +239,13 @@ int phc_track_host(int nsys, const int *dim, int maxvar, const int *mono_off, co
       out = PHC_ERR_CUDA;
     } else {
       std::memcpy(xend, h, xbytes);
-      std::memcpy(info, h + (o_info - o_xend), (size_t)npaths * 12);
+      std::memcpy(info, h + (o_info - o_xend), (size_t)npaths * 4 * kTrackInfo);
       std::memcpy(dinfo, h + (o_dinfo - o_xend), (size_t)npaths * 16);
     }
   }
   if (out < 0) return out;
   int fails = 0;
-  for (int p = 0; p < npaths; ++p) fails += info[3 * p] != 0;
+  for (int p = 0; p < npaths; ++p) fails += info[(long)kTrackInfo * p] != 0;
   return fails;
 }
 

@@ -68,129 +68,10 @@ __device__ void fabry_one(const double *c, int K, int off, typename N::T &z, dou
   }
 }
 
-// |error estimate| of one component's Pade approximant (numerator degree
-// pdeg, denominator degree qdeg): at the last index top <= min(pdeg + qdeg
-// + 2, K) with |c_top| > 1e-5, the coefficient of the series times the
-// denominator, subtracted from the numerator's when top <= pdeg; 1 when no
-// coefficient passes the threshold or the estimate is below 1e-5.
-template <class N>
-__device__ double pade_error_one(const double *c, int K, const double *num, int pdeg, const double *den, int qdeg) {
-  typedef typename N::T T;
-  const int endidx = min(pdeg + qdeg + 2, K);
-  int top = -1;
-  for (int i = endidx; i >= 0; --i)
-    if (N::mag(ldn_at<N>(c, i)) > 1e-5) {
-      top = i;
-      break;
-    }
-  T res = N::one();
-  if (top >= 0) {
-    res = ldn_at<N>(c, top);
-    for (int i = 1; i <= qdeg && i <= top; ++i) res = N::add(res, N::mul(ldn_at<N>(den, i), ldn_at<N>(c, top - i)));
-    if (top <= pdeg) res = N::sub(ldn_at<N>(num, top), res);
-  }
-  const double a = N::mag(res);
-  return a < 1e-5 ? 1.0 : a;
-}
-
-__device__ __forceinline__ double2 cmul_d(double2 a, double2 b) {
-  return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
-}
-
-// Hessian of equation i of system s at (x, t) in complex double, column-
-// major n x n in H; x: n complex doubles.  One warp: the terms in order,
-// lanes over the ordered pairs of the monomial's variables (distinct
-// variables, so distinct cells within a term).
-__device__ void warp_hessian(const TrackDev &S, int s, int i, int n, double t, const double2 *x, double2 *H) {
-  const int lane = threadIdx.x & 31;
-  for (int q = lane; q < n * n; q += 32) H[q] = make_double2(0.0, 0.0);
-  __syncwarp();
-  const int eq = S.eq_off[s] + i;
-  for (int tr = S.term_off[eq]; tr < S.term_off[eq + 1]; ++tr) {
-    const int gm = S.term_mono[tr];
-    const int nv = S.mono_nvr[gm];
-    const int *ix = S.mono_idx + (long)gm * S.maxvar;
-    const int *ex = S.mono_exp + (long)gm * S.maxvar;
-    // the coefficient (1 - t) a + t b
-    const double2 c = make_double2(fma(S.term_b[2 * tr] - S.term_a[2 * tr], t, S.term_a[2 * tr]),
-                                   fma(S.term_b[2 * tr + 1] - S.term_a[2 * tr + 1], t, S.term_a[2 * tr + 1]));
-    for (int q = lane; q < nv * nv; q += 32) {
-      const int u = q / nv, v = q % nv;
-      const double mult = u == v ? (double)ex[u] * (ex[u] - 1) : (double)ex[u] * ex[v];
-      if (mult == 0.0) continue;
-      double2 acc = make_double2(c.x * mult, c.y * mult);
-      for (int w = 0; w < nv; ++w) {
-        const double2 xw = x[ix[w]];
-        for (int e = ex[w] - (w == u) - (w == v); e > 0; --e) acc = cmul_d(acc, xw);
-      }
-      double2 &h = H[(long)ix[v] * n + ix[u]];
-      h = make_double2(h.x + acc.x, h.y + acc.y);
-    }
-    __syncwarp();
-  }
-}
-
-// Smallest (x) and largest (y) singular value of the n x n complex matrix
-// A (column-major, shared memory, overwritten) by one-sided Jacobi
-// rotations of its columns (Hestenes): a column pair (p, q) with
-// g = a_p^H a_q is rotated when |g| > 1e-15 |a_p| |a_q|; at most 40 sweeps;
-// the singular values are the final column norms.  One warp, lane r holding
-// row r; the butterfly sums give every lane the same value, so the
-// decisions are uniform over the warp.
-__device__ double2 warp_singular_values(int n, double2 *A) {
-  const int lane = threadIdx.x & 31;
-  const double2 z0 = make_double2(0.0, 0.0);
-  for (int sweep = 0; sweep < 40; ++sweep) {
-    bool rotated = false;
-    for (int p = 0; p + 1 < n; ++p)
-      for (int q = p + 1; q < n; ++q) {
-        const double2 ap = lane < n ? A[(long)p * n + lane] : z0;
-        const double2 aq = lane < n ? A[(long)q * n + lane] : z0;
-        double al = ap.x * ap.x + ap.y * ap.y, be = aq.x * aq.x + aq.y * aq.y;
-        double gr = ap.x * aq.x + ap.y * aq.y, gi = ap.x * aq.y - ap.y * aq.x;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-          al += __shfl_xor_sync(0xffffffffu, al, o);
-          be += __shfl_xor_sync(0xffffffffu, be, o);
-          gr += __shfl_xor_sync(0xffffffffu, gr, o);
-          gi += __shfl_xor_sync(0xffffffffu, gi, o);
-        }
-        const double g = hypot(gr, gi);
-        if (!(g > 1e-15 * sqrt(al) * sqrt(be))) continue;
-        rotated = true;
-        // the real symmetric 2 x 2 Gram matrix [al g; g be] of (a_p, a_q
-        // times the conjugate phase of g) diagonalised by [c s; -s c]
-        const double zeta = (be - al) / (2.0 * g);
-        const double az = fabs(zeta);
-        const double tt = (az > 1e150 ? 0.5 / az : 1.0 / (az + sqrt(1.0 + az * az))) * (zeta < 0.0 ? -1.0 : 1.0);
-        const double c = 1.0 / sqrt(1.0 + tt * tt), sn = c * tt;
-        const double pr = gr / g, pi = gi / g;
-        const double2 aqt = make_double2(pr * aq.x + pi * aq.y, pr * aq.y - pi * aq.x);
-        if (lane < n) {
-          A[(long)p * n + lane] = make_double2(c * ap.x - sn * aqt.x, c * ap.y - sn * aqt.y);
-          A[(long)q * n + lane] = make_double2(sn * ap.x + c * aqt.x, sn * ap.y + c * aqt.y);
-        }
-      }
-    if (!rotated) break;
-  }
-  double smin = INFINITY, smax = 0.0;
-  for (int j = 0; j < n; ++j) {
-    const double2 a = lane < n ? A[(long)j * n + lane] : z0;
-    double s2 = a.x * a.x + a.y * a.y;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) s2 += __shfl_xor_sync(0xffffffffu, s2, o);
-    const double sv = sqrt(s2);
-    smin = fmin(smin, sv);
-    smax = fmax(smax, sv);
-  }
-  return make_double2(smin, smax);
-}
-
-__host__ __device__ inline long diag_svd_offset(const TrackLayout &L) { return (L.total + 1) & ~1L; }
-
 // One CTA per point: Newton at (x, t), the Taylor series to degree K, Fabry
-// over the components, the Pade error estimates, and the singular values of
-// the Jacobian and of the n Hessians (a job per warp).
+// over the components, the Pade error estimates, and the extreme singular
+// values of the Jacobian and of the n Hessians (a job per warp, the warp
+// routines of the tracker's curvature step).
 template <class PN>
 __global__ void __launch_bounds__(kTrackThreads, 1)
     k_series_diag(TrackDev S, DiagParDev D, int npaths, const int *__restrict__ path_sys,
@@ -205,8 +86,8 @@ __global__ void __launch_bounds__(kTrackThreads, 1)
   int nm_max = 0;
   for (int s = 0; s < S.nsys; ++s) nm_max = max(nm_max, S.mono_off[s + 1] - S.mono_off[s]);
   const TrackLayout L = track_layout(n_max, K, D.dendeg, nm_max, S.maxvar, Wp, Wp, S.gstaged);
-  double2 *svd = reinterpret_cast<double2 *>(sm + diag_svd_offset(L));  // 5 matrices of n_max^2
-  double *sv = sm + diag_svd_offset(L) + 10L * n_max * n_max;          // n_max + 1 singular values
+  double2 *svd = reinterpret_cast<double2 *>(sm + L.svd);  // kSvdSlots matrices of n_max^2
+  double *sv = sm + L.sv;                                   // n_max + 1 singular values
   double *red = sm + L.red;
   int *piv = reinterpret_cast<int *>(sm + L.piv);
   double *dinv = sm + L.dinv;
@@ -236,17 +117,17 @@ __global__ void __launch_bounds__(kTrackThreads, 1)
     const int i = q / (K + 1), k = q % (K + 1);
     stn_at<PN>(xs, q, k == 0 ? ldn_at<PN>(xc, i) : PN::zero());
   }
-  double2 *xd = reinterpret_cast<double2 *>(sm + L.xp);
+  double2 *xd = reinterpret_cast<double2 *>(sm + L.xd);
   for (int i = ctid(); i < n; i += blockDim.x) {
     const T v = ldn_at<PN>(xc, i);
     xd[i] = make_double2(md::lead(v.re), md::lead(v.im));
   }
   __syncthreads();
   hom_eval_cta<PN>(S, s, 0, t, xs, K + 1, sm + L.V, sm + L.G, sm + L.hs, sm + L.J0);
-  double2 *Jd = svd + 4L * n_max * n_max;
+  double2 *Jd = svd + (long)(kSvdSlots - 1) * n * n;
   for (int q = ctid(); q < n * n; q += blockDim.x) {
     const T v = ldn_at<PN>(sm + L.J0, q);
-    Jd[(long)(q % n) * n + q / n] = make_double2(md::lead(v.re), md::lead(v.im));
+    Jd[q] = make_double2(md::lead(v.re), md::lead(v.im));
   }
   __syncthreads();
   if (ctid() < 32) {
@@ -295,9 +176,9 @@ __global__ void __launch_bounds__(kTrackThreads, 1)
   // singular values: job j < n the Hessian of equation j (largest), job n
   // the Jacobian (smallest)
   for (int j = warp; j <= n; j += kTrackThreads / 32) {
-    double2 *A = j < n ? svd + (long)warp * n_max * n_max : Jd;
-    if (j < n) warp_hessian(S, s, j, n, t, xd, A);
-    const double2 mm = warp_singular_values(n, A);
+    double2 *A = j < n ? svd + (long)warp * n * n : Jd;
+    if (j < n) warp_hessian_rows(S, s, j, n, t, xd, A);
+    const double2 mm = warp_singular_extremes(n, A, j < n ? 2 : 1);
     if (lane == 0) sv[j] = j < n ? mm.y : mm.x;
   }
   __syncthreads();
@@ -354,7 +235,7 @@ namespace phc {
 long diag_smem_bytes(int maxdim, int K, int M, int nmono_max, int maxvar, int pmode, int gst) {
   const int W = 2 * pmode;
   const TrackLayout L = track_layout(maxdim, K, M, nmono_max, maxvar, W, W, gst);
-  return (diag_svd_offset(L) + 10L * maxdim * maxdim + maxdim + 2) * (long)sizeof(double);
+  return L.total * (long)sizeof(double);
 }
 
 // The checks of the precision, the dimension, the degrees and the limbs of

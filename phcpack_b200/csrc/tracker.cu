@@ -22,6 +22,7 @@ int track_check(const TrackParDev &P, int pmode, int rmode, int maxdim) {
   PHC_REQUIRE(maxdim >= 1 && maxdim <= 32, "track: dimension %d not in [1,32]", maxdim);
   PHC_REQUIRE(P.deg >= 3 && P.deg <= kTrackKmax && P.numdeg + P.dendeg == P.deg && P.dendeg <= 8 && P.nit >= 1,
               "track: need 3 <= deg = numdeg + dendeg <= %d, dendeg <= 8", kTrackKmax);
+  PHC_REQUIRE(P.cbeta > 0.0 && P.cbeta < INFINITY, "track: cbeta %g is not positive", P.cbeta);
   return PHC_OK;
 }
 

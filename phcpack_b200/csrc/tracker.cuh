@@ -87,8 +87,13 @@ __host__ __device__ inline bool simple_monomial(int k, const int *ex) {
 // Tracking parameters (include/phc_b200.h, phc_track: ipar and dpar)
 struct TrackParDev {
   int deg, numdeg, dendeg, nit, corsteps, maxsteps, refine_steps, step_mode;
-  double pbeta, alpha, maxsize, minsize, tolres, epsilon, restol, learn_scale;
+  double pbeta, alpha, maxsize, minsize, tolres, epsilon, restol, learn_scale, cbeta;
 };
+
+// Words per path of the tracker's info output: status, steps, rejected
+// steps, and the times the step was the pole step, the curvature step and
+// maxsize (nbpole, nbhess, nbmaxm of the reference's Minimum).
+static const int kTrackInfo = 6;
 
 // Parameters of the end-game diagnostics (include/phc_b200.h,
 // phc_series_diagnostics: ipar and dpar)
@@ -533,6 +538,257 @@ __device__ TRACK_FN void warp_luinverse(int n, const double *A, const int *ipvt,
   }
 }
 
+// ------------------------------------------------------------ singular values
+// The curvature step of the predictor needs the smallest singular value of
+// the Jacobian and the largest of each Hessian at the current point
+// (Hesse_Pade, Curves/dobldobl_predictor_convolutions.adb:383-406; the
+// reference computes full SVDs with LINPACK's zsvdc, Math_Lib/Matrices/
+// dobldobl_complex_singular_values.adb).  Here one warp finds the two
+// extreme singular values of an n x n complex matrix: Householder
+// bidiagonalization (Golub and Kahan), then bisection with Sturm counts on
+// the 2n x 2n zero-diagonal tridiagonal form of the real bidiagonal (its
+// eigenvalues are +-sigma_i), 33-way per round (one trial point per lane).
+
+__device__ __forceinline__ double2 cx_conj_mul(double2 a, double2 b) {  // conj(a) b
+  return make_double2(fma(a.x, b.x, a.y * b.y), fma(a.x, b.y, -a.y * b.x));
+}
+__device__ __forceinline__ double2 cx_mul(double2 a, double2 b) {
+  return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
+}
+__device__ __forceinline__ double warp_sum_d(double a) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+  return a;
+}
+
+// Number of eigenvalues below x of the 2n x 2n symmetric tridiagonal with
+// zero diagonal and off-diagonals c_0 = d_0, c_1 = e_0, c_2 = d_1, ...,
+// c_{2n-2} = d_{n-1} (d held by lane k as dk, e as ek): the sign changes of
+// its leading principal minors p_m = -x p_{m-1} - c_{m-1}^2 p_{m-2} (a zero
+// minor takes the sign opposite to its predecessor), rescaled by powers of
+// two to stay in range.  Every lane passes its own x.
+static __device__ int gk_count(int n, double dk, double ek, double x) {
+  double pm2 = 1.0, pm1 = -x;
+  int cnt = pm1 < 0.0 ? 1 : 0;
+  bool neg = pm1 < 0.0 || pm1 == 0.0;  // sign of p_{m-1} (a zero counts as a change)
+  for (int m = 1; m < 2 * n; ++m) {
+    const int k = (m - 1) >> 1;
+    const double c = __shfl_sync(0xffffffffu, (m - 1) & 1 ? ek : dk, k);
+    const double p = fma(-x, pm1, -(c * c) * pm2);
+    const bool pn = (p == 0.0) ? !neg : p < 0.0;
+    cnt += (pn != neg) ? 1 : 0;
+    neg = pn;
+    pm2 = pm1;
+    pm1 = p;
+    const double s = fmax(fabs(pm1), fabs(pm2));
+    if (s > 0x1p+500) {
+      pm1 *= 0x1p-500;
+      pm2 *= 0x1p-500;
+    } else if (s < 0x1p-500 && s > 0.0) {
+      pm1 *= 0x1p+500;
+      pm2 *= 0x1p+500;
+    }
+  }
+  return cnt;
+}
+
+// The eigenvalue of the Golub-Kahan form in (lo, hi] where the count first
+// reaches target: 33-way bisection until hi - lo <= 2^-52 hi (at most 30
+// rounds); the decisions are uniform over the warp.
+static __device__ double gk_bisect(int n, double dk, double ek, double lo, double hi, int target) {
+  const int lane = threadIdx.x & 31;
+  for (int round = 0; round < 30 && hi - lo > 0x1p-52 * hi; ++round) {
+    const double x = lo + (hi - lo) * (double)(lane + 1) * (1.0 / 33.0);
+    const unsigned m = __ballot_sync(0xffffffffu, gk_count(n, dk, ek, x) >= target);
+    if (m == 0u) {
+      lo = __shfl_sync(0xffffffffu, x, 31);
+    } else {
+      const int l = __ffs(m) - 1;
+      const double xh = __shfl_sync(0xffffffffu, x, l);
+      const double xl = __shfl_sync(0xffffffffu, x, l > 0 ? l - 1 : 0);
+      if (l > 0) lo = xl;
+      hi = xh;
+    }
+  }
+  return hi;
+}
+
+// Extreme singular values (x: smallest, y: largest) of the n x n complex
+// matrix A (column-major, shared memory, n <= 32; destroyed).  want: 1 the
+// smallest, 2 the largest, 3 both (the other is returned as 0).  One warp,
+// all lanes; a matrix with a non-finite entry gives (0, inf).
+static __device__ double2 warp_singular_extremes(int n, double2 *A, int want) {
+  const int lane = threadIdx.x & 31;
+  double amax = 0.0;
+  for (int q = lane; q < n * n; q += 32) {
+    const double2 a = A[q];
+    const double m = fmax(fabs(a.x), fabs(a.y));
+    amax = (m == m) ? fmax(amax, m) : INFINITY;
+  }
+  amax = warp_max(amax);
+  if (amax == 0.0) return make_double2(0.0, 0.0);
+  if (!(amax < INFINITY)) return make_double2(0.0, INFINITY);
+  // scale by a power of two: the largest |entry| in [1, 2)
+  int ex;
+  frexp(amax, &ex);
+  const double sc = ldexp(1.0, 1 - ex);
+  for (int q = lane; q < n * n; q += 32) A[q] = make_double2(A[q].x * sc, A[q].y * sc);
+  __syncwarp();
+  double dk = 0.0, ek = 0.0;  // lane k keeps d_k and e_k of the bidiagonal
+  for (int k = 0; k < n; ++k) {
+    // left reflector on column k, rows k..n-1 (lanes over the rows)
+    const double2 x = (lane >= k && lane < n) ? A[(long)k * n + lane] : make_double2(0.0, 0.0);
+    const double s2 = warp_sum_d(lane > k && lane < n ? x.x * x.x + x.y * x.y : 0.0);
+    const double2 xk = make_double2(__shfl_sync(0xffffffffu, x.x, k), __shfl_sync(0xffffffffu, x.y, k));
+    const double ak = hypot(xk.x, xk.y);
+    const double nrm = sqrt(fma(ak, ak, s2));
+    if (lane == k) dk = nrm;
+    if (s2 > 0.0) {
+      // v = x - alpha e_k, alpha = -(x_k / |x_k|) |x|; tau = 2 / v^H v
+      const double2 ph = ak > 0.0 ? make_double2(xk.x / ak, xk.y / ak) : make_double2(1.0, 0.0);
+      const double vk = ak + nrm;
+      const double tau = 2.0 / fma(vk, vk, s2);
+      __syncwarp();
+      if (lane == k) A[(long)k * n + k] = make_double2(ph.x * vk, ph.y * vk);
+      __syncwarp();
+      for (int j = k + 1 + lane; j < n; j += 32) {  // lanes over the columns to the right
+        double2 w = make_double2(0.0, 0.0);
+        for (int r = k; r < n; ++r) {
+          const double2 p = cx_conj_mul(A[(long)k * n + r], A[(long)j * n + r]);
+          w.x += p.x;
+          w.y += p.y;
+        }
+        w = make_double2(w.x * tau, w.y * tau);
+        for (int r = k; r < n; ++r) {
+          const double2 p = cx_mul(A[(long)k * n + r], w);
+          A[(long)j * n + r] = make_double2(A[(long)j * n + r].x - p.x, A[(long)j * n + r].y - p.y);
+        }
+      }
+      __syncwarp();
+    }
+    if (k + 1 >= n) break;
+    // right reflector on row k, columns k+1..n-1 (lanes over the columns)
+    const double2 y = (lane > k && lane < n) ? A[(long)lane * n + k] : make_double2(0.0, 0.0);
+    const double t2 = warp_sum_d(lane > k + 1 && lane < n ? y.x * y.x + y.y * y.y : 0.0);
+    const double2 yk = make_double2(__shfl_sync(0xffffffffu, y.x, k + 1), __shfl_sync(0xffffffffu, y.y, k + 1));
+    const double bk = hypot(yk.x, yk.y);
+    const double nr = sqrt(fma(bk, bk, t2));
+    if (lane == k) ek = nr;
+    if (t2 > 0.0) {
+      // A <- A (I - tau conj(u) u^T) with u = y - beta e_{k+1}, beta = -(y_{k+1} / |y_{k+1}|) |y|
+      const double2 ph = bk > 0.0 ? make_double2(yk.x / bk, yk.y / bk) : make_double2(1.0, 0.0);
+      const double uk = bk + nr;
+      const double tau = 2.0 / fma(uk, uk, t2);
+      __syncwarp();
+      if (lane == k) A[(long)(k + 1) * n + k] = make_double2(ph.x * uk, ph.y * uk);
+      __syncwarp();
+      for (int r = k + 1 + lane; r < n; r += 32) {  // lanes over the rows below
+        double2 z = make_double2(0.0, 0.0);
+        for (int c = k + 1; c < n; ++c) {
+          const double2 p = cx_conj_mul(A[(long)c * n + k], A[(long)c * n + r]);
+          z.x += p.x;
+          z.y += p.y;
+        }
+        z = make_double2(z.x * tau, z.y * tau);
+        for (int c = k + 1; c < n; ++c) {
+          const double2 p = cx_mul(z, A[(long)c * n + k]);
+          A[(long)c * n + r] = make_double2(A[(long)c * n + r].x - p.x, A[(long)c * n + r].y - p.y);
+        }
+      }
+      __syncwarp();
+    }
+  }
+  double smin = 0.0, smax = 0.0;
+  if (want & 2) {
+    // sigma_max in [max entry of the bidiagonal, Gershgorin bound of the GK form]
+    const double ekm = __shfl_up_sync(0xffffffffu, ek, 1);
+    const double em = lane > 0 ? ekm : 0.0;
+    double lo = lane < n ? fmax(dk, ek) : 0.0, hi = lane < n ? dk + fmax(ek, em) : 0.0;
+    lo = warp_max(lo);
+    hi = warp_max(hi);
+    smax = gk_bisect(n, dk, ek, lo, hi, 2 * n) / sc;
+  }
+  if (want & 1) {
+    // sigma_min in (0, min |d_k|] (a triangular matrix's smallest singular
+    // value is at most its smallest diagonal entry)
+    double hi = lane < n ? dk : INFINITY;
+    for (int o = 16; o > 0; o >>= 1) hi = fmin(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    smin = hi > 0.0 ? gk_bisect(n, dk, ek, 0.0, hi, n + 1) / sc : 0.0;
+  }
+  return make_double2(smin, smax);
+}
+
+// Hessian of equation i of system s at (x, t) in complex double, column-
+// major n x n in H; x: n complex doubles.  Lane j builds row j from the
+// Jacobian gather list of (equation i, variable j): a partial that is a
+// constant contributes nothing, 2 x_j gives 2c on the diagonal, x_l gives
+// c at column l, and a staged partial of a monomial of degree >= 3 the
+// second derivatives of c x^e by the common factors.  Deterministic: every
+// cell has one writer and a fixed order.  One warp, n <= 32.
+static __device__ void warp_hessian_rows(const TrackDev &S, int s, int i, int n, double t, const double2 *x, double2 *H) {
+  const int j = threadIdx.x & 31;
+  for (int l = 0; l < n && j < n; ++l) H[(long)l * n + j] = make_double2(0.0, 0.0);
+  if (j < n) {
+    const int g = (S.eq_off[s] + i) * S.maxdim + j;
+    for (int q = S.jg_off[g]; q < S.jg_off[g + 1]; ++q) {
+      const int tr = S.jg_term[q], sl = S.jg_slot[q];
+      if (sl == -1) continue;
+      // the coefficient (1 - t) a + t b
+      const double2 c = make_double2(fma(S.term_b[2 * tr] - S.term_a[2 * tr], t, S.term_a[2 * tr]),
+                                     fma(S.term_b[2 * tr + 1] - S.term_a[2 * tr + 1], t, S.term_a[2 * tr + 1]));
+      if (sl == -2) {
+        double2 &h = H[(long)j * n + j];
+        h = make_double2(h.x + 2.0 * c.x, h.y + 2.0 * c.y);
+      } else if (sl <= -3) {
+        double2 &h = H[(long)(-sl - 3) * n + j];
+        h = make_double2(h.x + c.x, h.y + c.y);
+      } else {
+        const int gm = S.term_mono[tr];
+        const int nv = S.mono_nvr[gm];
+        const int *ix = S.mono_idx + (long)gm * S.maxvar;
+        const int *ex = S.mono_exp + (long)gm * S.maxvar;
+        for (int u = 0; u < nv; ++u) {
+          const double mult = u == sl ? (double)ex[u] * (ex[u] - 1) : (double)ex[u] * ex[sl];
+          if (mult == 0.0) continue;
+          double2 acc = make_double2(c.x * mult, c.y * mult);
+          for (int w = 0; w < nv; ++w)
+            for (int e = ex[w] - (w == u) - (w == sl); e > 0; --e) acc = cx_mul(acc, x[ix[w]]);
+          double2 &h = H[(long)ix[u] * n + j];
+          h = make_double2(h.x + acc.x, h.y + acc.y);
+        }
+      }
+    }
+  }
+  __syncwarp();
+}
+
+// |error estimate| of one component's Pade approximant (numerator degree
+// pdeg, denominator degree qdeg): at the last index top <= min(pdeg + qdeg
+// + 2, K) with |c_top| > 1e-5, the coefficient of the series times the
+// denominator, subtracted from the numerator's when top <= pdeg; 1 when no
+// coefficient passes the threshold or the estimate is below 1e-5
+// (Solution_Error_Estimate and Threshold_Index,
+// Curves/homotopy_pade_approximants.adb:558-568,717-754).
+template <class N>
+__device__ double pade_error_one(const double *c, int K, const double *num, int pdeg, const double *den, int qdeg) {
+  typedef typename N::T T;
+  const int endidx = min(pdeg + qdeg + 2, K);
+  int top = -1;
+  for (int i = endidx; i >= 0; --i)
+    if (N::mag(ldn_at<N>(c, i)) > 1e-5) {
+      top = i;
+      break;
+    }
+  T res = N::one();
+  if (top >= 0) {
+    res = ldn_at<N>(c, top);
+    for (int i = 1; i <= qdeg && i <= top; ++i) res = N::add(res, N::mul(ldn_at<N>(den, i), ldn_at<N>(c, top - i)));
+    if (top <= pdeg) res = N::sub(ldn_at<N>(num, top), res);
+  }
+  const double a = N::mag(res);
+  return a < 1e-5 ? 1.0 : a;
+}
+
 // y = M b, M n x n, one thread per row
 template <class N>
 __device__ void cta_matvec(int n, const double *M, const double *b, double *y) {
@@ -547,8 +803,13 @@ __device__ void cta_matvec(int n, const double *M, const double *b, double *y) {
 
 // Shared-memory layout of a path's CTA (in doubles)
 struct TrackLayout {
-  long xs, V, G, hs, J0, M, r, num, den, xp, xc, hc, Jc, Vc, Gc, red, piv, dinv, feat, mag, degs, hbuf, total;
+  long xs, V, G, hs, J0, M, r, num, den, xp, xc, hc, Jc, Vc, Gc, red, piv, dinv, feat, mag, degs, hbuf, svd, xd, sv,
+      total;
 };
+
+// Matrices of the singular-value jobs of a predictor step: one per warp
+// (the Hessians) and one for the Jacobian.
+static const int kSvdSlots = kTrackThreads / 32 + 1;
 
 __host__ __device__ inline TrackLayout track_layout(int n, int K, int M, int nm, int mv, int Wp, int Wr, int gst) {
   TrackLayout L;
@@ -573,6 +834,9 @@ __host__ __device__ inline TrackLayout track_layout(int n, int K, int M, int nm,
   L.mag = take(n * K1);
   L.degs = take(n);
   L.hbuf = take(2 * 128 + 8);
+  L.svd = take((long)kSvdSlots * n * n * 2);  // complex doubles
+  L.xd = take(2L * n);
+  L.sv = take(n + 2);
   // scratch of the Taylor series and the predictor feedback ...
   const long ov = o;
   L.V = take(nm * 2 * Wp);  // two coefficients per monomial (point evaluations use one)

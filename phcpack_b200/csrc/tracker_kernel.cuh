@@ -126,7 +126,7 @@ __global__ void __launch_bounds__(kTrackThreads, (track_min_blocks<PN, RN, WIDE>
             int *__restrict__ info, double *__restrict__ dinfo, float *__restrict__ log, int log_cap,
             int *__restrict__ log_count) {
   extern __shared__ __align__(16) double sm[];
-  __shared__ int cur;
+  __shared__ int cur, svd_next;
   const int K = P.deg;
   const int Wp = PN::width, Wr = RN::width;
   const int n_max = S.maxdim;
@@ -163,7 +163,7 @@ __global__ void __launch_bounds__(kTrackThreads, (track_min_blocks<PN, RN, WIDE>
     double t = 0.0, dxn;
     point_newton<CN, PN>(S, s, n, 0.0, xc, sm + L.hc, sm + L.Jc, sm + L.Vc, sm + L.Gc, piv, dinv, red, P.corsteps,
                      P.tolres, 1, &dxn);
-    int status = 2, nsteps = 0, nrej = 0;
+    int status = 2, nsteps = 0, nrej = 0, nbpole = 0, nbhess = 0, nbmaxm = 0;
     bool failed = false;
     for (int step_it = 0; step_it < P.maxsteps; ++step_it) {
       // ---------------- predictor: the Taylor series of the path in PN
@@ -184,9 +184,42 @@ __global__ void __launch_bounds__(kTrackThreads, (track_min_blocks<PN, RN, WIDE>
       }
       __syncthreads();
       hom_eval_cta<PN>(S, s, 0, t, xs, K + 1, sm + L.V, sm + L.G, sm + L.hs, sm + L.J0);
+      // the Jacobian and the point in complex double for the singular values
+      double2 *svd = reinterpret_cast<double2 *>(sm + L.svd);
+      double2 *xd = reinterpret_cast<double2 *>(sm + L.xd);
+      double *sv = sm + L.sv;
+      for (int q = ctid(); q < n * n; q += blockDim.x) {
+        const typename PN::T v = ldn_at<PN>(sm + L.J0, q);
+        svd[(long)(kSvdSlots - 1) * n * n + q] = make_double2(md::lead(v.re), md::lead(v.im));
+      }
+      for (int i = ctid(); i < n; i += blockDim.x) {
+        const typename PN::T v = ldn_at<PN>(xs, (long)i * (K + 1));
+        xd[i] = make_double2(md::lead(v.re), md::lead(v.im));
+      }
+      if (ctid() == 0) svd_next = 0;
+      __syncthreads();
+      // the lead warp factors J_0 and forms its inverse; meanwhile the other
+      // warps, and the lead warp when it is done, take the singular-value
+      // jobs of the curvature step: job i < n the largest singular value of
+      // the Hessian of equation i, job n the smallest of the Jacobian
       if (ctid() < 32) {
         warp_lufac<PN>(n, sm + L.J0, piv, dinv);
         warp_luinverse<PN>(n, sm + L.J0, piv, dinv, sm + L.M);
+      }
+      for (;;) {
+        int job = 0;
+        if ((ctid() & 31) == 0) job = atomicAdd(&svd_next, 1);
+        job = __shfl_sync(0xffffffffu, job, 0);
+        if (job > n) break;
+        if (job < n) {
+          double2 *H = svd + (long)(ctid() >> 5) * n * n;
+          warp_hessian_rows(S, s, job, n, t, xd, H);
+          const double2 e = warp_singular_extremes(n, H, 2);
+          if ((ctid() & 31) == 0) sv[job] = e.y;
+        } else {
+          const double2 e = warp_singular_extremes(n, svd + (long)(kSvdSlots - 1) * n * n, 1);
+          if ((ctid() & 31) == 0) sv[n] = e.x;
+        }
       }
       __syncthreads();
       for (int k = 1; k <= K; ++k) {
@@ -199,14 +232,17 @@ __global__ void __launch_bounds__(kTrackThreads, (track_min_blocks<PN, RN, WIDE>
         }
         __syncthreads();
       }
-      // ---------------- Pade and the pole step
+      // ---------------- Pade, the pole step and the curvature step
       int pdeg_i = 0, qdeg_i = 0;
-      double rmin = 1e300;
+      double rmin = 1e300, perr2 = 0.0;
       double *num = sm + L.num, *den = sm + L.den;
       for (int i = ctid(); i < n; i += blockDim.x) {
         const double *ci = xs + (long)i * (K + 1) * Wp;
-        pdeg_i = pade_one<PN>(P.numdeg, P.dendeg, K, ci, num + (long)i * (K + 1) * Wp, den + (long)i * (P.dendeg + 1) * Wp);
+        double *numi = num + (long)i * (K + 1) * Wp, *deni = den + (long)i * (P.dendeg + 1) * Wp;
+        pdeg_i = pade_one<PN>(P.numdeg, P.dendeg, K, ci, numi, deni);
         qdeg_i = (pdeg_i == P.numdeg) ? P.dendeg : 0;
+        const double pe = pade_error_one<PN>(ci, K, numi, pdeg_i, deni, qdeg_i);
+        perr2 = pe * pe;
         const double cd = PN::mag(ldn_at<PN>(ci, K - 2));
         if (cd != 0.0) rmin = fmin(rmin, PN::mag(ldn_at<PN>(ci, K - 3)) / cd);
         double *mg = sm + L.mag + (long)i * (K + 1);
@@ -219,19 +255,38 @@ __global__ void __launch_bounds__(kTrackThreads, (track_min_blocks<PN, RN, WIDE>
         degs[2 * ctid() + 1] = qdeg_i;
       }
       const double r = block_min(rmin, red);
+      const double perr = sqrt(block_sum<md::num<double, false> >(perr2, red));
       const bool rfail = !(r < 1e299);
-      double pole_step = rfail ? P.maxsize : P.pbeta * r;
-      if (pole_step > P.maxsize) pole_step = P.maxsize;
-      double step = pole_step;
+      const double pole_step = rfail ? P.maxsize : P.pbeta * r;
+      // Hesse_Pade (Curves/dobldobl_predictor_convolutions.adb:383-406):
+      // eta = 2 sigma_min(J) / |(sigma_max(H_1), ..., sigma_max(H_n))|_2
+      // (Distance), the curvature step (cbeta eta / |Pade errors|_2)^(1/K)
+      // (Step_Distance, Curves/series_and_predictors.adb:813-825)
+      double hsum = 0.0;
+      for (int i = 0; i < n; ++i) hsum = fma(sv[i], sv[i], hsum);
+      const double eta = hsum > 0.0 ? 2.0 * sv[n] / sqrt(hsum) : INFINITY;
+      const double curv_step = pow(P.cbeta * eta / perr, 1.0 / K);
+      // the smallest of the pole step, the curvature step and maxsize
+      // (Minimum, Curves/three_way_minima.adb:48-62, with its counts)
+      double plain_step;
+      if (pole_step < curv_step) {
+        if (pole_step < P.maxsize) { plain_step = pole_step; ++nbpole; }
+        else { plain_step = P.maxsize; ++nbmaxm; }
+      } else {
+        if (curv_step < P.maxsize) { plain_step = curv_step; ++nbhess; }
+        else { plain_step = P.maxsize; ++nbmaxm; }
+      }
+      if (!(plain_step == plain_step)) plain_step = 0.0;  // a NaN curvature step
+      double step = plain_step;
       bool learned = false;
       float *feat = reinterpret_cast<float *>(sm + L.feat);
       if ((P.step_mode == 1 && model != nullptr) || log != nullptr) {
-        track_features(ctid(), n, K, t, pole_step, sm + L.mag, feat);
+        track_features(ctid(), n, K, t, plain_step, sm + L.mag, feat);
         __syncthreads();
       }
       if (P.step_mode == 1 && model != nullptr) {
         const float lr = mlp_forward_cta(model, feat, reinterpret_cast<float *>(sm + L.hbuf));
-        const double prop = pole_step * exp((double)lr) * P.learn_scale;
+        const double prop = plain_step * exp((double)lr) * P.learn_scale;
         if (prop > P.minsize && prop == prop) {
           step = fmin(prop, P.maxsize);
           learned = true;
@@ -244,9 +299,16 @@ __global__ void __launch_bounds__(kTrackThreads, (track_min_blocks<PN, RN, WIDE>
           // the learned proposal was rejected: redo the step with the plain one
           if (!learned) break;
           learned = false;
-          step = pole_step;
+          step = plain_step;
         }
-        if (t + step > 1.0) step = 1.0 - t;
+        // Bounded_Update (Curves/three_way_minima.adb:96-109): a step that
+        // comes within minsize of t = 1 goes to t = 1
+        if (t + step >= 1.0 - P.minsize) step = 1.0 - t;
+        if (!(step > 0.0)) {  // a zero curvature step (singular Jacobian)
+          if (learned) continue;
+          failed = true;
+          break;
+        }
         // predictor feedback on the mixed residual
         double *xp = sm + L.xp;
         bool ok = false;
@@ -293,13 +355,13 @@ __global__ void __launch_bounds__(kTrackThreads, (track_min_blocks<PN, RN, WIDE>
       }
       if (failed || !accepted) { failed = true; break; }
       // training log: features, accepted step, plain step, proposal, t and
-      // the largest probed step (pole step times 1.5, 2, 3, 4, 6, at most
+      // the largest probed step (plain step times 1.5, 2, 3, 4, 6, at most
       // maxsize and 1 - t) whose Pade prediction still passes the feedback
       if (log != nullptr) {
         double best = step;
         const double mults[5] = {1.5, 2.0, 3.0, 4.0, 6.0};
         for (int q = 0; q < 5; ++q) {
-          double sp = fmin(pole_step * mults[q], P.maxsize);
+          double sp = fmin(plain_step * mults[q], P.maxsize);
           if (t + sp > 1.0) sp = 1.0 - t;
           if (sp <= best) continue;
           const double mr = pade_mixres<PN>(S, s, n, K, P.dendeg, t, sp, num, den, degs, sm + L.xp, sm + L.V,
@@ -312,7 +374,7 @@ __global__ void __launch_bounds__(kTrackThreads, (track_min_blocks<PN, RN, WIDE>
             float *f = log + (long)slot * 32;
             for (int q = 0; q < 24; ++q) f[q] = feat[q];
             f[24] = (float)step;
-            f[25] = (float)pole_step;
+            f[25] = (float)plain_step;
             f[26] = (float)step0;
             f[27] = (float)t;
             f[28] = (float)best;
@@ -358,9 +420,13 @@ __global__ void __launch_bounds__(kTrackThreads, (track_min_blocks<PN, RN, WIDE>
       xend[((long)path * n_max) * 2 * XL + q] = v;
     }
     if (ctid() == 0) {
-      info[3 * path] = status;
-      info[3 * path + 1] = nsteps;
-      info[3 * path + 2] = nrej;
+      int *io = info + (long)kTrackInfo * path;
+      io[0] = status;
+      io[1] = nsteps;
+      io[2] = nrej;
+      io[3] = nbpole;
+      io[4] = nbhess;
+      io[5] = nbmaxm;
       dinfo[2 * path] = t;
       dinfo[2 * path + 1] = res;
     }

@@ -23,7 +23,10 @@ from . import _lib
 # 1024-path benchmark workload: degree-8 series, [4/4] Pade, 3 corrector steps.
 DEFAULT_IPAR = dict(deg=8, numdeg=4, dendeg=4, nit=4, corsteps=3, maxsteps=1000, refine_steps=4)
 DEFAULT_DPAR = dict(pbeta=0.5, alpha=1e-3, maxsize=0.1, minsize=1e-6, tolres=1e-8, epsilon=1e-12,
-                    restol=1e-24, learn_scale=1.0)
+                    restol=1e-24, learn_scale=1.0, cbeta=0.005)
+# ints per path in the tracker's info output: status, steps, rejected steps,
+# and the times the step was the pole step, the curvature step and maxsize
+INFO_WORDS = 6
 STATUS = {0: "success", 1: "step below minsize", 2: "maxsteps reached", 3: "residual above restol"}
 
 
@@ -40,7 +43,7 @@ def params(**kw):
     ipar = np.array([ip[k] for k in ("deg", "numdeg", "dendeg", "nit", "corsteps", "maxsteps", "refine_steps")],
                     np.int32)
     dpar = np.array([dp[k] for k in ("pbeta", "alpha", "maxsize", "minsize", "tolres", "epsilon", "restol",
-                                     "learn_scale")], np.float64)
+                                     "learn_scale", "cbeta")], np.float64)
     return ipar, dpar
 
 
@@ -267,6 +270,9 @@ class TrackResult:
     t: np.ndarray
     residual: np.ndarray
     limbs: int = 4
+    nbpole: np.ndarray = None   # steps set by the pole step,
+    nbhess: np.ndarray = None   # by the curvature step,
+    nbmaxm: np.ndarray = None   # by maxsize
 
     def endpoints(self, maxdim):
         """complex128 end points (leading limbs)"""
@@ -281,10 +287,10 @@ def xend_limbs(rmode):
 
 
 def _result(xend, info, dinfo, limbs=4):
-    info = info.reshape(-1, 3)
+    info = info.reshape(-1, INFO_WORDS)
     dinfo = dinfo.reshape(-1, 2)
     return TrackResult(xend, info[:, 0].copy(), info[:, 1].copy(), info[:, 2].copy(), dinfo[:, 0].copy(),
-                       dinfo[:, 1].copy(), limbs)
+                       dinfo[:, 1].copy(), limbs, info[:, 3].copy(), info[:, 4].copy(), info[:, 5].copy())
 
 
 def track_host(pb: TrackProblem, pmode=1, rmode=2, step_mode=0, model=None, stream_ptr=0, **kw) -> TrackResult:
@@ -293,7 +299,7 @@ def track_host(pb: TrackProblem, pmode=1, rmode=2, step_mode=0, model=None, stre
     out.  stream_ptr: a cudaStream_t as an int (0 = default stream)."""
     ipar, dpar = params(**kw)
     xend = np.zeros(pb.npaths * pb.maxdim * 2 * xend_limbs(rmode))
-    info = np.zeros(pb.npaths * 3, np.int32)
+    info = np.zeros(pb.npaths * INFO_WORDS, np.int32)
     dinfo = np.zeros(pb.npaths * 2)
     m = np.ascontiguousarray(model) if model is not None else None
     _lib.call("phc_track_host", pb.nsys, _lib.ptr(pb.dim), pb.maxvar, _lib.ptr(pb.mono_off), _lib.ptr(pb.mono_nvr),
@@ -336,7 +342,7 @@ class DeviceTracker:
         self.gstaged = int(jg[3])
         self.xend = torch.zeros(pb.npaths * pb.maxdim * 16, dtype=torch.float64, device=device)  # room for rmode 8
         self.rmode = 2
-        self.info = torch.zeros(pb.npaths * 3, dtype=torch.int32, device=device)
+        self.info = torch.zeros(pb.npaths * INFO_WORDS, dtype=torch.int32, device=device)
         self.dinfo = torch.zeros(pb.npaths * 2, dtype=torch.float64, device=device)
         self.queue = torch.zeros(1, dtype=torch.int32, device=device)
         self.log_cap = log_cap

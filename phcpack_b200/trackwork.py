@@ -141,7 +141,7 @@ class TrackWork:
         h2d = (pb.dim.nbytes + pb.mono_off.nbytes + pb.mono_nvr.nbytes + pb.mono_idx.nbytes + pb.mono_exp.nbytes
                + pb.eq_off.nbytes + pb.term_off.nbytes + pb.term_mono.nbytes + pb.term_a.nbytes + pb.term_b.nbytes
                + pb.path_sys.nbytes + pb.x0.nbytes)
-        d2h = pb.npaths * (pb.maxdim * 64 + 12 + 16)
+        d2h = pb.npaths * (pb.maxdim * 64 + 4 * hm.INFO_WORDS + 16)
         return {"value": pb.npaths / t, "unit": self.unit, "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "path": "phc_track_host",
                 "success": int((r.status == 0).sum())}
@@ -196,7 +196,7 @@ def cpu_sample(seconds):
     t = time.perf_counter()
     _, info, _ = pyoracle.track(lib, sub, ipar, dpar, pmode=1, rmode=2, nthreads=cores)
     el = time.perf_counter() - t
-    ok = int((info.reshape(-1, 3)[:, 0] == 0).sum())
+    ok = int((info.reshape(-1, 6)[:, 0] == 0).sum())
     return {"value": n / el, "unit": "paths/s", "cores": cores, "kind": "port",
             "sample": f"{n} of the 1024 paths, {ok} successful, {cores} threads (std::thread), CPU: {model}; the "
                       "reference's tracker is Ada (no GNAT here), so this is the C++ restatement"}

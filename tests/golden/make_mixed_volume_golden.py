@@ -8,7 +8,7 @@ tests/test_rootcounts_mv.py checks the file and recomputes the smaller
 systems from the stored supports.
 
 Run from the repository root with the reference tree at hand:
-    python tests/golden/make_mixed_volume_golden.py /root/reference
+    python tests/golden/make_mixed_volume_golden.py <reference tree>
 """
 import json
 import os
@@ -74,4 +74,4 @@ if __name__ == "__main__":
     if len(sys.argv) > 2 and sys.argv[1] == "--one":
         one(sys.argv[2], None)
     else:
-        main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+        main(sys.argv[1]) if len(sys.argv) > 1 else sys.exit("usage: " + sys.argv[0] + " <reference tree>")

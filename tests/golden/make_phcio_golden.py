@@ -8,7 +8,7 @@ variables are recomputed (phcpack_b200.rootcounts).  The summary goes to
 tests/golden/phcio_demo.json; tests/test_phcio.py checks it.
 
 Run from the repository root with the reference tree at hand:
-    python tests/golden/make_phcio_golden.py /root/reference
+    python tests/golden/make_phcio_golden.py <reference tree>
 """
 import json
 import os
@@ -92,4 +92,4 @@ def main(root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    main(sys.argv[1]) if len(sys.argv) > 1 else sys.exit("usage: " + sys.argv[0] + " <reference tree>")

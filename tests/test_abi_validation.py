@@ -54,7 +54,7 @@ def track_args(pb, pmode=1, rmode=2, ipar=None):
     if ipar is not None:
         ip = np.array(ipar, dtype=np.int32)
     xend = np.zeros(pb.npaths * pb.maxdim * 16)
-    info = np.zeros(pb.npaths * 3, np.int32)
+    info = np.zeros(pb.npaths * 6, np.int32)
     dinfo = np.zeros(pb.npaths * 2)
     p = _lib.ptr
     return (pb.nsys, p(pb.dim), pb.maxvar, p(pb.mono_off), p(pb.mono_nvr), p(pb.mono_idx), p(pb.mono_exp),

@@ -46,7 +46,7 @@ def _worker(rank, world, port, out_path):
     xend, info, dinfo = pyoracle.track(pyoracle.oracle(), sub, ipar, dpar, pmode=1, rmode=2)
     elapsed = time.perf_counter() - t
     tmax = multirank.max_over_ranks(elapsed, dist)
-    rows = np.concatenate([info.reshape(-1, 3).astype(np.float64), dinfo.reshape(-1, 2),
+    rows = np.concatenate([info.reshape(-1, 6).astype(np.float64), dinfo.reshape(-1, 2),
                            xend.reshape(len(mine), -1)], axis=1)
     allrows = multirank.gather_rows(rows, pb.npaths, dist)
     if rank == 0:
@@ -65,7 +65,7 @@ def test_two_gloo_ranks_track_shards_and_gather(tmp_path):
     pb = hm.subset(hm.config4(), np.arange(0, 1024, 64))
     ipar, dpar = hm.params()
     xend, info, dinfo = pyoracle.track(pyoracle.oracle(), pb, ipar, dpar, pmode=1, rmode=2)
-    one = np.concatenate([info.reshape(-1, 3).astype(np.float64), dinfo.reshape(-1, 2),
+    one = np.concatenate([info.reshape(-1, 6).astype(np.float64), dinfo.reshape(-1, 2),
                           xend.reshape(pb.npaths, -1)], axis=1)
     assert np.array_equal(d["rows"], one)  # same per-path results, in path order
     assert float(d["tmax"]) >= float(d["mine"])

@@ -15,6 +15,7 @@ import pytest
 from mdcheck import absdiff
 from oracle import pyoracle
 from phcpack_b200 import newton
+from newton_problems import exponential_test_system
 
 pytestmark = pytest.mark.gpu
 ORC = pyoracle.oracle()
@@ -31,7 +32,7 @@ def check(gpu, orc, exact, prec, cplx, nsys, dim, n1):
 @pytest.mark.parametrize("prec,cplx", [(2, False), (2, True), (4, False), (4, True)])
 def test_newton_schedule_vs_oracle_known_answer(prec, cplx):
     # the n=8, degree-15 workload: <= 3 variables per monomial, exponents {1,2}
-    b, sol = newton.exponential_test_system(7, 4, 8, 15, 8, 3, prec, cplx)
+    b, sol = exponential_test_system(7, 4, 8, 15, 8, 3, prec, cplx)
     ser, fl = newton.newton_host(b, 14, szt=4, schedule=1)
     so, flo = pyoracle.newton_steps(ORC, b, b.deg, 14, schedule=1)
     assert np.array_equal(fl.reshape(-1, 5)[:, 4], flo.reshape(-1, 5)[:, 4])
@@ -43,7 +44,7 @@ def test_newton_schedule_vs_oracle_known_answer(prec, cplx):
 def test_newton_fixed_degree_four_steps_vs_oracle(prec, cplx):
     # 4 steps at fixed working degree 15 (tile 8), started from the series
     # after 6 steps of the reference schedule
-    b, sol = newton.exponential_test_system(5, 3, 8, 15, 8, 3, prec, cplx)
+    b, sol = exponential_test_system(5, 3, 8, 15, 8, 3, prec, cplx)
     so6, _ = pyoracle.newton_steps(ORC, b, b.deg, 6, schedule=1)
     b.input = so6
     ser, fl = newton.newton_host(b, 4, szt=8, schedule=0)
@@ -55,7 +56,24 @@ def test_newton_fixed_degree_four_steps_vs_oracle(prec, cplx):
 def test_newton_known_answer_accuracy_double_double():
     # a system whose error amplification is mild: the exponential series is
     # recovered to double-double accuracy through degree 15
-    b, sol = newton.exponential_test_system(7, 4, 8, 15, 8, 3, 2, False)
+    b, sol = exponential_test_system(7, 4, 8, 15, 8, 3, 2, False)
     ser, _ = newton.newton_host(b, 14, szt=8, schedule=1)
     err = absdiff(ser, sol, 2, False).reshape(4, -1).max(axis=1)
     assert err[1] < 1e-22
+
+
+@pytest.mark.parametrize("prec,cplx,tol", [(2, False, 1e-28), (2, True, 1e-28), (4, False, 1e-60), (4, True, 1e-60)])
+def test_newton_coefficients_equal_oracle_directly(prec, cplx, tol):
+    """The GPU's series against the oracle's, coefficient by coefficient (not
+    through the exact solution): relative difference <= 1e-28 (dd) / 1e-60
+    (qd) of the coefficient's size, at the start (the leading coefficient,
+    max 1) and after each of 6 steps of the reference's schedule."""
+    b, _ = exponential_test_system(11, 3, 8, 15, 8, 3, prec, cplx)
+    for nsteps in (1, 3, 6):
+        ser, _ = newton.newton_host(b, nsteps, szt=4, schedule=1)
+        so, _ = pyoracle.newton_steps(ORC, b, b.deg, nsteps, schedule=1)
+        d = absdiff(ser, so, prec, cplx)
+        mag = np.maximum(np.abs(so.reshape(-1, prec * (2 if cplx else 1))[:, 0]), 1.0 / 6.0)
+        if cplx:
+            mag = np.maximum(mag, np.abs(so.reshape(-1, 2 * prec)[:, prec]))
+        assert (d <= tol * mag).all(), (nsteps, float((d / mag).max()))

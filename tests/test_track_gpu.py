@@ -27,13 +27,49 @@ def endpoint_diff(pb, xa, xb, limbs, width=4):
     return d.max(axis=1)
 
 
+def compare_with_oracle(pb, g, xo, io, max_step_diff):
+    """Identical classification, end points within 1e-26, residuals <= 1e-24,
+    and per-path step counts and step-rule counts close to the oracle's."""
+    io = io.reshape(-1, 6)
+    assert np.array_equal(g.status, io[:, 0])
+    ok = g.status == 0
+    assert (g.residual[ok] <= 1e-24).all()
+    assert (endpoint_diff(pb, g.xend, xo, 2)[ok] <= 1e-26).all()
+    # the same step rules; rounding may move a few decisions of a path
+    assert np.abs(g.steps - io[:, 1]).max() <= max_step_diff
+    assert abs(g.steps.mean() - io[:, 1].mean()) <= 0.05 * io[:, 1].mean()
+    # one step-size decision (pole, curvature or maxsize) per predictor step
+    assert np.array_equal((g.nbpole + g.nbhess + g.nbmaxm)[ok], g.steps[ok])
+    assert abs(g.nbhess.sum() - io[:, 4].sum()) <= 0.05 * max(1, io[:, 4].sum())
+    return ok
+
+
+@pytest.mark.parametrize("step_mode", [0, 1])
+def test_track_config4_all_paths_vs_oracle(step_mode):
+    """All 1024 paths of the dense quadratic n = 10 workload with the FP64
+    predictor and the double-double corrector, with the plain step and with
+    the learned step (the committed model) against the oracle's run with the
+    same step rule and the same network."""
+    from phcpack_b200 import trackwork
+    pb = hm.config4()
+    ipar, dpar = hm.params()
+    model = trackwork.load_model_bytes() if step_mode else None
+    if step_mode:
+        assert model is not None
+    g = hm.track_host(pb, pmode=1, rmode=2, step_mode=step_mode, model=model)
+    xo, io, _ = pyoracle.track(ORC, pb, ipar, dpar, pmode=1, rmode=2, nthreads=16, step_mode=step_mode,
+                               model=model)
+    ok = compare_with_oracle(pb, g, xo, io, max_step_diff=4)
+    assert ok.all()
+
+
 @pytest.mark.parametrize("pmode", [1, 2])
 def test_track_config4_sample_vs_oracle(pmode):
     pb = hm.subset(hm.config4(), np.arange(0, 1024, 16))
     ipar, dpar = hm.params()
     g = hm.track_host(pb, pmode=pmode, rmode=2)
     xo, io, do = pyoracle.track(ORC, pb, ipar, dpar, pmode=pmode, rmode=2, nthreads=8)
-    io = io.reshape(-1, 3)
+    io = io.reshape(-1, 6)
     assert np.array_equal(g.status, io[:, 0])
     ok = g.status == 0
     assert ok.mean() > 0.9
@@ -48,7 +84,7 @@ def test_track_quad_double_refinement():
     ipar, dpar = hm.params(restol=1e-50)
     g = hm.track_host(pb, pmode=1, rmode=4, restol=1e-50)
     xo, io, _ = pyoracle.track(ORC, pb, ipar, dpar, pmode=1, rmode=4)
-    assert np.array_equal(g.status, io.reshape(-1, 3)[:, 0])
+    assert np.array_equal(g.status, io.reshape(-1, 6)[:, 0])
     ok = g.status == 0
     assert ok.all()
     assert (endpoint_diff(pb, g.xend, xo, 4)[ok] <= 1e-50).all()
@@ -62,7 +98,7 @@ def test_track_octo_double_refinement():
     ipar, dpar = hm.params(restol=1e-100, refine_steps=6)
     g = hm.track_host(pb, pmode=1, rmode=8, restol=1e-100, refine_steps=6)
     xo, io, _ = pyoracle.track(ORC, pb, ipar, dpar, pmode=1, rmode=8)
-    assert np.array_equal(g.status, io.reshape(-1, 3)[:, 0])
+    assert np.array_equal(g.status, io.reshape(-1, 6)[:, 0])
     ok = g.status == 0
     assert ok.all()
     assert (g.residual <= 1e-100).all()
@@ -94,7 +130,7 @@ def test_track_mixed_sizes_vs_oracle():
     # success / failure classification; on diverging paths (solutions at
     # infinity of these sparse systems) the failure mode itself (step below
     # minsize or a large residual at t = 1) depends on rounding
-    assert np.array_equal(g.status == 0, io.reshape(-1, 3)[:, 0] == 0)
+    assert np.array_equal(g.status == 0, io.reshape(-1, 6)[:, 0] == 0)
     ok = g.status == 0
     assert (endpoint_diff(pb, g.xend, xo, 2)[ok] <= 1e-26 * np.maximum(1, np.abs(g.endpoints(pb.maxdim)).max(axis=1)[ok])).all()
 
@@ -132,7 +168,7 @@ def test_track_dimension_extremes_vs_oracle(n):
     ipar, dpar = hm.params()
     g = hm.track_host(pb, pmode=1, rmode=2)
     xo, io, _ = pyoracle.track(ORC, pb, ipar, dpar, pmode=1, rmode=2)
-    io = io.reshape(-1, 3)
+    io = io.reshape(-1, 6)
     assert np.array_equal(g.status == 0, io[:, 0] == 0)
     ok = (g.status == 0) & (io[:, 0] == 0)
     assert ok.any()

@@ -31,7 +31,7 @@ def test_oracle_tracker_config4_sample():
     pb = hm.subset(hm.config4(), np.arange(0, 1024, 128))
     ipar, dpar = hm.params()
     xe, info, di = pyoracle.track(ORC, pb, ipar, dpar, pmode=1, rmode=2, nthreads=4)
-    info = info.reshape(-1, 3)
+    info = info.reshape(-1, 6)
     di = di.reshape(-1, 2)
     assert (info[:, 0] == 0).all()
     assert (di[:, 1] <= 1e-24).all()
@@ -46,7 +46,7 @@ def test_oracle_tracker_all_dd_predictor_same_endpoints():
     ipar, dpar = hm.params()
     x1, i1, _ = pyoracle.track(ORC, pb, ipar, dpar, pmode=1, rmode=2)
     x2, i2, _ = pyoracle.track(ORC, pb, ipar, dpar, pmode=2, rmode=2)
-    assert np.array_equal(i1.reshape(-1, 3)[:, 0], i2.reshape(-1, 3)[:, 0])
+    assert np.array_equal(i1.reshape(-1, 6)[:, 0], i2.reshape(-1, 6)[:, 0])
     e1 = x1.reshape(-1, 8)
     e2 = x2.reshape(-1, 8)
     assert np.abs((e1[:, 0] - e2[:, 0]) + (e1[:, 1] - e2[:, 1])).max() < 1e-26

@@ -5,9 +5,10 @@ device memory to their own allocator, or must not allocate once set up
 cannot let the library allocate; this entry point takes its
 workspace from a static device array instead.  Checked through the C ABI
 against phc_bals_solve with a caller-provided workspace, on two calls in a
-row with different shapes and precisions (the shared array keeps the first
-call's contents), within the tolerance of the other least-squares tests:
-per degree block, 1e4 * eps_md * max(1, |x|)."""
+row of the same shape, and on two calls in a row of different shapes and
+precisions (the shared array keeps the previous call's contents), within
+the tolerance of the other least-squares tests: per degree block,
+1e4 * eps_md * max(1, |x|)."""
 import numpy as np
 import pytest
 
@@ -51,6 +52,19 @@ def test_static_workspace_matches_allocating_entry_point_twice(shape):
     prec, cplx, ninst, n, degp1, szt = shape
     rng = np.random.default_rng(n * degp1)
     for call in range(2):  # two calls in a row share the static array
+        mat = wl.random_numbers(rng, (ninst, degp1, n, n), prec, cplx, "normal")
+        rhs = wl.random_numbers(rng, (ninst, degp1, n), prec, cplx, "normal")
+        xs, fs = run(True, prec, cplx, ninst, n, degp1, szt, mat, rhs)
+        xr, fr = run(False, prec, cplx, ninst, n, degp1, szt, mat, rhs)
+        assert np.array_equal(fs, fr)
+        assert agree(xs, xr, prec, cplx, ninst, degp1, n)
+
+
+def test_static_workspace_two_shapes_back_to_back():
+    """A quad-double real call, then a double-double complex call of another
+    shape right after it, each against the allocating entry point."""
+    rng = np.random.default_rng(77)
+    for prec, cplx, ninst, n, degp1, szt in [(4, False, 3, 64, 8, 32), (2, True, 5, 16, 9, 8)]:
         mat = wl.random_numbers(rng, (ninst, degp1, n, n), prec, cplx, "normal")
         rhs = wl.random_numbers(rng, (ninst, degp1, n), prec, cplx, "normal")
         xs, fs = run(True, prec, cplx, ninst, n, degp1, szt, mat, rhs)
