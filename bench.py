@@ -23,7 +23,6 @@ from __future__ import annotations
 import argparse
 import json
 import os
-import re
 import subprocess
 import sys
 import threading
@@ -44,6 +43,7 @@ def parse():
     ap.add_argument("--workload", default=os.environ.get("PHC_BENCH_WORKLOAD", "track"),
                     choices=["track", "eval", "qr"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="budget of the CPU baseline sample")
+    ap.add_argument("--no-blocks", action="store_true", help="track: leave out the eval and qr blocks")
     return ap.parse_args()
 
 
@@ -129,15 +129,6 @@ def fp64_peak_tflops(torch, dev):
     return 2.0 * n ** 3 / best / 1e12
 
 
-def profile_traffic(kernel_tag: str):
-    """DRAM bytes per launch recorded from an ncu capture in profiles/."""
-    path = os.path.join(ROOT, "profiles", f"{kernel_tag}.md")
-    if not os.path.exists(path):
-        return None
-    m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", open(path).read())
-    return float(m.group(1)) if m else None
-
-
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -211,7 +202,7 @@ def main():
     fp64 = fp64_peak_tflops(torch, dev)
     mean_kernel = float(np.mean(kern_s)) / max(1, work.dominant_launches_per_step)
     achieved = work.dominant_flops_per_launch / mean_kernel / 1e12
-    traffic = profile_traffic(work.kernel_tag)
+    traffic = getattr(work, "traffic_bytes_per_launch", None)
     cpu = benchwork.cpu_baseline(args.workload, args.cpu_seconds) if (world == 1 or rank == 0) else None
     out = {
         "metric": work.metric,
@@ -239,6 +230,9 @@ def main():
         "clocks": clk,
         "check": check,
     }
+    if args.workload == "track" and not args.no_blocks and world == 1:
+        out["blocks"] = {name: benchwork.side_block(name, torch, dev, fp64, peaks.get("hbm_gbs"))
+                         for name in ("eval", "qr")}
     print(json.dumps(out), flush=True)
     return 0
 

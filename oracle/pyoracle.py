@@ -25,6 +25,9 @@ _I = ctypes.POINTER(ctypes.c_int)
 
 
 SHIM_BIN = os.path.join(HERE, "_ref", "test_dbl2_polynomials")
+# the reference's matrix test programs linked with ref_shim_matrices.cu
+SHIM_MATRIX_BINS = {name: os.path.join(HERE, "_ref", name) for name in ("test_dbl2_baqr", "test_dbl4_baqr",
+                                                                        "test_dbl2_tabs")}
 
 
 def build(ref: bool = True) -> None:
@@ -36,7 +39,7 @@ def build(ref: bool = True) -> None:
     if ref and REF_TREE and os.path.isdir(REF_TREE):
         targets.append("_ref/libphcref.so")
         if os.path.exists(os.path.join(HERE, "..", "phcpack_b200", "libphcb200.so")):
-            targets.append("_ref/test_dbl2_polynomials")
+            targets += ["_ref/test_dbl2_polynomials", "_ref/test_dbl2_baqr", "_ref/test_dbl4_baqr", "_ref/test_dbl2_tabs"]
     subprocess.run(["make", "-s", "-C", HERE, f"REF={REF_TREE}"] + targets, check=True)
 
 

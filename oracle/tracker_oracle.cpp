@@ -362,6 +362,7 @@ template <> void convert(const cx<dd> &a, cx<double> &b) { b = cx<double>(a.re.h
 template <> void convert(const cx<dd> &a, cx<dd> &b) { b = a; }
 template <> void convert(const cx<double> &a, cx<double> &b) { b = a; }
 template <> void convert(const cx<double> &a, cx<dd> &b) { b = cx<dd>(dd(a.re), dd(a.im)); }
+template <> void convert(const cx<double> &a, cx<qd> &b) { b = cx<qd>(qd(a.re), qd(a.im)); }
 template <> void convert(const cx<dd> &a, cx<qd> &b) { b = cx<qd>(qd(a.re), qd(a.im)); }
 template <> void convert(const cx<qd> &a, cx<qd> &b) { b = a; }
 template <> void convert(const cx<dd> &a, cx<od> &b) { b = cx<od>(od(a.re), od(a.im)); }
@@ -935,7 +936,8 @@ extern "C" {
 
 // Track npaths paths with nthreads host threads.  pmode: predictor
 // precision (1 double, 2 double-double); rmode: refinement precision
-// (2 dd, 4 qd, 8 od); the corrector is double-double; step_mode 1 with a
+// (2 dd, 4 qd, 8 od; 1 with pmode 1: all in double, corrector included);
+// the corrector is double-double otherwise; step_mode 1 with a
 // model buffer: the learned step.  ipar and dpar as in phc_track (dpar[8]
 // = cbeta).  x0: start points, maxdim complex doubles per path; xend:
 // maxdim complex quad-doubles per path (octo-doubles for rmode 8; lower
@@ -957,7 +959,10 @@ int orc_track(int nsys, const int *dim, int maxvar, const int *mono_off, const i
   P.step_mode = step_mode;
   P.model = step_mode == 1 ? static_cast<const unsigned char *>(model) : nullptr;
   if (P.numdeg + P.dendeg != P.deg || P.deg < 3 || !(P.cbeta > 0.0)) return -1;
-  if ((pmode != 1 && pmode != 2) || (rmode != 2 && rmode != 4 && rmode != 8)) return -1;
+  // rmode 1 (with pmode 1): everything in double, the FP64 run the
+  // multiple-double results are compared with
+  if ((pmode != 1 && pmode != 2) || (rmode != 1 && rmode != 2 && rmode != 4 && rmode != 8)) return -1;
+  if (rmode == 1 && pmode != 1) return -1;
   std::atomic<int> next(0);
   auto work = [&]() {
     for (;;) {
@@ -967,7 +972,8 @@ int orc_track(int nsys, const int *dim, int maxvar, const int *mono_off, const i
       PathOut o;
       double *xe = xend + (long)p * maxdim * (rmode == 8 ? 16 : 8);
       const double *xs = x0 + (long)p * maxdim * 2;
-      if (pmode == 1 && rmode == 2) o = track_path<cx<double>, cx<dd>, cx<dd> >(S, s, P, xs, xe);
+      if (rmode == 1) o = track_path<cx<double>, cx<double>, cx<double> >(S, s, P, xs, xe);
+      else if (pmode == 1 && rmode == 2) o = track_path<cx<double>, cx<dd>, cx<dd> >(S, s, P, xs, xe);
       else if (pmode == 1 && rmode == 4) o = track_path<cx<double>, cx<dd>, cx<qd> >(S, s, P, xs, xe);
       else if (pmode == 1) o = track_path<cx<double>, cx<dd>, cx<od> >(S, s, P, xs, xe);
       else if (rmode == 2) o = track_path<cx<dd>, cx<dd>, cx<dd> >(S, s, P, xs, xe);

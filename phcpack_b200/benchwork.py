@@ -111,6 +111,9 @@ class EvalWork:
     unit = "systems/s"
     dtype = "f64 (complex double-double limbs)"
     kernel_tag = "k_system_evaldiff_config2"
+    # DRAM bytes of one launch on the 4096 systems, from the ncu capture of
+    # profiles/k_system_evaldiff_config2.md (512 systems, scaled by 8)
+    traffic_bytes_per_launch = 1.6408e10
     l2_note = None
     dominant_launches_per_step = 1
 
@@ -194,6 +197,42 @@ def make(name, dev, rank):
         from . import qrwork
         return qrwork.QRWork(torch, dev, rank)
     raise ValueError(name)
+
+
+def side_block(name, torch, dev, fp64_tflops, hbm_gbs, steps=3, warm=2):
+    """A short timed run of another workload of the path (eval: the
+    4096-system eval/diff; qr: the 512-instance quad-double least squares)
+    for the track line: CUDA events around each launch, inputs resident,
+    inputs larger than L2, and the workload's roofline."""
+    work = make(name, dev, 0)
+    stream = torch.cuda.Stream(device=dev)
+    for _ in range(warm):
+        work.step(stream)
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        work.step(stream)
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1) / 1e3)
+    t = float(np.mean(times))
+    achieved = work.dominant_flops_per_launch / t / 1e12
+    out = {"metric": work.metric, "value": work.units_per_step / t, "unit": work.unit, "steps": steps,
+           "ms_per_step": t * 1e3, "config": work.config,
+           "roofline": {"bound": "fp64", "achieved": achieved, "peak": fp64_tflops, "unit": "TFLOP/s",
+                        "frac": achieved / fp64_tflops, "flops_convention": work.flops_note,
+                        "traffic": getattr(work, "traffic_bytes_per_launch", None),
+                        "hbm_gbs_achieved": work.dominant_bytes_per_launch / t / 1e9, "hbm_peak_gbs": hbm_gbs}}
+    try:
+        out["check"] = work.check()
+    except Exception as e:
+        out["check"] = {"error": str(e)[:200]}
+    del work
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    return out
 
 
 # ---------------------------------------------------------- CPU baseline

@@ -126,7 +126,7 @@ __global__ void __launch_bounds__(kTrackThreads, (track_min_blocks<PN, RN, WIDE>
             int *__restrict__ info, double *__restrict__ dinfo, float *__restrict__ log, int log_cap,
             int *__restrict__ log_count) {
   extern __shared__ __align__(16) double sm[];
-  __shared__ int cur, svd_next;
+  __shared__ int cur;
   const int K = P.deg;
   const int Wp = PN::width, Wr = RN::width;
   const int n_max = S.maxdim;
@@ -196,29 +196,22 @@ __global__ void __launch_bounds__(kTrackThreads, (track_min_blocks<PN, RN, WIDE>
         const typename PN::T v = ldn_at<PN>(xs, (long)i * (K + 1));
         xd[i] = make_double2(md::lead(v.re), md::lead(v.im));
       }
-      if (ctid() == 0) svd_next = 0;
       __syncthreads();
       // the lead warp factors J_0 and forms its inverse; meanwhile the other
-      // warps, and the lead warp when it is done, take the singular-value
-      // jobs of the curvature step: job i < n the largest singular value of
-      // the Hessian of equation i, job n the smallest of the Jacobian
+      // warps form the Hessians at the point and their Frobenius norms, upper
+      // bounds of their largest singular values (sv[i] = |H_i|_F^2)
       if (ctid() < 32) {
         warp_lufac<PN>(n, sm + L.J0, piv, dinv);
         warp_luinverse<PN>(n, sm + L.J0, piv, dinv, sm + L.M);
-      }
-      for (;;) {
-        int job = 0;
-        if ((ctid() & 31) == 0) job = atomicAdd(&svd_next, 1);
-        job = __shfl_sync(0xffffffffu, job, 0);
-        if (job > n) break;
-        if (job < n) {
-          double2 *H = svd + (long)(ctid() >> 5) * n * n;
-          warp_hessian_rows(S, s, job, n, t, xd, H);
-          const double2 e = warp_singular_extremes(n, H, 2);
-          if ((ctid() & 31) == 0) sv[job] = e.y;
-        } else {
-          const double2 e = warp_singular_extremes(n, svd + (long)(kSvdSlots - 1) * n * n, 1);
-          if ((ctid() & 31) == 0) sv[n] = e.x;
+      } else {
+        const int hw = (ctid() >> 5), nhw = kTrackThreads / 32 - 1;
+        for (int i = hw - 1; i < n; i += nhw) {
+          double2 *H = svd + (long)hw * n * n;
+          warp_hessian_rows(S, s, i, n, t, xd, H);
+          double f = 0.0;
+          for (int q = ctid() & 31; q < n * n; q += 32) f = fma(H[q].x, H[q].x, fma(H[q].y, H[q].y, f));
+          f = warp_sum_d(f);
+          if ((ctid() & 31) == 0) sv[i] = f;
         }
       }
       __syncthreads();
@@ -242,7 +235,7 @@ __global__ void __launch_bounds__(kTrackThreads, (track_min_blocks<PN, RN, WIDE>
         pdeg_i = pade_one<PN>(P.numdeg, P.dendeg, K, ci, numi, deni);
         qdeg_i = (pdeg_i == P.numdeg) ? P.dendeg : 0;
         const double pe = pade_error_one<PN>(ci, K, numi, pdeg_i, deni, qdeg_i);
-        perr2 = pe * pe;
+        perr2 = fma(pe, pe, perr2);
         const double cd = PN::mag(ldn_at<PN>(ci, K - 2));
         if (cd != 0.0) rmin = fmin(rmin, PN::mag(ldn_at<PN>(ci, K - 3)) / cd);
         double *mg = sm + L.mag + (long)i * (K + 1);
@@ -261,11 +254,51 @@ __global__ void __launch_bounds__(kTrackThreads, (track_min_blocks<PN, RN, WIDE>
       // Hesse_Pade (Curves/dobldobl_predictor_convolutions.adb:383-406):
       // eta = 2 sigma_min(J) / |(sigma_max(H_1), ..., sigma_max(H_n))|_2
       // (Distance), the curvature step (cbeta eta / |Pade errors|_2)^(1/K)
-      // (Step_Distance, Curves/series_and_predictors.adb:813-825)
-      double hsum = 0.0;
-      for (int i = 0; i < n; ++i) hsum = fma(sv[i], sv[i], hsum);
-      const double eta = hsum > 0.0 ? 2.0 * sv[n] / sqrt(hsum) : INFINITY;
-      const double curv_step = pow(P.cbeta * eta / perr, 1.0 / K);
+      // (Step_Distance, Curves/series_and_predictors.adb:813-825).
+      // sigma_min(J) >= 1 / |J^{-1}|_F and sigma_max(H_i) <= |H_i|_F bound
+      // eta, and so the curvature step, from below; when that bound is
+      // already above min(pole step, maxsize) the curvature step cannot be
+      // the smallest and the minimum below takes the same branch with it as
+      // with +inf, so the singular values are computed only otherwise (a 1 %
+      // margin covers the rounding of the bounds).
+      double mf2 = 0.0;
+      for (int q = ctid(); q < n * n; q += blockDim.x) {
+        const double a = PN::mag(ldn_at<PN>(sm + L.M, q));
+        mf2 = fma(a, a, mf2);
+      }
+      mf2 = block_sum<md::num<double, false> >(mf2, red);
+      double hf2 = 0.0;
+      for (int i = 0; i < n; ++i) hf2 += sv[i];
+      const double cap = fmin(pole_step, P.maxsize);
+      double curv_step = INFINITY;
+      bool exact = hf2 > 0.0;  // all Hessians zero: eta and the curvature step are +inf
+      if (exact && mf2 > 0.0 && mf2 < INFINITY && hf2 < INFINITY) {
+        const double curv_lo = pow(P.cbeta * (2.0 / sqrt(mf2 * hf2)) / perr, 1.0 / K);
+        exact = !(curv_lo > 1.01 * cap);
+      }
+      if (exact) {
+        // the singular values, a job per warp: job i < n the largest of the
+        // Hessian of equation i, job n the smallest of the Jacobian (its copy
+        // from before the LU); every thread has read the norms in sv
+        __syncthreads();
+        for (int job = ctid() >> 5; job <= n; job += kTrackThreads / 32) {
+          if (job < n) {
+            double2 *H = svd + (long)(ctid() >> 5) * n * n;
+            warp_hessian_rows(S, s, job, n, t, xd, H);
+            const double2 e = warp_singular_extremes(n, H, 2);
+            if ((ctid() & 31) == 0) sv[job] = e.y;
+          } else {
+            const double2 e = warp_singular_extremes(n, svd + (long)(kSvdSlots - 1) * n * n, 1);
+            if ((ctid() & 31) == 0) sv[n] = e.x;
+          }
+        }
+        __syncthreads();
+        double hsum = 0.0;
+        for (int i = 0; i < n; ++i) hsum = fma(sv[i], sv[i], hsum);
+        const double eta = hsum > 0.0 ? 2.0 * sv[n] / sqrt(hsum) : INFINITY;
+        curv_step = pow(P.cbeta * eta / perr, 1.0 / K);
+        __syncthreads();
+      }
       // the smallest of the pole step, the curvature step and maxsize
       // (Minimum, Curves/three_way_minima.adb:48-62, with its counts)
       double plain_step;

@@ -89,6 +89,9 @@ class TrackWork:
     unit = "paths/s"
     dtype = "f64 predictor + double-double corrector (complex)"
     kernel_tag = "k_track_config4"
+    # DRAM bytes of one launch on the 1024 paths, from the ncu capture of
+    # profiles/k_track_config4.md (dram__bytes_read.sum + dram__bytes_write.sum)
+    traffic_bytes_per_launch = 5.159e6
     dominant_launches_per_step = 1
 
     def __init__(self, torch, dev, rank, npaths=1024):
@@ -146,9 +149,33 @@ class TrackWork:
                 "d2h_bytes_per_step": int(d2h), "path": "phc_track_host",
                 "success": int((r.status == 0).sum())}
 
+    def timed(self, dt, stream, reps=3, **kw):
+        """Median CUDA-event seconds of `reps` batched launches of dt.run(**kw)
+        after one untimed launch; returns (seconds, result)."""
+        torch = self.torch
+        dt.run(stream=stream, **kw)
+        times = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            dt.run(stream=stream, **kw)
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1) / 1e3)
+        return float(np.median(times)), dt.result()
+
+    @staticmethod
+    def summary(npaths, t, r):
+        ok = r.status == 0
+        return {"paths_per_s": npaths / t, "ms": t * 1e3, "success": int(ok.sum()),
+                "max_residual_success": float(r.residual[ok].max()) if ok.any() else None,
+                "mean_steps": float(r.steps.mean()), "max_steps": int(r.steps.max()),
+                "rejected": int(r.rejected.sum()), "steps_pole_curvature_maxsize":
+                    [int(r.nbpole.sum()), int(r.nbhess.sum()), int(r.nbmaxm.sum())]}
+
     def plain(self, stream):
-        """The plain arrangement: all double-double, plain pole step, one
-        path per launch."""
+        """The plain arrangement: all double-double, plain step, one path
+        per launch."""
         torch = self.torch
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         self.dt.run(pmode=2, rmode=2, step_mode=0, one_per_launch=True, stream=stream)  # warm
@@ -161,6 +188,75 @@ class TrackWork:
         r = self.dt.result()
         return t, r
 
+    def ablation(self, stream):
+        """The three patterns apart on the same 1024 paths, each batched:
+        all double-double with the plain step, the precision split with the
+        plain step, the precision split with the learned step (the measured
+        arm), and the plain one-path-per-launch all-dd arrangement."""
+        n = self.pb.npaths
+        out = {}
+        t, r = self.timed(self.dt, stream, pmode=2, rmode=2, step_mode=0)
+        out["batched_all_dd_plain_step"] = self.summary(n, t, r)
+        t, r = self.timed(self.dt, stream, pmode=1, rmode=2, step_mode=0)
+        out["batched_split_plain_step"] = self.summary(n, t, r)
+        plain_split = r
+        if self.step_mode:
+            t, r = self.timed(self.dt, stream, pmode=1, rmode=2, step_mode=1)
+            out["batched_split_learned_step"] = self.summary(n, t, r)
+            out["batched_split_learned_step"]["same_classification_as_plain"] = bool(
+                np.array_equal(r.status == 0, plain_split.status == 0))
+        tp, rp = self.plain(stream)
+        out["plain_one_path_per_launch"] = dict(self.summary(n, tp, rp), same_classification=bool(
+            np.array_equal(rp.status == 0, plain_split.status == 0)))
+        return out
+
+    def config5(self, stream):
+        """The mixed-size workload: 64 sparse quadratic systems, n in 6..14,
+        total-degree paths capped at 256 per system, learned step (when a
+        model is present), quad-double endpoint refinement; classification
+        against the plain step."""
+        pb = hm.config5()
+        dt = hm.DeviceTracker(pb, device=self.dt.xend.device)
+        out = {"workload": pb.note, "paths": pb.npaths, "dims": [int(pb.dim.min()), int(pb.dim.max())]}
+        t0, r0 = self.timed(dt, stream, reps=2, pmode=1, rmode=4, step_mode=0)
+        out["plain_step"] = self.summary(pb.npaths, t0, r0)
+        if self.step_mode:
+            dt.set_model(self.model)
+            t1, r1 = self.timed(dt, stream, reps=2, pmode=1, rmode=4, step_mode=1)
+            out["learned_step"] = self.summary(pb.npaths, t1, r1)
+            out["learned_step"]["same_classification_as_plain"] = bool(np.array_equal(r1.status == 0,
+                                                                                      r0.status == 0))
+        return out
+
+    def endpoint_errors(self, npaths=16):
+        """North-star (a): end points of a sample of paths against an
+        octo-double run of the host oracle (same step rule; od refinement),
+        for the GPU's double-double end points and for an FP64 run of the
+        same tracker on the host (all double, corrector included)."""
+        from oracle import pyoracle
+        lib = pyoracle.oracle()
+        sub = hm.subset(self.pb, np.arange(0, self.pb.npaths, self.pb.npaths // npaths)[:npaths])
+        ipar, dpar = hm.params()
+        g = hm.track_host(sub, pmode=1, rmode=2)
+        x8, i8, _ = pyoracle.track(lib, sub, ipar, dpar, pmode=1, rmode=8, nthreads=npaths)
+        _, dp64 = hm.params(restol=1e-12)
+        x1, i1, _ = pyoracle.track(lib, sub, ipar, dp64, pmode=1, rmode=1, nthreads=npaths)
+        md = sub.maxdim
+
+        def err(xq, limbs_q):
+            a = xq.reshape(-1, md, 2, limbs_q)
+            b = x8.reshape(-1, md, 2, 8)
+            d = np.zeros(a.shape[:3])
+            for l in range(limbs_q - 1, -1, -1):
+                d = d + (a[..., l] - b[..., l])
+            d = d + (-b[..., limbs_q:].sum(axis=-1))
+            mag = np.maximum(1.0, np.abs(b[..., 0]).max(axis=(1, 2)))
+            return float((np.abs(d).max(axis=(1, 2)) / mag).max())
+        ok = (g.status == 0) & (i8.reshape(-1, 6)[:, 0] == 0)
+        return {"paths": int(sub.npaths), "all_succeeded": bool(ok.all()),
+                "max_rel_error_vs_od_oracle": {"gpu_double_double": err(g.xend, 4),
+                                               "host_fp64_run": err(x1, 4)}}
+
     def check(self):
         torch = self.torch
         out = {}
@@ -171,11 +267,15 @@ class TrackWork:
         out["mean_steps"] = float(r.steps.mean())
         out["rejected"] = int(r.rejected.sum())
         s = torch.cuda.Stream(device=self.dt.xend.device)
-        tp, rp = self.plain(s)
-        out["plain_one_path_per_launch"] = {"paths_per_s": self.pb.npaths / tp, "seconds": tp,
-                                            "success": int((rp.status == 0).sum()),
-                                            "mean_steps": float(rp.steps.mean()),
-                                            "same_classification": bool(np.array_equal(rp.status == 0, ok))}
+        out["ablation"] = self.ablation(s)
+        try:
+            out["config5"] = self.config5(s)
+        except Exception as e:  # a side block never decides the headline
+            out["config5"] = {"error": str(e)[:200]}
+        try:
+            out["endpoint_errors"] = self.endpoint_errors()
+        except Exception as e:
+            out["endpoint_errors"] = {"error": str(e)[:200]}
         return out
 
 

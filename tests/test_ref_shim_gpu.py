@@ -29,3 +29,55 @@ def test_reference_tester_through_the_shim(dim, nterms, deg, seed):
     assert run.returncode == 0, run.stderr[-2000:]
     assert "on real data" in out and "on complex data" in out, out[-2000:]
     assert "All tests passed." in out, out[-3000:]
+
+
+def run_program(name, stdin):
+    path = pyoracle.SHIM_MATRIX_BINS[name]
+    if not os.path.exists(path):
+        pytest.skip(f"the reference's {name} was not built here")
+    run = subprocess.run([path], input=stdin, capture_output=True, text=True, timeout=600)
+    assert run.returncode == 0, run.stderr[-2000:]
+    assert "failed" not in run.stderr, run.stderr[-2000:]
+    return run.stdout
+
+
+@pytest.mark.parametrize("name,szt,nbt,nrows", [("test_dbl2_baqr", 8, 2, 16), ("test_dbl2_baqr", 8, 4, 40),
+                                                ("test_dbl4_baqr", 32, 2, 64), ("test_dbl4_baqr", 8, 3, 30)])
+def test_reference_blocked_qr_tester_through_the_shim(name, szt, nbt, nrows):
+    """PHCpack's test_dbl2_baqr / test_dbl4_baqr (Matrices/, unchanged) with
+    GPU_dbl{2,4}_blocked_houseqr and GPU_cmplx{2,4}_blocked_houseqr of
+    oracle/ref_shim_matrices.cu: in mode 2 the tester factors a random real
+    and a random complex matrix on its CPU code and through the GPU entry
+    points and probes Q^T A = R and the orthogonality of Q at its own
+    tolerance (1e-20 dd, 1e-40 qd) for each: four passes."""
+    one = f"7\n{szt}\n{nbt}\n{nrows}\n0\n2\n"
+    out = run_program(name, one + one)
+    assert out.count("The test succeeded.") == 4, out[-3000:]
+    assert "The test failed" not in out
+
+
+def sums(out, label):
+    import re
+    return [float(v) for v in re.findall(re.escape(label) + r"\s*:\s*([0-9.eE+-]+)", out)]
+
+
+@pytest.mark.parametrize("dim,szt,nbt", [(8, 8, 4), (16, 16, 2), (12, 4, 6)])
+def test_reference_tiled_solver_tester_through_the_shim(dim, szt, nbt):
+    """PHCpack's test_dbl2_tabs (Matrices/, unchanged) with
+    GPU_dbl2_upper_inverse, GPU_cmplx2_upper_inverse,
+    GPU_dbl2_upper_tiled_solver and GPU_cmplx2_upper_tiled_solver of the
+    shim: random upper triangular matrices (real and complex), the GPU
+    inverse of one tile and the tiled solve.  The tester prints the sums of
+    the differences between its CPU results and the GPU's (inverse, the
+    inverted diagonal tiles) and the errors of both solutions against the
+    exact one; the GPU's are at double-double rounding level."""
+    stdin = f"{dim}\n0\n{dim}\n0\n{szt}\n{nbt}\n0\n1\n{szt}\n{nbt}\n0\n1\n"
+    out = run_program("test_dbl2_tabs", stdin)
+    inv = sums(out, "Sum of errors on inverse")
+    diag = sums(out, "Sum of errors on diagonal tiles")
+    cpu = sums(out, "Sum of CPU errors on solution")
+    gpu = sums(out, "Sum of GPU errors on solution")
+    assert len(inv) == 2 and len(diag) == 2 and len(cpu) == 2 and len(gpu) == 2, out[-3000:]
+    assert max(inv) <= 1e-20 and max(diag) <= 1e-20, (inv, diag)
+    for c, g in zip(cpu, gpu):
+        assert g <= max(100 * c, 1e-26), (cpu, gpu)

@@ -198,3 +198,21 @@ def test_track_batch_beyond_one_wave_matches_smaller_batches():
     d = endpoint_diff(pb, whole.xend, np.concatenate([a.xend, b.xend]), 2)
     scale = np.maximum(1.0, np.abs(whole.endpoints(pb.maxdim)).max(axis=1))
     assert (d[ok] <= 1e-26 * scale[ok]).all()
+
+
+def test_track_curvature_step_binding_vs_oracle():
+    """With a tiny cbeta the curvature step is the smallest step nearly
+    everywhere, so the tracker computes the singular values of the Jacobian
+    and of the Hessians at every step (its bound never settles the minimum):
+    same classification as the oracle, end points within 1e-26, and about
+    as many curvature-step decisions."""
+    pb = hm.subset(hm.config4(), np.arange(0, 1024, 128))
+    ipar, dpar = hm.params(cbeta=1e-16)
+    g = hm.track_host(pb, pmode=1, rmode=2, cbeta=1e-16)
+    xo, io, _ = pyoracle.track(ORC, pb, ipar, dpar, pmode=1, rmode=2, nthreads=8)
+    io = io.reshape(-1, 6)
+    assert np.array_equal(g.status, io[:, 0]) and (g.status == 0).all()
+    assert (endpoint_diff(pb, g.xend, xo, 2) <= 1e-26).all()
+    assert g.nbhess.sum() >= 0.6 * g.steps.sum()
+    assert abs(g.nbhess.sum() - io[:, 4].sum()) <= 0.02 * io[:, 4].sum()
+    assert np.abs(g.steps - io[:, 1]).max() <= 4
