@@ -32,6 +32,19 @@ extern "C" {
 const char *phc_last_error(void);
 int phc_abi_version(void);
 
+/* Launch-shape knobs, process-wide, set by the autotuner
+ * (phcpack_b200/autotune.py); value 0 restores the built-in rule.  No
+ * counterpart in the reference, whose launch shapes are fixed at compile
+ * time or passed per call.
+ *   knob 0: polynomials (warps) per CTA of phc_system_evaldiff, 1..8
+ *           (the rule: min(dim, 8), fewer when the scratch needs it);
+ *   knob 1: variant of the split tracker's kernel, 1 the 64-register one
+ *           (8 paths per SM), 2 the 72-register one (7 paths per SM) (the
+ *           rule: 2 when the batch fits in one wave at 7 per SM).
+ * phc_tune_get returns the value (>= 0) or an error. */
+int phc_tune_set(int knob, int value);
+int phc_tune_get(int knob);
+
 /* Evaluation and differentiation of a batch of nsys polynomial systems of
  * dimension dim at a vector of power series truncated at degree deg.
  *
@@ -105,6 +118,19 @@ int phc_bals_solve(int prec, int cplx, int ninst, int dim, int degp1, int szt, i
                    double *rhs, double *sol, double *Q, double *R, int *flags, double *work, void *stream);
 int phc_bals_solve_host(int prec, int cplx, int ninst, int dim, int degp1, int szt, int tailidx, const double *mat,
                         double *rhs, double *sol, double *Q, double *R, int *flags, void *stream);
+
+/* The residual of the linearised power-series system: for tailidx <= i <
+ * degp1, res_i = rhs_i - sum_{j=0}^{i-tailidx} A_j sol_{i-j} (rows i <
+ * tailidx of res are left as they are), for ninst instances laid out as in
+ * phc_bals_solve; resmax: prec doubles per instance, the per-limb
+ * magnitudes of the entry of res with the largest leading limb (|re| + |im|
+ * for complex numbers), as the reference's resmaxhi, resmaxlo.  Replaces
+ * Newton/dbl2_tail_kernels.h GPU_dbl2_linear_residue (body at
+ * dbl2_tail_kernels.cu:383, host twin dbl2_bals_host.cpp:548) and twins. */
+int phc_linear_residue(int prec, int cplx, int ninst, int dim, int degp1, int tailidx, const double *mat,
+                       const double *rhs, const double *sol, double *res, double *resmax, void *stream);
+int phc_linear_residue_host(int prec, int cplx, int ninst, int dim, int degp1, int tailidx, const double *mat,
+                            const double *rhs, const double *sol, double *res, double *resmax, void *stream);
 
 /* The same QR and least-squares solve with a choice of how the four WY
  * trailing products of each tile (R += Y (W^T C), Q += (Q W^T) Y) run:

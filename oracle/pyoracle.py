@@ -25,21 +25,24 @@ _I = ctypes.POINTER(ctypes.c_int)
 
 
 SHIM_BIN = os.path.join(HERE, "_ref", "test_dbl2_polynomials")
-# the reference's matrix test programs linked with ref_shim_matrices.cu
+# the reference's matrix, Newton and quad double polynomial test programs
+# linked with ref_shim_matrices.cu, ref_shim_newton.cu and ref_shim_polynomials.cu
 SHIM_MATRIX_BINS = {name: os.path.join(HERE, "_ref", name) for name in ("test_dbl2_baqr", "test_dbl4_baqr",
-                                                                        "test_dbl2_tabs")}
+                                                                        "test_dbl2_tabs", "test_dbl2_newton",
+                                                                        "test_dbl4_newton", "test_dbl4_polynomials")}
 
 
 def build(ref: bool = True) -> None:
     """Compile liboracle.so and, where the reference tree exists,
-    _ref/libphcref.so and _ref/test_dbl2_polynomials (the reference's
-    polynomial test program on this library through ref_shim_polynomials.cu;
-    needs phcpack_b200/libphcb200.so built first)."""
+    _ref/libphcref.so and the reference's test programs for polynomials,
+    blocked QR, tiled back substitution and Newton linked with this library
+    through the ref_shim_*.cu files (needs phcpack_b200/libphcb200.so built
+    first)."""
     targets = ["liboracle.so"]
     if ref and REF_TREE and os.path.isdir(REF_TREE):
         targets.append("_ref/libphcref.so")
         if os.path.exists(os.path.join(HERE, "..", "phcpack_b200", "libphcb200.so")):
-            targets += ["_ref/test_dbl2_polynomials", "_ref/test_dbl2_baqr", "_ref/test_dbl4_baqr", "_ref/test_dbl2_tabs"]
+            targets += ["shim"]
     subprocess.run(["make", "-s", "-C", HERE, f"REF={REF_TREE}"] + targets, check=True)
 
 
@@ -100,6 +103,19 @@ class Lib:
         assert rc == 0
         return sol, rhs, Q, R, fl
 
+
+    def linear_residue(self, prec, cplx, dim, degp1, tailidx, mat, rhs, sol, res=None):
+        """Reference library only: CPU_dbl2_linear_residue and its twins."""
+        W = prec * (2 if cplx else 1)
+        mat = np.ascontiguousarray(mat, dtype=np.float64)
+        rhs = np.ascontiguousarray(rhs, dtype=np.float64)
+        sol = np.ascontiguousarray(sol, dtype=np.float64)
+        res = np.zeros(degp1 * dim * W) if res is None else np.array(res, dtype=np.float64, copy=True)
+        mx = np.zeros(prec)
+        rc = self._fn("linear_residue")(prec, int(cplx), dim, degp1, tailidx, _dp(mat), _dp(rhs), _dp(sol), _dp(res),
+                                        _dp(mx))
+        assert rc == 0
+        return res, mx
 
     def od_binop(self, op, a, b):
         """Octo-double add (0), mul (1), div (2) or multiply by a double (3,

@@ -274,6 +274,36 @@ int ref_bals_solve(int prec, int cplx, int dim, int degp1, int tailidx, const do
   return 0;
 }
 
+// The residual of the linearised system by the reference's host code
+// (Newton/dbl2_bals_host.cpp:548 CPU_dbl2_linear_residue and its cmplx2,
+// dbl4, cmplx4 twins): res rows tailidx..degp1-1, resmax prec doubles.
+int ref_linear_residue(int prec, int cplx, int dim, int degp1, int tailidx, const double *mat, const double *rhs,
+                       const double *sol, double *res, double *resmax) {
+  const int C = prec * (cplx ? 2 : 1);
+  Mat3 M(C, degp1, dim, dim);
+  M.in(mat);
+  Mat B(C, degp1, dim), X(C, degp1, dim), Rv(C, degp1, dim);
+  B.in(rhs);
+  X.in(sol);
+  Rv.in(res);
+  double mx[4] = {0.0, 0.0, 0.0, 0.0};
+  if (prec == 2 && !cplx)
+    CPU_dbl2_linear_residue(dim, degp1, tailidx, E2(M.p), E2(B.p), E2(X.p), E2(Rv.p), &mx[0], &mx[1], 0);
+  else if (prec == 2 && cplx)
+    CPU_cmplx2_linear_residue(dim, degp1, tailidx, E4(M.p), E4(B.p), E4(X.p), E4(Rv.p), &mx[0], &mx[1], 0);
+  else if (prec == 4 && !cplx)
+    CPU_dbl4_linear_residue(dim, degp1, tailidx, E4(M.p), E4(B.p), E4(X.p), E4(Rv.p), &mx[0], &mx[1], &mx[2],
+                            &mx[3], 0);
+  else if (prec == 4 && cplx)
+    CPU_cmplx4_linear_residue(dim, degp1, tailidx, E8(M.p), E8(B.p), E8(X.p), E8(Rv.p), &mx[0], &mx[1], &mx[2],
+                              &mx[3], 0);
+  else
+    return -1;
+  Rv.out(res);
+  for (int l = 0; l < prec; ++l) resmax[l] = mx[l];
+  return 0;
+}
+
 // Octo-double arithmetic of the reference (Norms/octo_double_functions.cpp):
 // op 0 add, 1 mul, 2 div, 3 multiply by the double b[0]; n numbers of eight
 // limbs each in a, b, out.

@@ -4,6 +4,9 @@
 //   GPU_dbl2_poly_evaldiff               Polynomials/dbl2_polynomials_kernels.h:812
 //   GPU_cmplx2_poly_evaldiff             Polynomials/dbl2_polynomials_kernels.h:870
 //   GPU_cmplx2vectorized_poly_evaldiff   Polynomials/dbl2_polynomials_kernels.h:960
+// and, compiled with -DSHIM_POLY4, their quad double twins GPU_dbl4_*,
+// GPU_cmplx4_* and GPU_cmplx4vectorized_poly_evaldiff
+// (Polynomials/dbl4_polynomials_kernels.h:1173, :1254, :1397).
 //
 // TEST INFRASTRUCTURE: the recipe of oracle/Makefile (target `shim`) compiles
 // this file against the reference's own header, so that any difference in
@@ -23,7 +26,11 @@
 #include <chrono>
 #include <cstdio>
 #include <vector>
+#if defined(SHIM_POLY4)
+#include "dbl4_polynomials_kernels.h"
+#else
 #include "dbl2_polynomials_kernels.h"
+#endif
 #include "phc_b200.h"
 
 namespace {
@@ -65,32 +72,32 @@ void get(const std::vector<double> &src, size_t at, int n1, int W, double *const
 
 // Evaluate and differentiate; pl[q][l] are the limb arrays of quantity q
 // (constant, coefficients, inputs, outputs) in the order of the limbs.
-void evaldiff(int cplx, int dim, int nbr, int deg, const int *nvr, int *const *idx, double *const *cst,
+void evaldiff(int prec, int cplx, int dim, int nbr, int deg, const int *nvr, int *const *idx, double *const *cst,
               double **const *cff, double **const *input, double **const *output, double *cnvlapms,
               double *addlapms, double *elapsedms, double *walltimesec, const char *name) {
-  const int W = cplx ? 4 : 2, n1 = deg + 1;
+  const int W = prec * (cplx ? 2 : 1), n1 = deg + 1;
   const Supports s = supports(dim, nbr, nvr, idx);
   std::vector<double> c((size_t)dim * n1 * W, 0.0), f((size_t)(nbr > 0 ? nbr : 1) * n1 * W, 0.0);
   std::vector<double> x((size_t)dim * n1 * W), out((size_t)dim * (dim + 1) * n1 * W, 0.0);
   put(c, 0, n1, W, cst);
   for (int m = 0; m < nbr; ++m) {
-    const double *pm[4];
+    const double *pm[8];
     for (int l = 0; l < W; ++l) pm[l] = cff[l][m];
     put(f, (size_t)m * n1 * W, n1, W, pm);
   }
   for (int v = 0; v < dim; ++v) {
-    const double *pv[4];
+    const double *pv[8];
     for (int l = 0; l < W; ++l) pv[l] = input[l][v];
     put(x, (size_t)v * n1 * W, n1, W, pv);
   }
   const auto t0 = std::chrono::steady_clock::now();
-  const int rc = phc_system_evaldiff_host(2, cplx, 1, dim, deg, s.maxvar, s.mon_off.data(), s.nvr.data(),
+  const int rc = phc_system_evaldiff_host(prec, cplx, 1, dim, deg, s.maxvar, s.mon_off.data(), s.nvr.data(),
                                           s.idx.data(), s.exps.data(), c.data(), f.data(), x.data(), out.data(),
                                           nullptr);
   const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   if (rc < 0) std::fprintf(stderr, "%s: %s\n", name, phc_last_error());
   for (int r = 0; r <= dim; ++r) {
-    double *pr[4];
+    double *pr[8];
     for (int l = 0; l < W; ++l) pr[l] = output[l][r];
     get(out, (size_t)r * n1 * W, n1, W, pr);
   }
@@ -102,6 +109,8 @@ void evaldiff(int cplx, int dim, int nbr, int deg, const int *nvr, int *const *i
 
 }  // namespace
 
+#if !defined(SHIM_POLY4)
+
 void GPU_dbl2_poly_evaldiff(int BS, int dim, int nbr, int deg, int *nvr, int **idx, double *csthi, double *cstlo,
                             double **cffhi, double **cfflo, double **inputhi, double **inputlo, double **outputhi,
                             double **outputlo, ConvolutionJobs cnvjobs, AdditionJobs addjobs, double *cnvlapms,
@@ -109,7 +118,7 @@ void GPU_dbl2_poly_evaldiff(int BS, int dim, int nbr, int deg, int *nvr, int **i
   (void)BS; (void)cnvjobs; (void)addjobs; (void)vrblvl;
   double *cst[2] = {csthi, cstlo};
   double **cff[2] = {cffhi, cfflo}, **in[2] = {inputhi, inputlo}, **out[2] = {outputhi, outputlo};
-  evaldiff(0, dim, nbr, deg, nvr, idx, cst, cff, in, out, cnvlapms, addlapms, elapsedms, walltimesec,
+  evaldiff(2, 0, dim, nbr, deg, nvr, idx, cst, cff, in, out, cnvlapms, addlapms, elapsedms, walltimesec,
            "GPU_dbl2_poly_evaldiff");
 }
 
@@ -125,7 +134,7 @@ void GPU_cmplx2_poly_evaldiff(int BS, int dim, int nbr, int deg, int *nvr, int *
   double **cff[4] = {cffrehi, cffrelo, cffimhi, cffimlo};
   double **in[4] = {inputrehi, inputrelo, inputimhi, inputimlo};
   double **out[4] = {outputrehi, outputrelo, outputimhi, outputimlo};
-  evaldiff(1, dim, nbr, deg, nvr, idx, cst, cff, in, out, cnvlapms, addlapms, elapsedms, walltimesec,
+  evaldiff(2, 1, dim, nbr, deg, nvr, idx, cst, cff, in, out, cnvlapms, addlapms, elapsedms, walltimesec,
            "GPU_cmplx2_poly_evaldiff");
 }
 
@@ -142,6 +151,69 @@ void GPU_cmplx2vectorized_poly_evaldiff(int BS, int dim, int nbr, int deg, int *
   double **cff[4] = {cffrehi, cffrelo, cffimhi, cffimlo};
   double **in[4] = {inputrehi, inputrelo, inputimhi, inputimlo};
   double **out[4] = {outputrehi, outputrelo, outputimhi, outputimlo};
-  evaldiff(1, dim, nbr, deg, nvr, idx, cst, cff, in, out, cnvlapms, addlapms, elapsedms, walltimesec,
+  evaldiff(2, 1, dim, nbr, deg, nvr, idx, cst, cff, in, out, cnvlapms, addlapms, elapsedms, walltimesec,
            "GPU_cmplx2vectorized_poly_evaldiff");
 }
+
+#else  // quad double: Polynomials/dbl4_polynomials_kernels.h:1173, :1254, :1397
+
+void GPU_dbl4_poly_evaldiff(int BS, int dim, int nbr, int deg, int *nvr, int **idx, double *csthihi,
+                            double *cstlohi, double *csthilo, double *cstlolo, double **cffhihi, double **cfflohi,
+                            double **cffhilo, double **cfflolo, double **inputhihi, double **inputlohi,
+                            double **inputhilo, double **inputlolo, double **outputhihi, double **outputlohi,
+                            double **outputhilo, double **outputlolo, ConvolutionJobs cnvjobs, AdditionJobs addjobs,
+                            double *cnvlapms, double *addlapms, double *elapsedms, double *walltimesec,
+                            int vrblvl) {
+  (void)BS; (void)cnvjobs; (void)addjobs; (void)vrblvl;
+  double *cst[4] = {csthihi, cstlohi, csthilo, cstlolo};
+  double **cff[4] = {cffhihi, cfflohi, cffhilo, cfflolo};
+  double **in[4] = {inputhihi, inputlohi, inputhilo, inputlolo};
+  double **out[4] = {outputhihi, outputlohi, outputhilo, outputlolo};
+  evaldiff(4, 0, dim, nbr, deg, nvr, idx, cst, cff, in, out, cnvlapms, addlapms, elapsedms, walltimesec,
+           "GPU_dbl4_poly_evaldiff");
+}
+
+void GPU_cmplx4_poly_evaldiff(
+    int BS, int dim, int nbr, int deg, int *nvr, int **idx, double *cstrehihi, double *cstrelohi,
+    double *cstrehilo, double *cstrelolo, double *cstimhihi, double *cstimlohi, double *cstimhilo,
+    double *cstimlolo, double **cffrehihi, double **cffrelohi, double **cffrehilo, double **cffrelolo,
+    double **cffimhihi, double **cffimlohi, double **cffimhilo, double **cffimlolo, double **inputrehihi,
+    double **inputrelohi, double **inputrehilo, double **inputrelolo, double **inputimhihi, double **inputimlohi,
+    double **inputimhilo, double **inputimlolo, double **outputrehihi, double **outputrelohi,
+    double **outputrehilo, double **outputrelolo, double **outputimhihi, double **outputimlohi,
+    double **outputimhilo, double **outputimlolo, ConvolutionJobs cnvjobs, AdditionJobs addjobs, double *cnvlapms,
+    double *addlapms, double *elapsedms, double *walltimesec, int vrblvl) {
+  (void)BS; (void)cnvjobs; (void)addjobs; (void)vrblvl;
+  double *cst[8] = {cstrehihi, cstrelohi, cstrehilo, cstrelolo, cstimhihi, cstimlohi, cstimhilo, cstimlolo};
+  double **cff[8] = {cffrehihi, cffrelohi, cffrehilo, cffrelolo, cffimhihi, cffimlohi, cffimhilo, cffimlolo};
+  double **in[8] = {inputrehihi, inputrelohi, inputrehilo, inputrelolo,
+                    inputimhihi, inputimlohi, inputimhilo, inputimlolo};
+  double **out[8] = {outputrehihi, outputrelohi, outputrehilo, outputrelolo,
+                     outputimhihi, outputimlohi, outputimhilo, outputimlolo};
+  evaldiff(4, 1, dim, nbr, deg, nvr, idx, cst, cff, in, out, cnvlapms, addlapms, elapsedms, walltimesec,
+           "GPU_cmplx4_poly_evaldiff");
+}
+
+void GPU_cmplx4vectorized_poly_evaldiff(
+    int BS, int dim, int nbr, int deg, int *nvr, int **idx, double *cstrehihi, double *cstrelohi,
+    double *cstrehilo, double *cstrelolo, double *cstimhihi, double *cstimlohi, double *cstimhilo,
+    double *cstimlolo, double **cffrehihi, double **cffrelohi, double **cffrehilo, double **cffrelolo,
+    double **cffimhihi, double **cffimlohi, double **cffimhilo, double **cffimlolo, double **inputrehihi,
+    double **inputrelohi, double **inputrehilo, double **inputrelolo, double **inputimhihi, double **inputimlohi,
+    double **inputimhilo, double **inputimlolo, double **outputrehihi, double **outputrelohi,
+    double **outputrehilo, double **outputrelolo, double **outputimhihi, double **outputimlohi,
+    double **outputimhilo, double **outputimlolo, ComplexConvolutionJobs cnvjobs, ComplexIncrementJobs incjobs,
+    ComplexAdditionJobs addjobs, double *cnvlapms, double *addlapms, double *elapsedms, double *walltimesec,
+    int vrblvl) {
+  (void)BS; (void)cnvjobs; (void)incjobs; (void)addjobs; (void)vrblvl;
+  double *cst[8] = {cstrehihi, cstrelohi, cstrehilo, cstrelolo, cstimhihi, cstimlohi, cstimhilo, cstimlolo};
+  double **cff[8] = {cffrehihi, cffrelohi, cffrehilo, cffrelolo, cffimhihi, cffimlohi, cffimhilo, cffimlolo};
+  double **in[8] = {inputrehihi, inputrelohi, inputrehilo, inputrelolo,
+                    inputimhihi, inputimlohi, inputimhilo, inputimlolo};
+  double **out[8] = {outputrehihi, outputrelohi, outputrehilo, outputrelolo,
+                     outputimhihi, outputimlohi, outputimhilo, outputimlolo};
+  evaldiff(4, 1, dim, nbr, deg, nvr, idx, cst, cff, in, out, cnvlapms, addlapms, elapsedms, walltimesec,
+           "GPU_cmplx4vectorized_poly_evaldiff");
+}
+
+#endif

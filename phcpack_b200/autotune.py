@@ -1,0 +1,119 @@
+"""Autotuner of the library's launch shapes, run on the device.
+
+Three choices are swept once per shape and cached for the process:
+
+* the warps (polynomials) per CTA of ``phc_system_evaldiff`` (knob 0 of
+  ``phc_tune_set``), over 1, 2, 4 and 8;
+* the tile size ``szt`` of the blocked QR / least squares
+  (``phc_bals_solve``), over the divisors of the dimension among
+  8, 16, 32 and 64 (a call argument, returned to the caller);
+* the variant of the split tracker's kernel (knob 1), 1 the 64-register
+  kernel at 8 paths per SM, 2 the 72-register kernel at 7 paths per SM.
+
+Every candidate is timed with CUDA events on the caller's stream after one
+untimed run; the fastest is kept (ties to the built-in rule's choice).  The
+knobs change launch shapes only: results are the same for every choice
+(the tests check this).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import _lib
+
+KNOB_EVAL_WARPS = 0
+KNOB_TRACK_VARIANT = 1
+
+_cache: dict = {}
+
+
+def set_knob(knob: int, value: int) -> None:
+    _lib.call("phc_tune_set", int(knob), int(value))
+
+
+def get_knob(knob: int) -> int:
+    return _lib.call("phc_tune_get", int(knob))
+
+
+def _time(torch, stream, fn, reps: int = 3) -> float:
+    """Median CUDA-event seconds of fn() on stream, after one untimed run."""
+    fn()
+    times = []
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1) / 1e3)
+    return float(np.median(times))
+
+
+def tune_eval_warps(torch, stream, args, dim: int, key=None, reps: int = 3) -> dict:
+    """Sweep the warps per CTA of phc_system_evaldiff; args: the argument
+    tuple of the call (device pointers, the stream last).  Sets knob 0 to the
+    fastest and returns {"choice", "seconds": {warps: s}}."""
+    key = ("eval", key if key is not None else dim)
+    if key in _cache:
+        set_knob(KNOB_EVAL_WARPS, _cache[key]["choice"])
+        return _cache[key]
+    cands = [w for w in (1, 2, 4, 8) if w <= max(1, dim)]
+    secs = {}
+    for w in cands:
+        set_knob(KNOB_EVAL_WARPS, w)
+        secs[w] = _time(torch, stream, lambda: _lib.call("phc_system_evaldiff", *args), reps)
+    best = min(cands, key=lambda w: (secs[w], -w))
+    set_knob(KNOB_EVAL_WARPS, best)
+    _cache[key] = {"choice": best, "seconds": secs}
+    return _cache[key]
+
+
+def tune_bals_tile(torch, stream, prec, cplx, ninst, dim, degp1, mat, rhs0, sol, Q, R, flags, flag0, work,
+                   wy: int = 0, reps: int = 3, cands=(8, 16, 32, 64)) -> dict:
+    """Sweep the tile size of phc_bals_solve_wy on resident device buffers
+    (rhs and flags are restored from rhs0 and flag0 before every run; work
+    must hold the workspace of the smallest tile).  Returns {"choice",
+    "seconds"}; the caller passes the choice as szt."""
+    key = ("bals", prec, cplx, ninst, dim, degp1, wy)
+    if key in _cache:
+        return _cache[key]
+    tiles = [t for t in cands if dim % t == 0 and t <= dim]
+    if not tiles:
+        tiles = [dim]
+    rhs = torch.empty_like(rhs0)
+
+    def run(szt):
+        with torch.cuda.stream(stream):
+            rhs.copy_(rhs0)
+            flags.copy_(flag0)
+        _lib.call("phc_bals_solve_wy", prec, int(cplx), ninst, dim, degp1, szt, 1, _lib.ptr(mat), _lib.ptr(rhs),
+                  _lib.ptr(sol), _lib.ptr(Q), _lib.ptr(R), _lib.ptr(flags), _lib.ptr(work), int(wy),
+                  _lib.c_void_p(stream.cuda_stream))
+
+    secs = {t: _time(torch, stream, lambda t=t: run(t), reps) for t in tiles}
+    best = min(tiles, key=lambda t: (secs[t], t))
+    _cache[key] = {"choice": best, "seconds": secs}
+    return _cache[key]
+
+
+def tune_track_variant(torch, stream, tracker, reps: int = 2, **run_kw) -> dict:
+    """Time the two kernels of the split tracker on a DeviceTracker's own
+    batch (tracker.run(**run_kw)) and set knob 1 to the faster."""
+    key = ("track", tracker.pb.npaths, tracker.pb.maxdim, tuple(sorted(run_kw.items())))
+    if key in _cache:
+        set_knob(KNOB_TRACK_VARIANT, _cache[key]["choice"])
+        return _cache[key]
+    secs = {}
+    for v in (1, 2):
+        set_knob(KNOB_TRACK_VARIANT, v)
+        secs[v] = _time(torch, stream, lambda: tracker.run(stream=stream, **run_kw), reps)
+    best = min((1, 2), key=lambda v: secs[v])
+    set_knob(KNOB_TRACK_VARIANT, best)
+    _cache[key] = {"choice": best, "seconds": secs}
+    return _cache[key]
+
+
+def reset() -> None:
+    """Back to the built-in rules; the cache is kept."""
+    set_knob(KNOB_EVAL_WARPS, 0)
+    set_knob(KNOB_TRACK_VARIANT, 0)

@@ -204,8 +204,21 @@ def side_block(name, torch, dev, fp64_tflops, hbm_gbs, steps=3, warm=2):
     4096-system eval/diff; qr: the 512-instance quad-double least squares)
     for the track line: CUDA events around each launch, inputs resident,
     inputs larger than L2, and the workload's roofline."""
+    from . import autotune
     work = make(name, dev, 0)
     stream = torch.cuda.Stream(device=dev)
+    tuned = None
+    if name == "eval":
+        r = autotune.tune_eval_warps(torch, stream, work._args(stream.cuda_stream, work.out), work.d["dim"],
+                                     key="config2")
+        tuned = {"eval_warps_per_cta": r["choice"], "seconds": {str(k): round(v, 6) for k, v in r["seconds"].items()}}
+    elif name == "qr":
+        flag0 = torch.tensor([1, 0, 0, 0, 1], dtype=torch.int32, device=dev).repeat(work.ninst)
+        r = autotune.tune_bals_tile(torch, stream, 4, False, work.ninst, 64, 32, work.mat, work.rhs0, work.sol,
+                                    work.Q, work.R, work.flags, flag0, work.work, wy=work.wy, reps=1,
+                                    cands=tuple(work.tiles))
+        work.szt = r["choice"]
+        tuned = {"szt": r["choice"], "seconds": {str(k): round(v, 6) for k, v in r["seconds"].items()}}
     for _ in range(warm):
         work.step(stream)
     torch.cuda.synchronize()
@@ -219,8 +232,11 @@ def side_block(name, torch, dev, fp64_tflops, hbm_gbs, steps=3, warm=2):
         times.append(e0.elapsed_time(e1) / 1e3)
     t = float(np.mean(times))
     achieved = work.dominant_flops_per_launch / t / 1e12
+    config = dict(work.config)
+    if tuned is not None:
+        config["autotuned"] = tuned
     out = {"metric": work.metric, "value": work.units_per_step / t, "unit": work.unit, "steps": steps,
-           "ms_per_step": t * 1e3, "config": work.config,
+           "ms_per_step": t * 1e3, "config": config,
            "roofline": {"bound": "fp64", "achieved": achieved, "peak": fp64_tflops, "unit": "TFLOP/s",
                         "frac": achieved / fp64_tflops, "flops_convention": work.flops_note,
                         "traffic": getattr(work, "traffic_bytes_per_launch", None),
@@ -230,6 +246,7 @@ def side_block(name, torch, dev, fp64_tflops, hbm_gbs, steps=3, warm=2):
     except Exception as e:
         out["check"] = {"error": str(e)[:200]}
     del work
+    autotune.reset()
     torch.cuda.synchronize()
     torch.cuda.empty_cache()
     return out

@@ -8,6 +8,7 @@
 #include <cstring>
 #include <string>
 #include <mutex>
+#include <atomic>
 #include "common.cuh"
 #include "../../include/phc_b200.h"
 
@@ -34,6 +35,9 @@ int upper_tiled_solver(int prec, int cplx, int ninst, int dim, int szt, double *
                        cudaStream_t st);
 int bals_solve(int prec, int cplx, int ninst, int n, int degp1, int szt, int tailidx, const double *mat, double *rhs,
                double *sol, double *Q, double *R, int *flags, double *work, cudaStream_t st);
+
+int linear_residue(int prec, int cplx, int ninst, int n, int degp1, int tailidx, const double *mat, const double *rhs,
+                   const double *sol, double *res, double *resmax, cudaStream_t st);
 
 long newton_work_doubles(int prec, int cplx, int nsys, int dim, int deg, int maxdeg, int szt, long nmon);
 int newton_step(int prec, int cplx, int nsys, int dim, int deg, int maxdeg, int szt, int maxvar, const int *mon_off,
@@ -95,6 +99,10 @@ struct dbuf {
   }
 };
 
+static std::atomic<int> g_tune[kTuneKnobs];
+
+int tune_get(int knob) { return (knob >= 0 && knob < kTuneKnobs) ? g_tune[knob].load() : 0; }
+
 }  // namespace phc
 
 using namespace phc;
@@ -102,6 +110,20 @@ using namespace phc;
 extern "C" {
 
 const char *phc_last_error(void) { return get_error(); }
+
+int phc_tune_set(int knob, int value) {
+  PHC_REQUIRE(knob >= 0 && knob < kTuneKnobs, "tune_set: knob %d not in 0..%d", knob, kTuneKnobs - 1);
+  PHC_REQUIRE(value >= 0, "tune_set: value %d < 0", value);
+  if (knob == kTuneEvalWarps) PHC_REQUIRE(value <= 8, "tune_set: warps per CTA %d > 8", value);
+  if (knob == kTuneTrackVariant) PHC_REQUIRE(value <= 2, "tune_set: tracker variant %d not in 0..2", value);
+  g_tune[knob].store(value);
+  return PHC_OK;
+}
+
+int phc_tune_get(int knob) {
+  PHC_REQUIRE(knob >= 0 && knob < kTuneKnobs, "tune_get: knob %d not in 0..%d", knob, kTuneKnobs - 1);
+  return g_tune[knob].load();
+}
 
 int phc_abi_version(void) { return PHC_ABI_VERSION; }
 
@@ -292,6 +314,38 @@ int phc_bals_solve_host(int prec, int cplx, int ninst, int dim, int degp1, int s
   PHC_CUDA(cudaMemcpyAsync(Q, dQ, nq * 8, cudaMemcpyDeviceToHost, st));
   PHC_CUDA(cudaMemcpyAsync(R, dR, nq * 8, cudaMemcpyDeviceToHost, st));
   PHC_CUDA(cudaMemcpyAsync(flags, df, nf * 4, cudaMemcpyDeviceToHost, st));
+  PHC_CUDA(cudaStreamSynchronize(st));
+  return PHC_OK;
+}
+
+int phc_linear_residue(int prec, int cplx, int ninst, int dim, int degp1, int tailidx, const double *mat,
+                       const double *rhs, const double *sol, double *res, double *resmax, void *stream) {
+  return linear_residue(prec, cplx, ninst, dim, degp1, tailidx, mat, rhs, sol, res, resmax, (cudaStream_t)stream);
+}
+
+int phc_linear_residue_host(int prec, int cplx, int ninst, int dim, int degp1, int tailidx, const double *mat,
+                            const double *rhs, const double *sol, double *res, double *resmax, void *stream) {
+  PHC_REQUIRE(prec_ok(prec) && ninst >= 0 && dim >= 1 && degp1 >= 1 && tailidx >= 0 && tailidx <= degp1,
+              "linear_residue_host: bad sizes");
+  if (ninst == 0) return PHC_OK;
+  PHC_REQUIRE(mat && rhs && sol && res && resmax, "linear_residue_host: null pointer");
+  const size_t W = width_of(prec, cplx);
+  const size_t nm = (size_t)ninst * degp1 * dim * dim * W, nb = (size_t)ninst * degp1 * dim * W;
+  const size_t nr = (size_t)ninst * prec;
+  staged s;
+  int rc = s.alloc(al(nm * 8) + 3 * al(nb * 8) + al(nr * 8));
+  if (rc) return rc;
+  double *dm = s.take<double>(nm), *db = s.take<double>(nb), *dx = s.take<double>(nb), *dr = s.take<double>(nb);
+  double *dmax = s.take<double>(nr);
+  cudaStream_t st = (cudaStream_t)stream;
+  PHC_CUDA(cudaMemcpyAsync(dm, mat, nm * 8, cudaMemcpyHostToDevice, st));
+  PHC_CUDA(cudaMemcpyAsync(db, rhs, nb * 8, cudaMemcpyHostToDevice, st));
+  PHC_CUDA(cudaMemcpyAsync(dx, sol, nb * 8, cudaMemcpyHostToDevice, st));
+  PHC_CUDA(cudaMemcpyAsync(dr, res, nb * 8, cudaMemcpyHostToDevice, st));  // rows below tailidx stay as they are
+  rc = linear_residue(prec, cplx, ninst, dim, degp1, tailidx, dm, db, dx, dr, dmax, st);
+  if (rc) return rc;
+  PHC_CUDA(cudaMemcpyAsync(res, dr, nb * 8, cudaMemcpyDeviceToHost, st));
+  PHC_CUDA(cudaMemcpyAsync(resmax, dmax, nr * 8, cudaMemcpyDeviceToHost, st));
   PHC_CUDA(cudaStreamSynchronize(st));
   return PHC_OK;
 }

@@ -158,6 +158,95 @@ static int qr_launch(int ninst, int n, int ncols, int szt, const double *A, doub
   return PHC_OK;
 }
 
+// The residual of the linearised power-series system, one instance per CTA
+// and one thread per entry (i, L), tailidx <= i < degp1:
+//   res_i[L] = rhs_i[L] - sum_{j=0}^{i-tailidx} sum_k A_j[L][k] sol_{i-j}[k],
+// in the order of Newton/dbl2_bals_host.cpp:548-600 (CPU_dbl2_linear_residue;
+// complex numbers :602-680: re -= Are xre, re += Aim xim, im -= Are xim,
+// im -= Aim xre, each product rounded before it is added).  resmax: prec
+// doubles per instance, the magnitudes of the limbs of the first entry (in
+// the order of i, then L) with the largest |leading limb| (|re| + |im| for
+// complex numbers, limb by limb), zero when every entry is zero.
+template <class N>
+__device__ __forceinline__ void residue_dec(typename N::T &r, const typename N::T &a, const typename N::T &x) {
+  if constexpr (N::is_complex) {
+    typedef typename N::tr tr;
+    r.re = tr::sub(r.re, tr::mul(a.re, x.re));
+    r.re = tr::add(r.re, tr::mul(a.im, x.im));
+    r.im = tr::sub(r.im, tr::mul(a.re, x.im));
+    r.im = tr::sub(r.im, tr::mul(a.im, x.re));
+  } else {
+    r = N::sub(r, N::mul(a, x));
+  }
+}
+
+template <class N>
+__global__ void __launch_bounds__(kDenseThreads)
+    k_linear_residue(int n, int degp1, int tailidx, const double *__restrict__ mat, const double *__restrict__ rhs,
+                     const double *__restrict__ sol, double *__restrict__ res, double *__restrict__ resmax) {
+  typedef typename N::T T;
+  const int W = N::width;
+  const int limbs = N::tr::limbs;
+  const long inst = blockIdx.x;
+  const double *A = mat + inst * (long)degp1 * n * n * W;
+  const double *b = rhs + inst * (long)degp1 * n * W;
+  const double *x = sol + inst * (long)degp1 * n * W;
+  double *r = res + inst * (long)degp1 * n * W;
+  const int cnt = (degp1 - tailidx) * n;
+  double best = 0.0;
+  int bidx = -1;
+  for (int e = threadIdx.x; e < cnt; e += blockDim.x) {
+    const int i = tailidx + e / n, L = e % n;
+    T acc = ldn_at<N>(b, (long)i * n + L);
+    for (int j = 0; j <= i - tailidx; ++j) {
+      const double *Aj = A + (long)j * n * n * W;
+      const double *xj = x + (long)(i - j) * n * W;
+      for (int k = 0; k < n; ++k) residue_dec<N>(acc, ldn_at<N>(Aj, (long)L * n + k), ldn_at<N>(xj, k));
+    }
+    stn_at<N>(r, (long)i * n + L, acc);
+    const double v = N::lead(acc);
+    if (v > best) {  // a NaN is never taken, as in the reference
+      best = v;
+      bidx = e;
+    }
+  }
+  __shared__ double sv[kDenseThreads];
+  __shared__ int si[kDenseThreads];
+  sv[threadIdx.x] = best;
+  si[threadIdx.x] = bidx;
+  __syncthreads();
+  for (int o = kDenseThreads / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) {
+      const double v2 = sv[threadIdx.x + o];
+      const int i2 = si[threadIdx.x + o];
+      const double v1 = sv[threadIdx.x];
+      const int i1 = si[threadIdx.x];
+      if (i2 >= 0 && (i1 < 0 || v2 > v1 || (v2 == v1 && i2 < i1))) {
+        sv[threadIdx.x] = v2;
+        si[threadIdx.x] = i2;
+      }
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x < limbs) {
+    const int l = threadIdx.x, e = si[0];
+    double m = 0.0;
+    if (e >= 0) {
+      const double *p = r + ((long)(tailidx + e / n) * n + e % n) * W;
+      m = N::is_complex ? fabs(p[l]) + fabs(p[limbs + l]) : fabs(p[l]);
+    }
+    resmax[inst * limbs + l] = m;
+  }
+}
+
+template <class N>
+static int residue_launch(int ninst, int n, int degp1, int tailidx, const double *mat, const double *rhs,
+                          const double *sol, double *res, double *resmax, cudaStream_t st) {
+  k_linear_residue<N><<<ninst, kDenseThreads, 0, st>>>(n, degp1, tailidx, mat, rhs, sol, res, resmax);
+  PHC_CHECK_LAUNCH();
+  return PHC_OK;
+}
+
 template <class N>
 static int tabs_launch(int ninst, int dim, int szt, double *U, double *b, double *x, double *work, cudaStream_t st) {
   k_upper_tiled_solver<N><<<ninst, kDenseThreads, 0, st>>>(dim, szt, U, b, x, work);
@@ -240,6 +329,16 @@ int bals_solve_wy(int prec, int cplx, int ninst, int n, int degp1, int szt, int 
   if (ninst == 0) return PHC_OK;
   PHC_DISPATCH(prec, cplx,
                bals_launch<N>(ninst, n, degp1, szt, tailidx, mat, rhs, sol, Q, R, flags, work, st, wy != 0 && !cplx));
+}
+
+int linear_residue(int prec, int cplx, int ninst, int n, int degp1, int tailidx, const double *mat, const double *rhs,
+                   const double *sol, double *res, double *resmax, cudaStream_t st) {
+  PHC_REQUIRE(prec_ok(prec), "linear_residue: precision %d", prec);
+  PHC_REQUIRE(n >= 1 && degp1 >= 1 && tailidx >= 0 && tailidx <= degp1,
+              "linear_residue: need dim >= 1, degp1 >= 1, 0 <= tailidx <= degp1");
+  if (ninst == 0) return PHC_OK;
+  PHC_REQUIRE(mat && rhs && sol && res && resmax, "linear_residue: null pointer");
+  PHC_DISPATCH(prec, cplx, residue_launch<N>(ninst, n, degp1, tailidx, mat, rhs, sol, res, resmax, st));
 }
 
 }  // namespace phc

@@ -66,6 +66,8 @@ static int launch_system(int nsys, int dim, int deg, int maxvar, const int *mon_
   const long per_warp = (long)warp_slots(maxvar) * S * sizeof(double);
   const long xs = (long)((dim * S + 1) & ~1) * sizeof(double);
   int wpb = dim < kMaxWarpsPerBlock ? dim : kMaxWarpsPerBlock;
+  const int tuned = tune_get(kTuneEvalWarps);  // warps per CTA chosen by the autotuner
+  if (tuned > 0) wpb = tuned < dim ? tuned : dim;
   while (wpb > 1 && (long)wpb * per_warp > kMaxSmem) --wpb;
   const long scr = (long)wpb * per_warp;
   int stage = (scr + xs) <= 200 * 1024;

@@ -80,24 +80,34 @@ struct wser {
     __syncwarp();  // z may alias a buffer other lanes still read
     put(z, r, m);
   }
-  // row[k] += e*z in global memory (lane-owned coefficient)
-  static __device__ __forceinline__ void acc_global(double *row, const T &z, const lanemap &m, int e) {
+  // row[k] += e*z in global memory (lane-owned coefficient); the first
+  // contribution to a row (first == true) is stored without reading it
+  static __device__ __forceinline__ void acc_global(double *row, const T &z, const lanemap &m, int e, bool first) {
     if (m.valid) {
-      T v;
-      md::ldn(row + m.kout() * W, v);
       const T zz = (e > 1) ? N::scale_d(z, (double)e) : z;
-      md::stn(row + m.kout() * W, N::add(v, zz));
+      if (first) {
+        md::stn(row + m.kout() * W, zz);
+      } else {
+        T v;
+        md::ldn(row + m.kout() * W, v);
+        md::stn(row + m.kout() * W, N::add(v, zz));
+      }
     }
   }
   // row[k] += e*src[k] for a series src in shared memory, lane k
-  static __device__ __forceinline__ void acc_series(double *row, const double *src, int n1, int e) {
+  static __device__ __forceinline__ void acc_series(double *row, const double *src, int n1, int e, bool first) {
     const int lane = threadIdx.x & 31;
     if (lane < n1) {
-      T v, z;
-      md::ldn(row + lane * W, v);
+      T z;
       md::ldn(src + lane * W, z);
       if (e > 1) z = N::scale_d(z, (double)e);
-      md::stn(row + lane * W, N::add(v, z));
+      if (first) {
+        md::stn(row + lane * W, z);
+      } else {
+        T v;
+        md::ldn(row + lane * W, v);
+        md::stn(row + lane * W, N::add(v, z));
+      }
     }
   }
 };
@@ -110,7 +120,12 @@ __host__ __device__ inline int warp_slots(int maxvar) {
 }
 
 // Value and gradient of one polynomial of a system, accumulated by one warp
-// into out (dim+1 series in global memory; row dim is the value).
+// into out (dim+1 series in global memory; row dim is the value).  The
+// value is accumulated in registers (each lane its coefficients) and
+// written once.  A gradient row is stored at its first contribution and
+// read, added to and written back only after that (a 64-bit mask records
+// the rows 0..63 written so far; rows from 64 on are zeroed first and
+// always accumulated); rows no monomial reached are zeroed at the end.
 //
 // Per monomial: the common-factor method of Newton/dbl2_systems_host.cpp:
 // 18-110 (coefficient <- x^(e-1) * coefficient, derivative j scaled by e_j),
@@ -131,19 +146,23 @@ __device__ void warp_poly_evaldiff(int dim, int deg, int maxvar, int m0, int m1,
   const lanemap m(deg, lane);
   typedef wser<N> ws;
 
-  // rows 0..dim-1 start at zero, row dim at the constant series
-  for (int r = 0; r <= dim; ++r) {
-    if (lane < n1) {
-      T v = N::zero();
-      if (r == dim) md::ldn(cst + lane * W, v);
-      md::stn(out + r * S + lane * W, v);
-    }
-  }
+  // rows past the first 64 start at zero (the mask covers rows 0..63)
+  for (int r = 64; r < dim; ++r)
+    if (lane < n1) md::stn(out + r * S + lane * W, N::zero());
+  unsigned long long written = 0ull;  // gradient rows stored so far (uniform over the warp)
+  auto first_touch = [&](int r) {
+    if (r >= 64) return false;
+    const bool f = !((written >> r) & 1ull);
+    written |= 1ull << r;
+    return f;
+  };
+  // the value starts at the constant series, lane-owned coefficients
+  T vacc = N::zero();
+  if (m.valid) md::ldn(cst + m.kout() * W, vacc);
   double *C = scr;
   double *Tm = scr + S;
   double *F = scr + 2 * S;                 // f_0 .. f_{k-2}
   double *B = scr + (1 + maxvar) * S;      // b_0 .. b_{k-3}
-  double *val = out + dim * S;
 
   for (int mon = m0; mon < m1; ++mon) {
     const int k = nvr[mon];
@@ -171,23 +190,23 @@ __device__ void warp_poly_evaldiff(int dim, int deg, int maxvar, int m0, int m1,
     }
     if (k == 1) {
       const T z = ws::conv(X + ix[0] * S, C, m);
-      ws::acc_global(val, z, m, 1);
-      ws::acc_series(out + ix[0] * S, C, n1, ex[0]);
+      if (m.valid) vacc = N::add(vacc, z);
+      ws::acc_series(out + ix[0] * S, C, n1, ex[0], first_touch(ix[0]));
     } else if (k == 2) {
       ws::prod(X + ix[0] * S, X + ix[1] * S, Tm, m);
       T z = ws::conv(Tm, C, m);
-      ws::acc_global(val, z, m, 1);
+      if (m.valid) vacc = N::add(vacc, z);
       z = ws::conv(C, X + ix[0] * S, m);
-      ws::acc_global(out + ix[1] * S, z, m, ex[1]);
+      ws::acc_global(out + ix[1] * S, z, m, ex[1], first_touch(ix[1]));
       z = ws::conv(C, X + ix[1] * S, m);
-      ws::acc_global(out + ix[0] * S, z, m, ex[0]);
+      ws::acc_global(out + ix[0] * S, z, m, ex[0], first_touch(ix[0]));
     } else {
       // forward products f_i = f_{i-1} x_i, f_0 = c x_0
       ws::prod(C, X + ix[0] * S, F, m);
       for (int i = 1; i < k - 1; ++i) ws::prod(F + (i - 1) * S, X + ix[i] * S, F + i * S, m);
       T z = ws::conv(F + (k - 2) * S, X + ix[k - 1] * S, m);
-      ws::acc_global(val, z, m, 1);
-      ws::acc_series(out + ix[k - 1] * S, F + (k - 2) * S, n1, ex[k - 1]);
+      if (m.valid) vacc = N::add(vacc, z);
+      ws::acc_series(out + ix[k - 1] * S, F + (k - 2) * S, n1, ex[k - 1], first_touch(ix[k - 1]));
       // backward products b_0 = x_{k-1} x_{k-2}, b_i = b_{i-1} x_{k-2-i}
       ws::prod(X + ix[k - 1] * S, X + ix[k - 2] * S, B, m);
       for (int i = 1; i < k - 2; ++i) ws::prod(B + (i - 1) * S, X + ix[k - 2 - i] * S, B + i * S, m);
@@ -195,22 +214,26 @@ __device__ void warp_poly_evaldiff(int dim, int deg, int maxvar, int m0, int m1,
       z = ws::conv(B + (k - 3) * S, C, m);
       __syncwarp();
       ws::put(B + (k - 3) * S, z, m);
-      ws::acc_series(out + ix[0] * S, B + (k - 3) * S, n1, ex[0]);
+      ws::acc_series(out + ix[0] * S, B + (k - 3) * S, n1, ex[0], first_touch(ix[0]));
       // cross products: derivative in x_j, 1 <= j <= k-2
       if (k == 3) {
         z = ws::conv(F, X + ix[2] * S, m);
-        ws::acc_global(out + ix[1] * S, z, m, ex[1]);
+        ws::acc_global(out + ix[1] * S, z, m, ex[1], first_touch(ix[1]));
       } else {
         for (int i = 0; i < k - 3; ++i) {
           z = ws::conv(F + i * S, B + (k - 4 - i) * S, m);
-          ws::acc_global(out + ix[i + 1] * S, z, m, ex[i + 1]);
+          ws::acc_global(out + ix[i + 1] * S, z, m, ex[i + 1], first_touch(ix[i + 1]));
         }
         z = ws::conv(F + (k - 3) * S, X + ix[k - 1] * S, m);
-        ws::acc_global(out + ix[k - 2] * S, z, m, ex[k - 2]);
+        ws::acc_global(out + ix[k - 2] * S, z, m, ex[k - 2], first_touch(ix[k - 2]));
       }
     }
     __syncwarp();
   }
+  // the value, and zeros in the rows no monomial reached
+  if (m.valid) md::stn(out + dim * S + m.kout() * W, vacc);
+  for (int r = 0; r < dim && r < 64; ++r)
+    if (!((written >> r) & 1ull) && lane < n1) md::stn(out + r * S + lane * W, N::zero());
 }
 
 }  // namespace phc

@@ -804,7 +804,7 @@ __device__ void cta_matvec(int n, const double *M, const double *b, double *y) {
 // Shared-memory layout of a path's CTA (in doubles)
 struct TrackLayout {
   long xs, V, G, hs, J0, M, r, num, den, xp, xc, hc, Jc, Vc, Gc, red, piv, dinv, feat, mag, degs, hbuf, svd, xd, sv,
-      total;
+      part, total;
 };
 
 // Matrices of the singular-value jobs of a predictor step: one per warp
@@ -853,6 +853,9 @@ __host__ __device__ inline TrackLayout track_layout(int n, int K, int M, int nm,
   L.Jc = take(n * n * Wr);
   L.Vc = take(nm * Wr);
   L.Gc = take(gst ? nm * mv * Wr : 0);
+  // partial residuals of the split corrector (double predictor, no staged
+  // partials): one complex double-double per residual thread
+  L.part = take(Wp == 2 && !gst ? (kTrackThreads - 32) * 4 : 0);
   L.total = o > pend ? o : pend;
   return L;
 }
@@ -888,6 +891,189 @@ __device__ TRACK_FN bool point_newton(const TrackDev &S, int s, int n, double t,
         m = JN::mag(v);
         if (!(m == m)) m = INFINITY;
         if (info == 0) stn_at<N>(x, lane, N::add(ldn_at<N>(x, lane), conv_num<JN, N>::go(v)));
+      }
+      m = warp_max(m);
+      if (lane == 0) red[0] = info ? INFINITY : m;
+    }
+    __syncthreads();
+    const double m = red[0];
+    __syncthreads();
+    *lastdx = m;
+    if (!(m <= 1e300)) return false;
+    if (conv) {
+      if (--extra_left <= 0) break;
+    } else if (m <= tol) {
+      conv = true;
+      if (extra_left <= 0) break;
+    }
+  }
+  return conv;
+}
+
+// Compensated sum (Sum2 of Ogita, Rump and Oishi, 2005) of products of a
+// double and a double-double: two error-free transformations per product,
+// the rounding errors gathered in e; s + e carries about double-double
+// accuracy.
+struct sum2 {
+  double s, e;
+  __device__ __forceinline__ void zero() {
+    s = 0.0;
+    e = 0.0;
+  }
+  __device__ __forceinline__ void add_prod(double a, const md::dd &v) {
+    double ep, es;
+    const double p = md::two_prod(a, v.hi, ep);
+    s = md::two_sum(s, p, es);
+    e = __fma_rn(a, v.lo, md::add(e, md::add(es, ep)));
+  }
+  __device__ __forceinline__ md::dd value() const {
+    md::dd r;
+    r.hi = md::two_sum(s, e, r.lo);
+    return r;
+  }
+};
+
+// Barrier of the three residual warps of the split corrector (named
+// barrier 1; the lead warp does not take part).
+__device__ __forceinline__ void residual_warps_sync() {
+  asm volatile("bar.sync 1, %0;" ::"r"(kTrackThreads - 32) : "memory");
+}
+
+// First of the G residual threads that work on equation i when the n
+// equations (ci terms before equation i, T terms in all) share them in
+// proportion to their terms, each at least one: strictly increasing in i,
+// from 0 at i = 0 to G at i = n.
+__device__ __forceinline__ int eq_first_thread(int i, int n, int G, int ci, int T) {
+  return i + (T > 0 ? (int)((long long)(G - n) * ci / T) : 0);
+}
+
+// The corrector's Newton steps with a double Jacobian (the precision-split
+// tracker, for systems that stage no partials): the same steps, tests and
+// results as point_newton<N, double> (Curves/corrector_convolutions.adb
+// :1193-1224, LU_Newton_Steps), with the work of an iteration split over
+// the CTA.  The lead warp evaluates J(x) in complex double from the
+// Jacobian gather lists at the double copy xj of x (lanes over the n^2
+// entries) and factors it, while the other three warps evaluate h(x, t) in
+// double-double: the terms of each equation go to a group of threads (in
+// proportion to the terms, eq_first_thread), each thread forms the values
+// x^e of its terms in double-double and accumulates P = sum b x^e and Q =
+// sum a x^e with compensated sums, its share of h is Q + t (P - Q), and the
+// first thread of the group adds the shares in order.  Then the lead warp
+// solves, updates x (n numbers of N, double-double, in shared memory) and
+// xj.  part: (kTrackThreads - 32) complex double-doubles.
+template <class N>
+__device__ TRACK_FN bool point_newton_split(const TrackDev &S, int s, int n, double t, double *x, double *h,
+                                            double *Jm, double2 *xj, double *part, int *piv, double *dinv,
+                                            double *red, int maxit, double tol, int extra, double *lastdx) {
+  typedef md::num<double, true> JN;
+  typedef typename N::T T;
+  const int G = kTrackThreads - 32;
+  const int e0 = S.eq_off[s];
+  const int tb0 = S.term_off[e0], nterm = S.term_off[e0 + n] - tb0;
+  // residual thread ri: equation req, position rk in a group of rg threads
+  const int ri = ctid() - 32;
+  int req = 0, rk = 0, rg = 1;
+  if (ri >= 0) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (eq_first_thread(mid, n, G, S.term_off[e0 + mid] - tb0, nterm) <= ri) lo = mid;
+      else hi = mid - 1;
+    }
+    req = lo;
+    const int f0 = eq_first_thread(lo, n, G, S.term_off[e0 + lo] - tb0, nterm);
+    const int f1 = lo + 1 < n ? eq_first_thread(lo + 1, n, G, S.term_off[e0 + lo + 1] - tb0, nterm) : G;
+    rk = ri - f0;
+    rg = f1 - f0;
+  }
+  auto to_d2 = [](const T &v) {
+    return make_double2(__dadd_rn(v.re.hi, v.re.lo), __dadd_rn(v.im.hi, v.im.lo));
+  };
+  if (ctid() < n) xj[ctid()] = to_d2(ldn_at<N>(x, ctid()));
+  __syncwarp();
+  bool conv = false;
+  int extra_left = extra;
+  int info = 0;
+  *lastdx = 1e300;
+  for (int it = 0; it < maxit + extra; ++it) {
+    if (it >= maxit && !conv) break;
+    if (ctid() < 32) {
+      const int lane = ctid();
+      for (int e = lane; e < n * n; e += 32) {
+        const int i = e / n, j = e % n;
+        const int g = (e0 + i) * S.maxdim + j;
+        double2 acc = make_double2(0.0, 0.0);
+        for (int q = S.jg_off[g]; q < S.jg_off[g + 1]; ++q) {
+          const int tr = S.jg_term[q], sl = S.jg_slot[q];
+          const double ar = S.term_a[2 * tr], ai = S.term_a[2 * tr + 1];
+          const double2 c = make_double2(fma(S.term_b[2 * tr] - ar, t, ar), fma(S.term_b[2 * tr + 1] - ai, t, ai));
+          double2 v;
+          if (sl == -1) v = make_double2(1.0, 0.0);
+          else if (sl == -2) v = make_double2(2.0 * xj[j].x, 2.0 * xj[j].y);
+          else v = xj[-sl - 3];
+          acc.x = fma(c.x, v.x, fma(-c.y, v.y, acc.x));
+          acc.y = fma(c.x, v.y, fma(c.y, v.x, acc.y));
+        }
+        reinterpret_cast<double2 *>(Jm)[e] = acc;
+      }
+      __syncwarp();
+      info = warp_lufac<JN>(n, Jm, piv, dinv);
+    } else {
+      sum2 pr, pi, qr, qi;
+      pr.zero(); pi.zero(); qr.zero(); qi.zero();
+      for (int tr = S.term_off[e0 + req] + rk; tr < S.term_off[e0 + req + 1]; tr += rg) {
+        const int gm = S.term_mono[tr];
+        const int nv = S.mono_nvr[gm];
+        const int *ix = S.mono_idx + (long)gm * S.maxvar;
+        const int *ex = S.mono_exp + (long)gm * S.maxvar;
+        T v = N::one();
+        bool unit = true;
+        for (int u = 0; u < nv; ++u) {
+          const T xu = ldn_at<N>(x, ix[u]);
+          for (int q = 0; q < ex[u]; ++q) {
+            v = unit ? xu : N::mul(v, xu);
+            unit = false;
+          }
+        }
+        const double ar = S.term_a[2 * tr], ai = S.term_a[2 * tr + 1];
+        const double br = S.term_b[2 * tr], bi = S.term_b[2 * tr + 1];
+        pr.add_prod(br, v.re);
+        pr.add_prod(-bi, v.im);
+        pi.add_prod(br, v.im);
+        pi.add_prod(bi, v.re);
+        qr.add_prod(ar, v.re);
+        qr.add_prod(-ai, v.im);
+        qi.add_prod(ar, v.im);
+        qi.add_prod(ai, v.re);
+      }
+      T P, Q;
+      P.re = pr.value();
+      P.im = pi.value();
+      Q.re = qr.value();
+      Q.im = qi.value();
+      stn_at<N>(part, ri, N::add(Q, N::scale_d(N::sub(P, Q), t)));
+      residual_warps_sync();
+      if (rk == 0) {
+        T acc = ldn_at<N>(part, ri);
+        for (int k = 1; k < rg; ++k) acc = N::add(acc, ldn_at<N>(part, ri + k));
+        stn_at<N>(h, req, acc);
+      }
+    }
+    __syncthreads();
+    if (ctid() < 32) {
+      const int lane = ctid();
+      typename JN::T b = JN::zero();
+      if (lane < n) b = JN::neg(conv_num<N, JN>::go(ldn_at<N>(h, lane)));
+      const typename JN::T v = warp_lusolve<JN>(n, Jm, piv, dinv, b);
+      double m = 0.0;
+      if (lane < n) {
+        m = JN::mag(v);
+        if (!(m == m)) m = INFINITY;
+        if (info == 0) {
+          const T xn = N::add(ldn_at<N>(x, lane), conv_num<JN, N>::go(v));
+          stn_at<N>(x, lane, xn);
+          xj[lane] = to_d2(xn);
+        }
       }
       m = warp_max(m);
       if (lane == 0) red[0] = info ? INFINITY : m;

@@ -104,6 +104,22 @@ __device__ TRACK_FN double pade_mixres(const TrackDev &S, int s, int n, int K, i
   return block_sum<md::num<double, false> >(part, red) / n;
 }
 
+// The corrector's Newton steps at t (x: n numbers of CN in shared memory):
+// the split form of point_newton_split when the predictor is in double and
+// the system stages no partials, point_newton otherwise.
+template <class CN, class PN>
+__device__ TRACK_FN bool corrector_newton(const TrackDev &S, int s, int n, double t, double *x, double *sm,
+                                          const TrackLayout &L, int *piv, double *dinv, double *red, int maxit,
+                                          double tol, int extra, double *lastdx) {
+  if constexpr (PN::width == 2 && CN::width == 4) {
+    if (!S.gstaged)
+      return point_newton_split<CN>(S, s, n, t, x, sm + L.hc, sm + L.Jc, reinterpret_cast<double2 *>(sm + L.xd),
+                                    sm + L.part, piv, dinv, red, maxit, tol, extra, lastdx);
+  }
+  return point_newton<CN, PN>(S, s, n, t, x, sm + L.hc, sm + L.Jc, sm + L.Vc, sm + L.Gc, piv, dinv, red, maxit, tol,
+                              extra, lastdx);
+}
+
 // Track the paths of one CTA.  PN: predictor numbers, CN: corrector
 // (double-double), RN: refinement.  Output per path: xend (maxdim complex
 // quad-doubles), info (status, steps, rejected), dinfo (t, residual).
@@ -161,8 +177,7 @@ __global__ void __launch_bounds__(kTrackThreads, (track_min_blocks<PN, RN, WIDE>
     }
     __syncthreads();
     double t = 0.0, dxn;
-    point_newton<CN, PN>(S, s, n, 0.0, xc, sm + L.hc, sm + L.Jc, sm + L.Vc, sm + L.Gc, piv, dinv, red, P.corsteps,
-                     P.tolres, 1, &dxn);
+    corrector_newton<CN, PN>(S, s, n, 0.0, xc, sm, L, piv, dinv, red, P.corsteps, P.tolres, 1, &dxn);
     int status = 2, nsteps = 0, nrej = 0, nbpole = 0, nbhess = 0, nbmaxm = 0;
     bool failed = false;
     for (int step_it = 0; step_it < P.maxsteps; ++step_it) {
@@ -364,8 +379,8 @@ __global__ void __launch_bounds__(kTrackThreads, (track_min_blocks<PN, RN, WIDE>
           for (int i = ctid(); i < n; i += blockDim.x)
             stn_at<CN>(xc, i, conv_num<PN, CN>::go(ldn_at<PN>(xp, i)));
           __syncthreads();
-          if (point_newton<CN, PN>(S, s, n, t + step, xc, sm + L.hc, sm + L.Jc, sm + L.Vc, sm + L.Gc, piv, dinv, red,
-                               P.corsteps, P.tolres, 1, &dxn)) {
+          if (corrector_newton<CN, PN>(S, s, n, t + step, xc, sm, L, piv, dinv, red, P.corsteps, P.tolres, 1,
+                                       &dxn)) {
             cok = true;
             break;
           }
@@ -503,11 +518,14 @@ static int track_launch(const TrackDev &S, const TrackParDev &P, int nmono_max, 
   if (per < 1) per = 1;
   if constexpr (track_min_blocks<PN, RN, true>::split) {
     // one wave at the lower occupancy: take the variant with more registers
+    // (the autotuner's choice when it made one: 1 narrow, 2 wide)
     auto wide = k_track<PN, CN, RN, true>;
     PHC_CUDA(cudaFuncSetAttribute(wide, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_w = 0;
     PHC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_w, wide, kTrackThreads, smem));
-    if (per_w >= 1 && (long)npaths <= (long)nsm * per_w) {
+    const int variant = tune_get(kTuneTrackVariant);
+    const bool take_wide = variant == 2 || (variant == 0 && (long)npaths <= (long)nsm * per_w);
+    if (per_w >= 1 && take_wide) {
       kern = wide;
       per = per_w;
     }

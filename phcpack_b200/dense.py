@@ -63,6 +63,21 @@ def bals_solve_host(prec, cplx, mat, rhs, ninst, dim, degp1, szt, tailidx=1, fla
     return sol, rhs, Q, R, flags
 
 
+def linear_residue_host(prec, cplx, mat, rhs, sol, ninst, dim, degp1, tailidx, res=None):
+    """Residual rhs_i - sum_j A_j sol_{i-j} of the linearised system for
+    tailidx <= i < degp1 (phc_linear_residue_host); returns res (rows below
+    tailidx as given) and resmax (prec doubles per instance)."""
+    W = width(prec, cplx)
+    mat = np.ascontiguousarray(mat, dtype=np.float64)
+    rhs = np.ascontiguousarray(rhs, dtype=np.float64)
+    sol = np.ascontiguousarray(sol, dtype=np.float64)
+    res = np.zeros(ninst * degp1 * dim * W) if res is None else np.array(res, dtype=np.float64, copy=True)
+    resmax = np.zeros(ninst * prec)
+    _lib.call("phc_linear_residue_host", prec, int(cplx), ninst, dim, degp1, tailidx, _lib.ptr(mat), _lib.ptr(rhs),
+              _lib.ptr(sol), _lib.ptr(res), _lib.ptr(resmax), _lib.c_void_p(0))
+    return res, resmax
+
+
 class DeviceBals:
     """Resident buffers for repeated batched solves (torch CUDA tensors as
     device memory)."""

@@ -77,8 +77,11 @@ class QRWork:
         self.R = torch.zeros(ninst * DIM * DIM * PREC, **f64)
         self.flags = torch.zeros(ninst * 5, dtype=torch.int32, device=dev)
         self.flag0 = torch.tensor([1, 0, 0, 0, 1], dtype=torch.int32, device=dev).repeat(ninst)
-        nb = max(dense.workspace_bytes_wy(PREC, False, DIM, SZT, 1), dense.workspace_bytes_wy(PREC, False, DIM, SZT, 0))
+        # workspace for every tile size the autotuner may pick
+        self.tiles = [t for t in (8, 16, 32, 64) if DIM % t == 0]
+        nb = max(dense.workspace_bytes_wy(PREC, False, DIM, t, w) for t in self.tiles for w in (0, 1))
         self.work = torch.zeros(ninst * nb // 8, **f64)
+        self.szt = SZT
         self.units_per_step = ninst
         self.dominant_flops_per_launch = bals_flops() * ninst
         self.dominant_bytes_per_launch = float(self.mat.numel() * 8)
@@ -90,7 +93,7 @@ class QRWork:
         with self.torch.cuda.stream(stream):
             self.rhs.copy_(self.rhs0)
             self.flags.copy_(self.flag0)
-        _lib.call("phc_bals_solve_wy", PREC, 0, self.ninst, DIM, DEGP1, SZT, 1, _lib.ptr(self.mat),
+        _lib.call("phc_bals_solve_wy", PREC, 0, self.ninst, DIM, DEGP1, self.szt, 1, _lib.ptr(self.mat),
                   _lib.ptr(self.rhs), _lib.ptr(self.sol), _lib.ptr(self.Q), _lib.ptr(self.R), _lib.ptr(self.flags),
                   _lib.ptr(self.work), int(wy), _lib.c_void_p(stream.cuda_stream))
         return 1

@@ -111,6 +111,12 @@ class TrackWork:
         self.flops_note = None
         self.dominant_flops_per_launch = 0.0
         self.dominant_bytes_per_launch = float(pb.npaths * pb.maxdim * (16 + 64))
+        # the kernel variant of the split tracker, timed on this batch
+        from . import autotune
+        stream = torch.cuda.Stream(device=dev)
+        tv = autotune.tune_track_variant(torch, stream, self.dt, reps=2, pmode=1, rmode=2, step_mode=self.step_mode)
+        self.config["autotuned"] = {"track_variant": tv["choice"],
+                                    "seconds": {str(k): round(v, 6) for k, v in tv["seconds"].items()}}
 
     def step(self, stream):
         self.dt.run(pmode=1, rmode=2, step_mode=self.step_mode, stream=stream)

@@ -129,3 +129,34 @@ def test_bals_host_entry_matches_device_entry():
     sol2, fl2 = dense.bals_solve_wy(prec, cplx, mat, rhs, ninst, n, degp1, szt, wy=0)
     assert np.array_equal(fl, fl2)
     assert np.array_equal(sol, sol2)
+
+
+@pytest.mark.parametrize("prec,cplx", [(2, False), (2, True), (4, False), (4, True)])
+@pytest.mark.parametrize("tailidx", [0, 1, 3])
+def test_linear_residue_vs_reference(prec, cplx, tailidx):
+    """phc_linear_residue_host against the reference's own host code
+    (CPU_dbl2_linear_residue and twins, Newton/dbl2_bals_host.cpp:548,
+    through oracle/_ref): the residual entries agree within 1e2 * eps_md
+    of the largest product magnitude and the per-limb maximum is that of the
+    same entry (rows below tailidx stay as they were given)."""
+    ref = pyoracle.reference()
+    if ref is None:
+        pytest.skip("the reference's host code was not built here")
+    n, degp1, ninst = 8, 5, 3
+    W = prec * (2 if cplx else 1)
+    rng = np.random.default_rng(100 + 10 * prec + tailidx + (5 if cplx else 0))
+    mats = [wl.random_numbers(rng, (degp1, n, n), prec, cplx, "normal") for _ in range(ninst)]
+    rhss = [wl.random_numbers(rng, (degp1, n), prec, cplx, "normal") for _ in range(ninst)]
+    sols = [wl.random_numbers(rng, (degp1, n), prec, cplx, "normal") for _ in range(ninst)]
+    prev = [wl.random_numbers(rng, (degp1, n), prec, cplx, "normal") for _ in range(ninst)]
+    res, mx = dense.linear_residue_host(prec, cplx, batch_of(mats), batch_of(rhss), batch_of(sols), ninst, n, degp1,
+                                        tailidx, res=batch_of(prev))
+    res = res.reshape(ninst, -1)
+    mx = mx.reshape(ninst, prec)
+    for q in range(ninst):
+        r_ref, mx_ref = ref.linear_residue(prec, cplx, n, degp1, tailidx, mats[q], rhss[q], sols[q], res=prev[q])
+        scale = 2.0 * n * degp1  # |A|, |x| ~ 1: sums of n * degp1 products
+        assert absdiff(res[q], r_ref, prec, cplx).max() <= 1e2 * EPS[prec] * scale
+        rows = res[q].reshape(degp1, n * W)
+        assert np.array_equal(rows[:tailidx], np.asarray(prev[q]).reshape(degp1, n * W)[:tailidx])
+        assert abs(mx[q, 0] - mx_ref[0]) <= 1e-12 * mx_ref[0]

@@ -81,3 +81,75 @@ def test_reference_tiled_solver_tester_through_the_shim(dim, szt, nbt):
     assert max(inv) <= 1e-20 and max(diag) <= 1e-20, (inv, diag)
     for c, g in zip(cpu, gpu):
         assert g <= max(100 * c, 1e-26), (cpu, gpu)
+
+
+def newton_steps(out):
+    import re
+    return re.findall(r"up_h : (\d+)\s+bs_h : (\d+)\s+tail_h : (\d+)\s+up_d : (\d+)\s+bs_d : (\d+)\s+tail_d : (\d+)", out)
+
+
+def newton_tester(name, tol, cdata, dim, deg, problem, extra, szt, nbt):
+    """Runs one of the reference's Newton test programs in mode 2 and checks
+    its host-versus-device sums against tol and the skip and tail counts."""
+    nbsteps = 8
+    if problem == -3:  # the number of columns comes after the Newton steps
+        stdin = f"7\n{cdata}\n{dim}\n{deg}\n1\n{problem}\n{nbsteps}\n4\n2\n{nbt}\n{szt}\n"
+    else:
+        stdin = f"7\n{cdata}\n{dim}\n{deg}\n1\n{problem}\n{extra}{nbsteps}\n2\n{nbt}\n{szt}\n"
+    out = run_program(name, stdin)
+    errs = sums(out, "sum of errors")
+    steps = newton_steps(out)
+    assert len(steps) >= 3 and len(errs) >= 3 * len(steps), out[-3000:]
+    assert max(errs) <= tol, [e for e in errs if e > tol][:10]
+    for s in steps:
+        assert s[0:3] == s[3:6], steps
+    assert int(steps[-1][5]) >= deg, steps[-1]
+
+
+# seed 7, complex data, dimension, degree, verbose level 1, test problem
+# (3: unimodular monomial system, -1: lower triangular ones, -2: decoupled
+# monomials, -3: the columns of cyclic n-roots, -4: a 2-column system, -5:
+# the polynomials of cyclic n-roots in row form), [size of the numbers |
+# number of columns], 8 Newton steps, mode 2 (host and device), tiles, tile size
+@pytest.mark.parametrize("cdata,dim,deg,problem,extra,szt,nbt", [
+    (0, 8, 8, 3, "2\n", 4, 2), (1, 8, 8, 3, "2\n", 4, 2), (0, 8, 8, -1, "", 8, 1), (0, 8, 8, -2, "", 4, 2),
+    (0, 8, 8, -3, None, 4, 2), (1, 8, 8, -3, None, 4, 2), (1, 8, 8, -4, "", 4, 2), (0, 8, 8, -5, "", 4, 2),
+    (1, 8, 8, -5, "", 2, 4), (0, 16, 15, 3, "2\n", 8, 2)])
+def test_reference_newton_tester_through_the_shim(cdata, dim, deg, problem, extra, szt, nbt):
+    """PHCpack's test_dbl2_newton (Newton/, unchanged) with every device
+    entry point it calls taken from the shims: GPU_{dbl2,cmplx2}_bals_solve,
+    GPU_{dbl2,cmplx2}_linear_residue, GPU_dbl2_evaluate_monomials,
+    GPU_cmplx2vectorized_evaluate_monomials, GPU_{dbl2,cmplx2}_evaluate_columns
+    (oracle/ref_shim_newton.cu) and the polynomial evaluation of
+    oracle/ref_shim_polynomials.cu.  In mode 2 the tester runs each Newton
+    step on its CPU code and on the device path and prints the sum of the
+    differences of the evaluated system, Jacobian, right hand sides, Q, R,
+    updated right hand sides, solution update and series; all stay below
+    the reference's own tolerance 1e-20, and the skipped updates, skipped
+    back substitutions and tail indices of the host and device agree at
+    every step."""
+    newton_tester("test_dbl2_newton", 1e-20, cdata, dim, deg, problem, extra, szt, nbt)
+
+
+@pytest.mark.parametrize("cdata,dim,deg,problem,extra,szt,nbt", [
+    (0, 8, 8, 3, "2\n", 4, 2), (1, 8, 8, 3, "2\n", 4, 2), (0, 8, 8, -3, None, 4, 2), (1, 8, 8, -4, "", 8, 1),
+    (0, 8, 8, -5, "", 4, 2), (1, 8, 8, -5, "", 4, 2)])
+def test_reference_quad_double_newton_tester_through_the_shim(cdata, dim, deg, problem, extra, szt, nbt):
+    """PHCpack's test_dbl4_newton (Newton/, unchanged) with the quad double
+    twins of the Newton-layer entry points (ref_shim_newton.cu and
+    ref_shim_polynomials.cu compiled with -DSHIM_NEWTON4 / -DSHIM_POLY4):
+    every host-versus-device sum stays below the tester's own tolerance
+    1e-50 and the skip counts and tail indices agree at every step."""
+    newton_tester("test_dbl4_newton", 1e-50, cdata, dim, deg, problem, extra, szt, nbt)
+
+
+@pytest.mark.parametrize("dim,nterms,deg,seed", [(8, 16, 15, 7), (16, 32, 31, 11)])
+def test_reference_quad_double_polynomial_tester_through_the_shim(dim, nterms, deg, seed):
+    """PHCpack's test_dbl4_polynomials (Polynomials/, unchanged) with
+    GPU_dbl4_poly_evaldiff, GPU_cmplx4_poly_evaldiff and
+    GPU_cmplx4vectorized_poly_evaldiff of the shim; the tester's own
+    tolerance is 1e-56 on the sums of the differences."""
+    stdin = f"{seed}\n{dim}\n0\n{nterms}\n{deg}\n1\n2\n"
+    out = run_program("test_dbl4_polynomials", stdin)
+    assert "on real data" in out and "on complex data" in out, out[-2000:]
+    assert "All tests passed." in out, out[-3000:]
