@@ -804,7 +804,7 @@ __device__ void cta_matvec(int n, const double *M, const double *b, double *y) {
 // Shared-memory layout of a path's CTA (in doubles)
 struct TrackLayout {
   long xs, V, G, hs, J0, M, r, num, den, xp, xc, hc, Jc, Vc, Gc, red, piv, dinv, feat, mag, degs, hbuf, svd, xd, sv,
-      part, total;
+      part, padw, total;
 };
 
 // Matrices of the singular-value jobs of a predictor step: one per warp
@@ -845,6 +845,7 @@ __host__ __device__ inline TrackLayout track_layout(int n, int K, int M, int nm,
   L.J0 = take(n * n * Wp);
   L.M = take(n * n * Wp);
   L.r = take(n * Wp);
+  L.padw = take((long)n * (M * M + 2 * M + 1) * Wp);  // the Pade systems (pade_one_ws)
   const long pend = o;
   // ... overlaid by the scratch of the corrector and the refinement, which
   // run after the Pade approximants are formed
@@ -1138,6 +1139,72 @@ __device__ TRACK_FN int pade_one(int L, int M, int K, const double *c, double *n
     for (int i = 0; i <= L; ++i) {
       T acc = N::zero();
       for (int j = 0; j <= (i < M ? i : M); ++j) acc = N::add(acc, N::mul(q[j], ldn_at<N>(c, i - j)));
+      stn_at<N>(num, i, acc);
+    }
+    return L;
+  }
+  stn_at<N>(den, 0, N::one());
+  for (int i = 0; i <= K; ++i) stn_at<N>(num, i, ldn_at<N>(c, i));
+  return K;
+}
+
+// pade_one with the M x M system, its right hand side and the denominator in
+// shared memory (w: M*M + 2*M + 1 numbers of N) instead of per-thread local
+// arrays: the same operations in the same order, so the same results.  In
+// the tracker's CTA the local arrays of the threads that form the
+// approximants outgrow the L1 cache left beside the shared memory of eight
+// paths, and every access of the elimination would go to L2.
+template <class N>
+__device__ TRACK_FN int pade_one_ws(int L, int M, int K, const double *c, double *num, double *den, double *w) {
+  typedef typename N::T T;
+  const int W = N::width;
+  double *A = w, *b = w + (long)M * M * W, *q = w + (long)(M * M + M) * W;
+  auto a_at = [&](int i, int j) { return ldn_at<N>(A, (long)i * M + j); };
+  bool ok = true;
+  for (int i = 1; i <= M; ++i) {
+    for (int j = 1; j <= M; ++j) {
+      const int k = L + i - j;
+      stn_at<N>(A, (long)(i - 1) * M + (j - 1), k >= 0 ? ldn_at<N>(c, k) : N::zero());
+    }
+    stn_at<N>(b, i - 1, N::neg(ldn_at<N>(c, L + i)));
+  }
+  for (int col = 0; col < M && ok; ++col) {
+    int piv = col;
+    double best = N::mag(a_at(col, col));
+    for (int r = col + 1; r < M; ++r) {
+      const double m = N::mag(a_at(r, col));
+      if (m > best) { best = m; piv = r; }
+    }
+    if (!(best > 0.0)) { ok = false; break; }
+    if (piv != col) {
+      for (int j = 0; j < M; ++j) {
+        const T tt = a_at(piv, j);
+        stn_at<N>(A, (long)piv * M + j, a_at(col, j));
+        stn_at<N>(A, (long)col * M + j, tt);
+      }
+      const T tt = ldn_at<N>(b, piv);
+      stn_at<N>(b, piv, ldn_at<N>(b, col));
+      stn_at<N>(b, col, tt);
+    }
+    const T acc = a_at(col, col);
+    const T bc = ldn_at<N>(b, col);
+    for (int r = col + 1; r < M; ++r) {
+      const T f = N::div(a_at(r, col), acc);
+      for (int j = col; j < M; ++j) stn_at<N>(A, (long)r * M + j, N::sub(a_at(r, j), N::mul(f, a_at(col, j))));
+      stn_at<N>(b, r, N::sub(ldn_at<N>(b, r), N::mul(f, bc)));
+    }
+  }
+  stn_at<N>(q, 0, N::one());
+  if (ok) {
+    for (int i = M - 1; i >= 0; --i) {
+      T acc = ldn_at<N>(b, i);
+      for (int j = i + 1; j < M; ++j) acc = N::sub(acc, N::mul(a_at(i, j), ldn_at<N>(q, j + 1)));
+      stn_at<N>(q, i + 1, N::div(acc, a_at(i, i)));
+    }
+    for (int i = 0; i <= M; ++i) stn_at<N>(den, i, ldn_at<N>(q, i));
+    for (int i = 0; i <= L; ++i) {
+      T acc = N::zero();
+      for (int j = 0; j <= (i < M ? i : M); ++j) acc = N::add(acc, N::mul(ldn_at<N>(q, j), ldn_at<N>(c, i - j)));
       stn_at<N>(num, i, acc);
     }
     return L;

@@ -247,7 +247,8 @@ __global__ void __launch_bounds__(kTrackThreads, (track_min_blocks<PN, RN, WIDE>
       for (int i = ctid(); i < n; i += blockDim.x) {
         const double *ci = xs + (long)i * (K + 1) * Wp;
         double *numi = num + (long)i * (K + 1) * Wp, *deni = den + (long)i * (P.dendeg + 1) * Wp;
-        pdeg_i = pade_one<PN>(P.numdeg, P.dendeg, K, ci, numi, deni);
+        pdeg_i = pade_one_ws<PN>(P.numdeg, P.dendeg, K, ci, numi, deni,
+                                 sm + L.padw + (long)i * (P.dendeg * P.dendeg + 2 * P.dendeg + 1) * Wp);
         qdeg_i = (pdeg_i == P.numdeg) ? P.dendeg : 0;
         const double pe = pade_error_one<PN>(ci, K, numi, pdeg_i, deni, qdeg_i);
         perr2 = fma(pe, pe, perr2);
