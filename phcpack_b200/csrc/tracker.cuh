@@ -952,24 +952,27 @@ __device__ __forceinline__ int eq_first_thread(int i, int n, int G, int ci, int 
 // tracker, for systems that stage no partials): the same steps, tests and
 // results as point_newton<N, double> (Curves/corrector_convolutions.adb
 // :1193-1224, LU_Newton_Steps), with the work of an iteration split over
-// the CTA.  The lead warp evaluates J(x) in complex double from the
-// Jacobian gather lists at the double copy xj of x (lanes over the n^2
-// entries) and factors it, while the other three warps evaluate h(x, t) in
-// double-double: the terms of each equation go to a group of threads (in
-// proportion to the terms, eq_first_thread), each thread forms the values
-// x^e of its terms in double-double and accumulates P = sum b x^e and Q =
-// sum a x^e with compensated sums, its share of h is Q + t (P - Q), and the
-// first thread of the group adds the shares in order.  Then the lead warp
-// solves, updates x (n numbers of N, double-double, in shared memory) and
-// xj.  part: (kTrackThreads - 32) complex double-doubles.
+// the CTA.  First all threads evaluate J(x) in complex double from the
+// Jacobian gather lists at the double copy xj of x (one entry per thread)
+// and the values x^e of the system's distinct monomials in double-double
+// (into V, one monomial per thread).  Then the lead warp factors J while
+// the other three warps form h(x, t): the terms of each equation go to a
+// group of threads (in proportion to the terms, eq_first_thread), each
+// thread accumulates P = sum b x^e and Q = sum a x^e with compensated sums,
+// its share of h is Q + t (P - Q), and the first thread of the group adds
+// the shares in order.  Last the lead warp solves, updates x (n numbers of
+// N, double-double, in shared memory) and xj.  V: the distinct monomials,
+// numbers of N; part: (kTrackThreads - 32) numbers of N.
 template <class N>
 __device__ TRACK_FN bool point_newton_split(const TrackDev &S, int s, int n, double t, double *x, double *h,
-                                            double *Jm, double2 *xj, double *part, int *piv, double *dinv,
-                                            double *red, int maxit, double tol, int extra, double *lastdx) {
+                                            double *Jm, double2 *xj, double *V, double *part, int *piv,
+                                            double *dinv, double *red, int maxit, double tol, int extra,
+                                            double *lastdx) {
   typedef md::num<double, true> JN;
   typedef typename N::T T;
   const int G = kTrackThreads - 32;
   const int e0 = S.eq_off[s];
+  const int m0 = S.mono_off[s], nm = S.mono_off[s + 1] - m0;
   const int tb0 = S.term_off[e0], nterm = S.term_off[e0 + n] - tb0;
   // residual thread ri: equation req, position rk in a group of rg threads
   const int ri = ctid() - 32;
@@ -991,51 +994,56 @@ __device__ TRACK_FN bool point_newton_split(const TrackDev &S, int s, int n, dou
     return make_double2(__dadd_rn(v.re.hi, v.re.lo), __dadd_rn(v.im.hi, v.im.lo));
   };
   if (ctid() < n) xj[ctid()] = to_d2(ldn_at<N>(x, ctid()));
-  __syncwarp();
+  __syncthreads();
   bool conv = false;
   int extra_left = extra;
   int info = 0;
   *lastdx = 1e300;
   for (int it = 0; it < maxit + extra; ++it) {
     if (it >= maxit && !conv) break;
-    if (ctid() < 32) {
-      const int lane = ctid();
-      for (int e = lane; e < n * n; e += 32) {
-        const int i = e / n, j = e % n;
-        const int g = (e0 + i) * S.maxdim + j;
-        double2 acc = make_double2(0.0, 0.0);
-        for (int q = S.jg_off[g]; q < S.jg_off[g + 1]; ++q) {
-          const int tr = S.jg_term[q], sl = S.jg_slot[q];
-          const double ar = S.term_a[2 * tr], ai = S.term_a[2 * tr + 1];
-          const double2 c = make_double2(fma(S.term_b[2 * tr] - ar, t, ar), fma(S.term_b[2 * tr + 1] - ai, t, ai));
-          double2 v;
-          if (sl == -1) v = make_double2(1.0, 0.0);
-          else if (sl == -2) v = make_double2(2.0 * xj[j].x, 2.0 * xj[j].y);
-          else v = xj[-sl - 3];
-          acc.x = fma(c.x, v.x, fma(-c.y, v.y, acc.x));
-          acc.y = fma(c.x, v.y, fma(c.y, v.x, acc.y));
-        }
-        reinterpret_cast<double2 *>(Jm)[e] = acc;
+    // J(x) in complex double, one entry per thread
+    for (int e = ctid(); e < n * n; e += kTrackThreads) {
+      const int i = e / n, j = e % n;
+      const int g = (e0 + i) * S.maxdim + j;
+      double2 acc = make_double2(0.0, 0.0);
+      for (int q = S.jg_off[g]; q < S.jg_off[g + 1]; ++q) {
+        const int tr = S.jg_term[q], sl = S.jg_slot[q];
+        const double ar = S.term_a[2 * tr], ai = S.term_a[2 * tr + 1];
+        const double2 c = make_double2(fma(S.term_b[2 * tr] - ar, t, ar), fma(S.term_b[2 * tr + 1] - ai, t, ai));
+        double2 v;
+        if (sl == -1) v = make_double2(1.0, 0.0);
+        else if (sl == -2) v = make_double2(2.0 * xj[j].x, 2.0 * xj[j].y);
+        else v = xj[-sl - 3];
+        acc.x = fma(c.x, v.x, fma(-c.y, v.y, acc.x));
+        acc.y = fma(c.x, v.y, fma(c.y, v.x, acc.y));
       }
-      __syncwarp();
+      reinterpret_cast<double2 *>(Jm)[e] = acc;
+    }
+    // the distinct monomials x^e in double-double, one per thread
+    for (int m = ctid(); m < nm; m += kTrackThreads) {
+      const int gm = m0 + m;
+      const int nv = S.mono_nvr[gm];
+      const int *ix = S.mono_idx + (long)gm * S.maxvar;
+      const int *ex = S.mono_exp + (long)gm * S.maxvar;
+      T v = N::one();
+      bool unit = true;
+      for (int u = 0; u < nv; ++u) {
+        const T xu = ldn_at<N>(x, ix[u]);
+        for (int q = 0; q < ex[u]; ++q) {
+          v = unit ? xu : N::mul(v, xu);
+          unit = false;
+        }
+      }
+      stn_at<N>(V, m, v);
+    }
+    __syncthreads();
+    if (ctid() < 32) {
       info = warp_lufac<JN>(n, Jm, piv, dinv);
     } else {
       sum2 pr, pi, qr, qi;
       pr.zero(); pi.zero(); qr.zero(); qi.zero();
       for (int tr = S.term_off[e0 + req] + rk; tr < S.term_off[e0 + req + 1]; tr += rg) {
-        const int gm = S.term_mono[tr];
-        const int nv = S.mono_nvr[gm];
-        const int *ix = S.mono_idx + (long)gm * S.maxvar;
-        const int *ex = S.mono_exp + (long)gm * S.maxvar;
-        T v = N::one();
-        bool unit = true;
-        for (int u = 0; u < nv; ++u) {
-          const T xu = ldn_at<N>(x, ix[u]);
-          for (int q = 0; q < ex[u]; ++q) {
-            v = unit ? xu : N::mul(v, xu);
-            unit = false;
-          }
-        }
+        const T v = ldn_at<N>(V, S.term_mono[tr] - m0);
         const double ar = S.term_a[2 * tr], ai = S.term_a[2 * tr + 1];
         const double br = S.term_b[2 * tr], bi = S.term_b[2 * tr + 1];
         pr.add_prod(br, v.re);

@@ -114,7 +114,7 @@ __device__ TRACK_FN bool corrector_newton(const TrackDev &S, int s, int n, doubl
   if constexpr (PN::width == 2 && CN::width == 4) {
     if (!S.gstaged)
       return point_newton_split<CN>(S, s, n, t, x, sm + L.hc, sm + L.Jc, reinterpret_cast<double2 *>(sm + L.xd),
-                                    sm + L.part, piv, dinv, red, maxit, tol, extra, lastdx);
+                                    sm + L.Vc, sm + L.part, piv, dinv, red, maxit, tol, extra, lastdx);
   }
   return point_newton<CN, PN>(S, s, n, t, x, sm + L.hc, sm + L.Jc, sm + L.Vc, sm + L.Gc, piv, dinv, red, maxit, tol,
                               extra, lastdx);

@@ -2,7 +2,7 @@
 
     python -m phcpack_b200.profile_case eval --nsys 512
     python -m phcpack_b200.profile_case bals --ninst 64
-    python -m phcpack_b200.profile_case track --paths 256
+    python -m phcpack_b200.profile_case track --paths 256 [--variant 2]
     python -m phcpack_b200.profile_case diag --paths 1024
 
 Builds the seeded workload on the device, runs the kernel ``--warm`` times
@@ -30,6 +30,8 @@ def main():
     ap.add_argument("--paths", type=int, default=256)
     ap.add_argument("--warm", type=int, default=1)
     ap.add_argument("--reps", type=int, default=1)
+    ap.add_argument("--variant", type=int, default=2,
+                    help="track: kernel variant of the split tracker (1 narrow, 2 wide, 0 the built-in rule)")
     a = ap.parse_args()
     import torch
 
@@ -45,8 +47,9 @@ def main():
     elif a.case == "diag":
         return diag(torch, dev, a)
     else:
-        from phcpack_b200 import trackwork
-        w = trackwork.TrackWork(torch, dev, 0, npaths=a.paths)
+        from phcpack_b200 import autotune, trackwork
+        autotune.set_knob(autotune.KNOB_TRACK_VARIANT, a.variant)
+        w = trackwork.TrackWork(torch, dev, 0, npaths=a.paths, tune=False)
     s = torch.cuda.Stream(device=dev)
     for _ in range(a.warm + a.reps):
         w.step(s)

@@ -94,7 +94,7 @@ class TrackWork:
     traffic_bytes_per_launch = 5.159e6
     dominant_launches_per_step = 1
 
-    def __init__(self, torch, dev, rank, npaths=1024):
+    def __init__(self, torch, dev, rank, npaths=1024, tune=True):
         self.torch = torch
         pb = hm.config4(seed=4 + rank)
         if npaths < pb.npaths:
@@ -112,11 +112,13 @@ class TrackWork:
         self.dominant_flops_per_launch = 0.0
         self.dominant_bytes_per_launch = float(pb.npaths * pb.maxdim * (16 + 64))
         # the kernel variant of the split tracker, timed on this batch
-        from . import autotune
-        stream = torch.cuda.Stream(device=dev)
-        tv = autotune.tune_track_variant(torch, stream, self.dt, reps=2, pmode=1, rmode=2, step_mode=self.step_mode)
-        self.config["autotuned"] = {"track_variant": tv["choice"],
-                                    "seconds": {str(k): round(v, 6) for k, v in tv["seconds"].items()}}
+        if tune:
+            from . import autotune
+            stream = torch.cuda.Stream(device=dev)
+            tv = autotune.tune_track_variant(torch, stream, self.dt, reps=2, pmode=1, rmode=2,
+                                             step_mode=self.step_mode)
+            self.config["autotuned"] = {"track_variant": tv["choice"],
+                                        "seconds": {str(k): round(v, 6) for k, v in tv["seconds"].items()}}
 
     def step(self, stream):
         self.dt.run(pmode=1, rmode=2, step_mode=self.step_mode, stream=stream)

@@ -88,19 +88,27 @@ def newton_steps(out):
     return re.findall(r"up_h : (\d+)\s+bs_h : (\d+)\s+tail_h : (\d+)\s+up_d : (\d+)\s+bs_d : (\d+)\s+tail_d : (\d+)", out)
 
 
-def newton_tester(name, tol, cdata, dim, deg, problem, extra, szt, nbt):
+def newton_tester(name, tol, drift, cdata, dim, deg, problem, extra, szt, nbt, nbsteps=8):
     """Runs one of the reference's Newton test programs in mode 2 and checks
-    its host-versus-device sums against tol and the skip and tail counts."""
-    nbsteps = 8
+    its host-versus-device sums: at the first Newton step (same input on
+    both sides) every sum is at most tol, the reference's own tolerance; the
+    host and the device then iterate independently, so later sums are the
+    first step's rounding differences as the iteration carries them, bounded
+    by drift; the skipped updates, skipped back substitutions and tail
+    indices agree at every step."""
     if problem == -3:  # the number of columns comes after the Newton steps
         stdin = f"7\n{cdata}\n{dim}\n{deg}\n1\n{problem}\n{nbsteps}\n4\n2\n{nbt}\n{szt}\n"
     else:
         stdin = f"7\n{cdata}\n{dim}\n{deg}\n1\n{problem}\n{extra}{nbsteps}\n2\n{nbt}\n{szt}\n"
     out = run_program(name, stdin)
-    errs = sums(out, "sum of errors")
     steps = newton_steps(out)
-    assert len(steps) >= 3 and len(errs) >= 3 * len(steps), out[-3000:]
-    assert max(errs) <= tol, [e for e in errs if e > tol][:10]
+    blocks = out.split("up_h :")
+    assert len(steps) >= 3 and len(blocks) == len(steps) + 1, out[-3000:]
+    first = sums(blocks[0], "sum of errors")
+    errs = sums(out, "sum of errors")
+    assert len(first) >= 3 and len(errs) >= 3 * len(steps), out[-3000:]
+    assert max(first) <= tol, first
+    assert max(errs) <= drift, [e for e in errs if e > drift][:10]
     for s in steps:
         assert s[0:3] == s[3:6], steps
     assert int(steps[-1][5]) >= deg, steps[-1]
@@ -125,10 +133,13 @@ def test_reference_newton_tester_through_the_shim(cdata, dim, deg, problem, extr
     step on its CPU code and on the device path and prints the sum of the
     differences of the evaluated system, Jacobian, right hand sides, Q, R,
     updated right hand sides, solution update and series; all stay below
-    the reference's own tolerance 1e-20, and the skipped updates, skipped
-    back substitutions and tail indices of the host and device agree at
-    every step."""
-    newton_tester("test_dbl2_newton", 1e-20, cdata, dim, deg, problem, extra, szt, nbt)
+    the reference's own tolerance 1e-20 (for the columns of cyclic n-roots
+    at the first step, the later steps drifting apart as the iteration
+    amplifies the first step's rounding differences, to about 1e-18 after
+    eight steps), and the skipped updates, skipped back substitutions and
+    tail indices of the host and device agree at every step."""
+    newton_tester("test_dbl2_newton", 1e-20, 1e-20 if problem != -3 else 1e-15, cdata, dim, deg, problem, extra,
+                  szt, nbt, nbsteps=12)
 
 
 @pytest.mark.parametrize("cdata,dim,deg,problem,extra,szt,nbt", [
@@ -138,9 +149,15 @@ def test_reference_quad_double_newton_tester_through_the_shim(cdata, dim, deg, p
     """PHCpack's test_dbl4_newton (Newton/, unchanged) with the quad double
     twins of the Newton-layer entry points (ref_shim_newton.cu and
     ref_shim_polynomials.cu compiled with -DSHIM_NEWTON4 / -DSHIM_POLY4):
-    every host-versus-device sum stays below the tester's own tolerance
-    1e-50 and the skip counts and tail indices agree at every step."""
-    newton_tester("test_dbl4_newton", 1e-50, cdata, dim, deg, problem, extra, szt, nbt)
+    at the first step every host-versus-device sum stays below the
+    tester's own tolerance 1e-50, and the skip counts and tail indices agree
+    at every step.  The tester sums differences limb by limb, so two
+    quad-doubles equal to 1e-63 but normalised differently (a leading limb
+    one ulp apart, the next limb compensating) count as about one ulp of the
+    leading limb; later steps are held to 1e-30 for that reason (seen once:
+    9.6e-35 from a Jacobian entry of -3.88e-19 whose two values differ by
+    9e-64)."""
+    newton_tester("test_dbl4_newton", 1e-50, 1e-30, cdata, dim, deg, problem, extra, szt, nbt, nbsteps=12)
 
 
 @pytest.mark.parametrize("dim,nterms,deg,seed", [(8, 16, 15, 7), (16, 32, 31, 11)])
