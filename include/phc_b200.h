@@ -40,7 +40,10 @@ int phc_abi_version(void);
  *           (the rule: min(dim, 8), fewer when the scratch needs it);
  *   knob 1: variant of the split tracker's kernel, 1 the 64-register one
  *           (8 paths per SM), 2 the 72-register one (7 paths per SM) (the
- *           rule: 2 when the batch fits in one wave at 7 per SM).
+ *           rule: 2 when the batch fits in one wave at 7 per SM);
+ *   knob 2: paths the tracker runs at once per SM, 1..32, at most what the
+ *           occupancy allows (the rule: that maximum); the work queue hands
+ *           out the other paths as paths finish.
  * phc_tune_get returns the value (>= 0) or an error. */
 int phc_tune_set(int knob, int value);
 int phc_tune_get(int knob);

@@ -8,7 +8,8 @@ Three choices are swept once per shape and cached for the process:
   (``phc_bals_solve``), over the divisors of the dimension among
   8, 16, 32 and 64 (a call argument, returned to the caller);
 * the variant of the split tracker's kernel (knob 1), 1 the 64-register
-  kernel at 8 paths per SM, 2 the 72-register kernel at 7 paths per SM.
+  kernel at 8 paths per SM, 2 the 72-register kernel at 7 paths per SM,
+  together with the paths tracked at once per SM (knob 2), 4 to 8.
 
 Every candidate is timed with CUDA events on the caller's stream after one
 untimed run; the fastest is kept (ties to the built-in rule's choice).  The
@@ -23,6 +24,7 @@ from . import _lib
 
 KNOB_EVAL_WARPS = 0
 KNOB_TRACK_VARIANT = 1
+KNOB_TRACK_PER_SM = 2
 
 _cache: dict = {}
 
@@ -96,20 +98,25 @@ def tune_bals_tile(torch, stream, prec, cplx, ninst, dim, degp1, mat, rhs0, sol,
     return _cache[key]
 
 
-def tune_track_variant(torch, stream, tracker, reps: int = 2, **run_kw) -> dict:
-    """Time the two kernels of the split tracker on a DeviceTracker's own
-    batch (tracker.run(**run_kw)) and set knob 1 to the faster."""
-    key = ("track", tracker.pb.npaths, tracker.pb.maxdim, tuple(sorted(run_kw.items())))
+def tune_track_variant(torch, stream, tracker, reps: int = 2, per_sm=(4, 5, 6, 7, 8), **run_kw) -> dict:
+    """Time the kernel variants of the split tracker and the paths per SM on
+    a DeviceTracker's own batch (tracker.run(**run_kw)); set knobs 1 and 2
+    to the fastest pair.  choice: the variant; per_sm: the paths per SM."""
+    key = ("track", tracker.pb.npaths, tracker.pb.maxdim, tuple(per_sm), tuple(sorted(run_kw.items())))
     if key in _cache:
         set_knob(KNOB_TRACK_VARIANT, _cache[key]["choice"])
+        set_knob(KNOB_TRACK_PER_SM, _cache[key]["per_sm"])
         return _cache[key]
     secs = {}
     for v in (1, 2):
         set_knob(KNOB_TRACK_VARIANT, v)
-        secs[v] = _time(torch, stream, lambda: tracker.run(stream=stream, **run_kw), reps)
-    best = min((1, 2), key=lambda v: secs[v])
-    set_knob(KNOB_TRACK_VARIANT, best)
-    _cache[key] = {"choice": best, "seconds": secs}
+        for k in per_sm:
+            set_knob(KNOB_TRACK_PER_SM, k)
+            secs[(v, k)] = _time(torch, stream, lambda: tracker.run(stream=stream, **run_kw), reps)
+    best = min(secs, key=lambda vk: (secs[vk], -vk[1]))
+    set_knob(KNOB_TRACK_VARIANT, best[0])
+    set_knob(KNOB_TRACK_PER_SM, best[1])
+    _cache[key] = {"choice": best[0], "per_sm": best[1], "seconds": {f"{v}/{k}": t for (v, k), t in secs.items()}}
     return _cache[key]
 
 
@@ -117,3 +124,4 @@ def reset() -> None:
     """Back to the built-in rules; the cache is kept."""
     set_knob(KNOB_EVAL_WARPS, 0)
     set_knob(KNOB_TRACK_VARIANT, 0)
+    set_knob(KNOB_TRACK_PER_SM, 0)

@@ -531,6 +531,11 @@ static int track_launch(const TrackDev &S, const TrackParDev &P, int nmono_max, 
       per = per_w;
     }
   }
+  // paths tracked at once per SM: all the resident CTAs the occupancy allows,
+  // or fewer when the autotuner found that faster (fewer paths share an SM's
+  // issue slots; the work queue hands the rest out as paths finish)
+  const int cap = tune_get(kTuneTrackPerSM);
+  if (cap > 0 && cap < per) per = cap;
   long grid = (long)nsm * per;
   if (grid > npaths) grid = npaths;
   if (grid < 1) return PHC_OK;

@@ -117,7 +117,7 @@ class TrackWork:
             stream = torch.cuda.Stream(device=dev)
             tv = autotune.tune_track_variant(torch, stream, self.dt, reps=2, pmode=1, rmode=2,
                                              step_mode=self.step_mode)
-            self.config["autotuned"] = {"track_variant": tv["choice"],
+            self.config["autotuned"] = {"track_variant": tv["choice"], "paths_per_sm": tv["per_sm"],
                                         "seconds": {str(k): round(v, 6) for k, v in tv["seconds"].items()}}
 
     def step(self, stream):

@@ -48,16 +48,19 @@ def test_track_variant_choice_does_not_change_results():
     pb = hm.subset(hm.config4(), np.arange(192))
     dt = hm.DeviceTracker(pb)
     results = {}
-    for v in (1, 2):
+    for v, k in ((1, 0), (2, 0), (2, 3), (1, 5)):
         autotune.set_knob(autotune.KNOB_TRACK_VARIANT, v)
+        autotune.set_knob(autotune.KNOB_TRACK_PER_SM, k)
         dt.run(pmode=1, rmode=2)
-        results[v] = dt.result()
-    a, b = results[1], results[2]
-    assert np.array_equal(a.status, b.status) and np.array_equal(a.steps, b.steps)
-    assert np.array_equal(a.xend, b.xend)
+        results[(v, k)] = dt.result()
+    a = results[(1, 0)]
+    for b in results.values():
+        assert np.array_equal(a.status, b.status) and np.array_equal(a.steps, b.steps)
+        assert np.array_equal(a.xend, b.xend)
     stream = torch.cuda.Stream()
-    res = autotune.tune_track_variant(torch, stream, dt, reps=1, pmode=1, rmode=2)
+    res = autotune.tune_track_variant(torch, stream, dt, reps=1, per_sm=(4, 8), pmode=1, rmode=2)
     assert res["choice"] in (1, 2) and autotune.get_knob(autotune.KNOB_TRACK_VARIANT) == res["choice"]
+    assert res["per_sm"] in (4, 8) and autotune.get_knob(autotune.KNOB_TRACK_PER_SM) == res["per_sm"]
 
 
 def test_bals_tile_choice_is_valid_and_accurate():
