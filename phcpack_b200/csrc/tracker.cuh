@@ -433,12 +433,12 @@ __device__ TRACK_FN int warp_lufac(int n, double *A, int *ipvt, double *dinv) {
       v = N::lead(ldn_at<N>(A, (long)lane * n + k));
       if (!(v == v)) v = INFINITY;  // a NaN pivot candidate reads as infinity
     }
-    int ix = (lane >= k && lane < n) ? lane : n;
-    for (int o = 16; o > 0; o >>= 1) {  // largest value, the first row on ties
-      const double v2 = __shfl_xor_sync(0xffffffffu, v, o);
-      const int ix2 = __shfl_xor_sync(0xffffffffu, ix, o);
-      if (v2 > v || (v2 == v && ix2 < ix)) { v = v2; ix = ix2; }
-    }
+    // the largest value, then the first row that holds it (one ballot)
+    double mx = v;
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    const unsigned hold = __ballot_sync(0xffffffffu, lane >= k && lane < n && v == mx);
+    const int ix = hold ? __ffs(hold) - 1 : n;
+    v = mx;
     const int ell = ix < n ? ix : n - 1;
     if (lane == 0) ipvt[k] = ell;
     if (v == 0.0) {
@@ -804,7 +804,7 @@ __device__ void cta_matvec(int n, const double *M, const double *b, double *y) {
 // Shared-memory layout of a path's CTA (in doubles)
 struct TrackLayout {
   long xs, V, G, hs, J0, M, r, num, den, xp, xc, hc, Jc, Vc, Gc, red, piv, dinv, feat, mag, degs, hbuf, svd, xd, sv,
-      part, padw, total;
+      part, padw, xa, total;
 };
 
 // Matrices of the singular-value jobs of a predictor step: one per warp
@@ -837,6 +837,7 @@ __host__ __device__ inline TrackLayout track_layout(int n, int K, int M, int nm,
   L.svd = take((long)kSvdSlots * n * n * 2);  // complex doubles
   L.xd = take(2L * n);
   L.sv = take(n + 2);
+  L.xa = take(n);  // |x_i| of the predicted point (mixed residual)
   // scratch of the Taylor series and the predictor feedback ...
   const long ov = o;
   L.V = take(nm * 2 * Wp);  // two coefficients per monomial (point evaluations use one)

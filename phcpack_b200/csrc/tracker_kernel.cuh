@@ -70,14 +70,16 @@ __device__ typename N::T horner(const double *a, int deg, const typename N::T &z
 // Curves/standard_predictor_convolutions.adb:958-993.
 template <class PN>
 __device__ TRACK_FN double pade_mixres(const TrackDev &S, int s, int n, int K, int dendeg, double t, double st,
-                              const double *num, const double *den, const int *degs, double *xp, double *V,
-                              double *G, double *hs, double *red) {
+                              const double *num, const double *den, const int *degs, double *xp, double *xa,
+                              double *V, double *G, double *hs, double *red) {
   const int Wp = PN::width;
   for (int i = ctid(); i < n; i += blockDim.x) {
     const typename PN::T z = PN::from(st);
     const typename PN::T nv = horner<PN>(num + (long)i * (K + 1) * Wp, degs[2 * i], z);
     const typename PN::T dv = horner<PN>(den + (long)i * (dendeg + 1) * Wp, degs[2 * i + 1], z);
-    stn_at<PN>(xp, i, PN::div(nv, dv));
+    const typename PN::T xi = PN::div(nv, dv);
+    stn_at<PN>(xp, i, xi);
+    xa[i] = PN::mag(xi);
   }
   __syncthreads();
   hom_eval_cta<PN>(S, s, 0, t + st, xp, 1, V, G, hs, nullptr);
@@ -93,8 +95,8 @@ __device__ TRACK_FN double pade_mixres(const TrackDev &S, int s, int n, int K, i
       double v = hypot(fma(S.term_b[2 * tr] - S.term_a[2 * tr], t + st, S.term_a[2 * tr]),
                        fma(S.term_b[2 * tr + 1] - S.term_a[2 * tr + 1], t + st, S.term_a[2 * tr + 1]));
       for (int u = 0; u < S.mono_nvr[gm]; ++u) {
-        const double xa = PN::mag(ldn_at<PN>(xp, S.mono_idx[(long)gm * S.maxvar + u]));
-        for (int e = 0; e < S.mono_exp[(long)gm * S.maxvar + u]; ++e) v *= xa;
+        const double xu = xa[S.mono_idx[(long)gm * S.maxvar + u]];
+        for (int e = 0; e < S.mono_exp[(long)gm * S.maxvar + u]; ++e) v *= xu;
       }
       ab += v;
     }
@@ -362,8 +364,8 @@ __global__ void __launch_bounds__(kTrackThreads, (track_min_blocks<PN, RN, WIDE>
         double *xp = sm + L.xp;
         bool ok = false;
         for (int h = 0; h < 64; ++h) {
-          const double mixres = pade_mixres<PN>(S, s, n, K, P.dendeg, t, step, num, den, degs, xp, sm + L.V,
-                                                sm + L.G, sm + L.hs, red);
+          const double mixres = pade_mixres<PN>(S, s, n, K, P.dendeg, t, step, num, den, degs, xp, sm + L.xa,
+                                                sm + L.V, sm + L.G, sm + L.hs, red);
           if (mixres < P.alpha) { ok = true; break; }
           step *= 0.5;
           ++nrej;
@@ -413,8 +415,8 @@ __global__ void __launch_bounds__(kTrackThreads, (track_min_blocks<PN, RN, WIDE>
           double sp = fmin(plain_step * mults[q], P.maxsize);
           if (t + sp > 1.0) sp = 1.0 - t;
           if (sp <= best) continue;
-          const double mr = pade_mixres<PN>(S, s, n, K, P.dendeg, t, sp, num, den, degs, sm + L.xp, sm + L.V,
-                                            sm + L.G, sm + L.hs, red);
+          const double mr = pade_mixres<PN>(S, s, n, K, P.dendeg, t, sp, num, den, degs, sm + L.xp, sm + L.xa,
+                                            sm + L.V, sm + L.G, sm + L.hs, red);
           if (mr < P.alpha) best = sp;
         }
         if (ctid() == 0) {
