@@ -43,7 +43,11 @@ int phc_abi_version(void);
  *           rule: 2 when the batch fits in one wave at 7 per SM);
  *   knob 2: paths the tracker runs at once per SM, 1..32, at most what the
  *           occupancy allows (the rule: that maximum); the work queue hands
- *           out the other paths as paths finish.
+ *           out the other paths as paths finish;
+ *   knob 3: blocked QR and least squares: 1 keeps the WY panels and the
+ *           column panel of R in global memory, 2 stages them in shared
+ *           memory whenever they fit (the rule: staged when they fit in
+ *           200 KB, as for n = 64 and tile 16 in quad-double).
  * phc_tune_get returns the value (>= 0) or an error. */
 int phc_tune_set(int knob, int value);
 int phc_tune_get(int knob);

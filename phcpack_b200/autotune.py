@@ -6,7 +6,9 @@ Three choices are swept once per shape and cached for the process:
   ``phc_tune_set``), over 1, 2, 4 and 8;
 * the tile size ``szt`` of the blocked QR / least squares
   (``phc_bals_solve``), over the divisors of the dimension among
-  8, 16, 32 and 64 (a call argument, returned to the caller);
+  8, 16, 32 and 64 (a call argument, returned to the caller), with the
+  WY panels and the column panel of R in global or in shared memory
+  (knob 3);
 * the variant of the split tracker's kernel (knob 1), 1 the 64-register
   kernel at 8 paths per SM, 2 the 72-register kernel at 7 paths per SM,
   together with the paths tracked at once per SM (knob 2), 4 to 8.
@@ -25,6 +27,7 @@ from . import _lib
 KNOB_EVAL_WARPS = 0
 KNOB_TRACK_VARIANT = 1
 KNOB_TRACK_PER_SM = 2
+KNOB_DENSE_STAGE = 3
 
 _cache: dict = {}
 
@@ -71,13 +74,16 @@ def tune_eval_warps(torch, stream, args, dim: int, key=None, reps: int = 3) -> d
 
 
 def tune_bals_tile(torch, stream, prec, cplx, ninst, dim, degp1, mat, rhs0, sol, Q, R, flags, flag0, work,
-                   wy: int = 0, reps: int = 3, cands=(8, 16, 32, 64)) -> dict:
-    """Sweep the tile size of phc_bals_solve_wy on resident device buffers
-    (rhs and flags are restored from rhs0 and flag0 before every run; work
-    must hold the workspace of the smallest tile).  Returns {"choice",
-    "seconds"}; the caller passes the choice as szt."""
-    key = ("bals", prec, cplx, ninst, dim, degp1, wy)
+                   wy: int = 0, reps: int = 3, cands=(8, 16, 32, 64), stages=(1, 2)) -> dict:
+    """Sweep the tile size of phc_bals_solve_wy and the staging of its panels
+    (knob 3: 1 global memory, 2 shared memory where they fit) on resident
+    device buffers (rhs and flags are restored from rhs0 and flag0 before
+    every run; work must hold the workspace of every tile).  Sets knob 3 and
+    returns {"choice": tile, "stage", "seconds"}; the caller passes the tile
+    as szt."""
+    key = ("bals", prec, cplx, ninst, dim, degp1, wy, tuple(cands), tuple(stages))
     if key in _cache:
+        set_knob(KNOB_DENSE_STAGE, _cache[key]["stage"])
         return _cache[key]
     tiles = [t for t in cands if dim % t == 0 and t <= dim]
     if not tiles:
@@ -92,9 +98,14 @@ def tune_bals_tile(torch, stream, prec, cplx, ninst, dim, degp1, mat, rhs0, sol,
                   _lib.ptr(sol), _lib.ptr(Q), _lib.ptr(R), _lib.ptr(flags), _lib.ptr(work), int(wy),
                   _lib.c_void_p(stream.cuda_stream))
 
-    secs = {t: _time(torch, stream, lambda t=t: run(t), reps) for t in tiles}
-    best = min(tiles, key=lambda t: (secs[t], t))
-    _cache[key] = {"choice": best, "seconds": secs}
+    secs = {}
+    for g in stages:
+        set_knob(KNOB_DENSE_STAGE, g)
+        for t in tiles:
+            secs[(t, g)] = _time(torch, stream, lambda t=t: run(t), reps)
+    best = min(secs, key=lambda tg: (secs[tg], tg[0], tg[1]))
+    set_knob(KNOB_DENSE_STAGE, best[1])
+    _cache[key] = {"choice": best[0], "stage": best[1], "seconds": {f"{t}/{g}": v for (t, g), v in secs.items()}}
     return _cache[key]
 
 
@@ -125,3 +136,4 @@ def reset() -> None:
     set_knob(KNOB_EVAL_WARPS, 0)
     set_knob(KNOB_TRACK_VARIANT, 0)
     set_knob(KNOB_TRACK_PER_SM, 0)
+    set_knob(KNOB_DENSE_STAGE, 0)

@@ -218,7 +218,8 @@ def side_block(name, torch, dev, fp64_tflops, hbm_gbs, steps=3, warm=2):
                                     work.Q, work.R, work.flags, flag0, work.work, wy=work.wy, reps=1,
                                     cands=tuple(work.tiles))
         work.szt = r["choice"]
-        tuned = {"szt": r["choice"], "seconds": {str(k): round(v, 6) for k, v in r["seconds"].items()}}
+        tuned = {"szt": r["choice"], "stage_in_shared_memory": r["stage"] == 2,
+                 "seconds": {str(k): round(v, 6) for k, v in r["seconds"].items()}}
     for _ in range(warm):
         work.step(stream)
     torch.cuda.synchronize()

@@ -117,6 +117,7 @@ int phc_tune_set(int knob, int value) {
   if (knob == kTuneEvalWarps) PHC_REQUIRE(value <= 8, "tune_set: warps per CTA %d > 8", value);
   if (knob == kTuneTrackVariant) PHC_REQUIRE(value <= 2, "tune_set: tracker variant %d not in 0..2", value);
   if (knob == kTuneTrackPerSM) PHC_REQUIRE(value <= 32, "tune_set: paths per SM %d > 32", value);
+  if (knob == kTuneDenseStage) PHC_REQUIRE(value <= 2, "tune_set: staging %d not in 0..2", value);
   g_tune[knob].store(value);
   return PHC_OK;
 }

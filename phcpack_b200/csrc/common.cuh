@@ -50,7 +50,7 @@ const char *get_error();
 inline int width_of(int prec, int cplx) { return prec * (cplx ? 2 : 1); }
 // Launch-shape knobs set by the autotuner (phc_tune_set); 0 leaves the
 // built-in rule.
-enum { kTuneEvalWarps = 0, kTuneTrackVariant = 1, kTuneTrackPerSM = 2, kTuneKnobs = 3 };
+enum { kTuneEvalWarps = 0, kTuneTrackVariant = 1, kTuneTrackPerSM = 2, kTuneDenseStage = 3, kTuneKnobs = 4 };
 int tune_get(int knob);
 inline bool prec_ok(int prec) { return prec == 1 || prec == 2 || prec == 4; }
 

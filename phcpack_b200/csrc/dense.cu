@@ -17,7 +17,7 @@ __host__ __device__ inline long dense_stride(int n, int szt, int W, bool oz) {
 template <class N, bool OZ>
 __global__ void __launch_bounds__(kDenseThreads)
     k_blocked_houseqr(int n, int ncols, int szt, const double *__restrict__ A, double *__restrict__ Q,
-                      double *__restrict__ Rm, double *__restrict__ work) {
+                      double *__restrict__ Rm, double *__restrict__ work, int stage) {
   extern __shared__ __align__(16) double sm[];
   const int W = N::width;
   const long inst = blockIdx.x;
@@ -25,9 +25,13 @@ __global__ void __launch_bounds__(kDenseThreads)
   const double *a = A + inst * n * ncols * W;
   double *q = Q + inst * n * n * W;
   double *r = Rm + inst * n * ncols * W;
+  double *wk = work + inst * dense_stride(n, szt, W, OZ);
+  // the WY panels and the column panel of R in shared memory when staged
+  double *ywpt = stage ? sm + dense_smem_doubles(n, szt, W) : wk;
+  double *panel = stage ? ywpt + 4L * n * szt * W : nullptr;
   for (long t = threadIdx.x; t < (long)n * ncols * W; t += blockDim.x) r[t] = a[t];
   __syncthreads();
-  block_houseqr<N, OZ>(n, ncols, szt, q, r, work + inst * dense_stride(n, szt, W, OZ), S);
+  block_houseqr<N, OZ>(n, ncols, szt, q, r, ywpt, wk + dense_work_numbers(n, szt) * W, S, panel);
 }
 
 // Like Matrices/dbl2_tabs_kernels.cu:952 (GPU_dbl2_upper_tiled_solver): b is
@@ -64,7 +68,7 @@ template <class N, bool OZ>
 __global__ void __launch_bounds__(kDenseThreads)
     k_bals_solve(int n, int degp1, int szt, int tailidx, const double *__restrict__ mat, double *__restrict__ rhs,
                  double *__restrict__ sol, double *__restrict__ Q, double *__restrict__ Rm, int *__restrict__ flags,
-                 double *__restrict__ work) {
+                 double *__restrict__ work, int stage) {
   extern __shared__ __align__(16) double sm[];
   typedef typename N::T T;
   const int W = N::width;
@@ -78,7 +82,11 @@ __global__ void __launch_bounds__(kDenseThreads)
   double *r = Rm + inst * nn * W;
   int *fl = flags + inst * 5;
   double *wk = work + inst * dense_stride(n, szt, W, OZ);
-  double *tinv = wk + 4L * n * szt * W;
+  // staged: the WY panels, the column panel of R and then the inverted
+  // diagonal tiles of R in shared memory
+  double *ywpt = stage ? sm + dense_smem_doubles(n, szt, W) : wk;
+  double *panel = stage ? ywpt + 4L * n * szt * W : nullptr;
+  double *tinv = stage ? panel : wk + 4L * n * szt * W;
   int zeroQ = fl[0], noqr = fl[1];
   const int tail0 = max(1, tailidx >= 0 ? tailidx : fl[4]);
   bool tinv_ok = false;
@@ -92,7 +100,7 @@ __global__ void __launch_bounds__(kDenseThreads)
     if (!noqr) {
       for (long t = threadIdx.x; t < nn * W; t += blockDim.x) r[t] = A[t];
       __syncthreads();
-      block_houseqr<N, OZ>(n, n, szt, q, r, wk, S);
+      block_houseqr<N, OZ>(n, n, szt, q, r, ywpt, wk + dense_work_numbers(n, szt) * W, S, panel);
       zeroQ = 0;
       block_invert_tiles<N>(n, szt, r, n, tinv);
       tinv_ok = true;
@@ -147,13 +155,24 @@ __global__ void __launch_bounds__(kDenseThreads)
   }
 }
 
+// Stage the WY panels and the column panel of R in shared memory?  When
+// they fit in 200 KB (knob 3 of phc_tune_set: 1 never, 2 whenever they fit).
+static bool dense_stage(int n, int szt, int W) {
+  const long staged = dense_smem_doubles_staged(n, szt, W) * (long)sizeof(double);
+  const int knob = tune_get(kTuneDenseStage);
+  if (knob == 1 || staged > 227L * 1024 - 1024) return false;
+  return knob == 2 || staged <= 200L * 1024;
+}
+
 template <class N>
 static int qr_launch(int ninst, int n, int ncols, int szt, const double *A, double *Q, double *R, double *work,
                      cudaStream_t st, bool oz) {
-  const long smem = dense_smem_doubles(n, szt, N::width) * sizeof(double);
+  const int stage = dense_stage(n, szt, N::width) ? 1 : 0;
+  const long smem = (stage ? dense_smem_doubles_staged(n, szt, N::width) : dense_smem_doubles(n, szt, N::width)) *
+                    (long)sizeof(double);
   auto kern = oz ? k_blocked_houseqr<N, true> : k_blocked_houseqr<N, false>;
   PHC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  kern<<<ninst, kDenseThreads, smem, st>>>(n, ncols, szt, A, Q, R, work);
+  kern<<<ninst, kDenseThreads, smem, st>>>(n, ncols, szt, A, Q, R, work, stage);
   PHC_CHECK_LAUNCH();
   return PHC_OK;
 }
@@ -257,10 +276,12 @@ static int tabs_launch(int ninst, int dim, int szt, double *U, double *b, double
 template <class N>
 static int bals_launch(int ninst, int n, int degp1, int szt, int tailidx, const double *mat, double *rhs, double *sol,
                        double *Q, double *R, int *flags, double *work, cudaStream_t st, bool oz) {
-  const long smem = dense_smem_doubles(n, szt, N::width) * sizeof(double);
+  const int stage = dense_stage(n, szt, N::width) ? 1 : 0;
+  const long smem = (stage ? dense_smem_doubles_staged(n, szt, N::width) : dense_smem_doubles(n, szt, N::width)) *
+                    (long)sizeof(double);
   auto kern = oz ? k_bals_solve<N, true> : k_bals_solve<N, false>;
   PHC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  kern<<<ninst, kDenseThreads, smem, st>>>(n, degp1, szt, tailidx, mat, rhs, sol, Q, R, flags, work);
+  kern<<<ninst, kDenseThreads, smem, st>>>(n, degp1, szt, tailidx, mat, rhs, sol, Q, R, flags, work, stage);
   PHC_CHECK_LAUNCH();
   return PHC_OK;
 }

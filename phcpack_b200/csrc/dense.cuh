@@ -125,6 +125,11 @@ __device__ dense_smem carve(double *sm, int n, int szt) {
   return s;
 }
 __host__ __device__ inline long dense_smem_doubles(int n, int szt, int W) { return (long)(3 * n + szt + 40) * W; }
+// with the WY panels (Y, W, P, T) and the current column panel of R staged
+// in shared memory as well
+__host__ __device__ inline long dense_smem_doubles_staged(int n, int szt, int W) {
+  return dense_smem_doubles(n, szt, W) + 5L * n * szt * W;
+}
 
 // Workspace in global memory per instance (numbers): Y, W, P (szt x n each),
 // T (n x szt) and the inverted diagonal tiles of R (n x szt).
@@ -210,9 +215,12 @@ __device__ void block_house(int m, const double *col, long ld, dense_smem &S) {
 }
 
 // R[c.., c..e) <- (I - beta v v^H) R[c.., c..e): w_j = beta sum_i conj(R_ij) v_i,
-// R_ij -= v_i conj(w_j)   (Matrices/dbl2_factorizations.cpp:534/:567)
+// R_ij -= v_i conj(w_j)   (Matrices/dbl2_factorizations.cpp:534/:567).
+// Entry (i, j) of R sits at Rm[(i - r0) * ld + (j - c0)]: the whole matrix
+// (r0 = c0 = 0, ld = ncols) or a panel of it staged in shared memory.
 template <class N>
-__device__ void block_apply_reflector(int n, int ncols, int c, int e, double *Rm, dense_smem &S) {
+__device__ void block_apply_reflector(int n, long ld, int c, int e, double *Rm, dense_smem &S, int r0 = 0,
+                                      int c0 = 0) {
   typedef typename N::T T;
   typedef typename N::real R;
   typedef md::num<R, false> RN;
@@ -224,7 +232,7 @@ __device__ void block_apply_reflector(int n, int ncols, int c, int e, double *Rm
     T acc = N::zero();
     if (j < e)
       for (int i = c + part; i < n; i += 4)
-        acc = N::add(acc, N::mul(N::conj(ldn_at<N>(Rm, (long)i * ncols + j)), ldn_at<N>(S.v, i - c)));
+        acc = N::add(acc, N::mul(N::conj(ldn_at<N>(Rm, (long)(i - r0) * ld + (j - c0))), ldn_at<N>(S.v, i - c)));
     acc = group4_sum<N>(acc);
     if (j < e && part == 0) stn_at<N>(S.w, j - c, N::scale(acc, beta));
   }
@@ -232,7 +240,7 @@ __device__ void block_apply_reflector(int n, int ncols, int c, int e, double *Rm
   const int nc = e - c;
   for (int t = threadIdx.x; t < (n - c) * nc; t += blockDim.x) {
     const int i = c + t / nc, j = c + t % nc;
-    const long o = (long)i * ncols + j;
+    const long o = (long)(i - r0) * ld + (j - c0);
     stn_at<N>(Rm, o, N::sub(ldn_at<N>(Rm, o), N::mul(ldn_at<N>(S.v, i - c), N::conj(ldn_at<N>(S.w, j - c)))));
   }
   __syncthreads();
@@ -244,12 +252,17 @@ __device__ void block_apply_reflector(int n, int ncols, int c, int e, double *Rm
 // the szt reflectors are applied to the panel column by column, then
 // W = -B (I + W Y^H) Y column by column (:13), the trailing columns get
 // R <- R + Y (W^H R) and Q <- Q + (Q W) Y^H.  R must hold A on entry.
-// work: dense_work_numbers(n, szt) numbers of this instance; with OZ (real
-// numbers only) the four trailing products run as Ozaki-split products on
-// the FP64 tensor cores (ozaki.cuh) in ozaki_work_doubles more doubles
-// after that; complex numbers keep the CUDA-core products.
+// work: the WY panels Y, W, the product P and T (4 n szt numbers), in
+// shared memory when the kernel staged them there, else in the instance's
+// global workspace; panel: shared memory for the current column panel of R
+// (n szt numbers: rows rowoff.., the tile's szt columns), or nullptr to
+// factor the panel in place in global memory.  With OZ (real numbers only)
+// the four trailing products run as Ozaki-split products on the FP64 tensor
+// cores (ozaki.cuh) with the scratch oz (ozaki_work_doubles, global);
+// complex numbers keep the CUDA-core products.
 template <class N, bool OZ = false>
-__device__ void block_houseqr(int n, int ncols, int szt, double *Q, double *Rm, double *work, dense_smem &S) {
+__device__ void block_houseqr(int n, int ncols, int szt, double *Q, double *Rm, double *work, double *oz,
+                              dense_smem &S, double *panel = nullptr) {
   typedef typename N::T T;
   typedef typename N::real R;
   typedef md::num<R, false> RN;
@@ -268,13 +281,28 @@ __device__ void block_houseqr(int n, int ncols, int szt, double *Q, double *Rm, 
     const int rowoff = k * szt;
     const int m = n - rowoff;
     const int endcol = (k + 1) * szt;
+    if (panel) {  // the tile's columns, rows rowoff.., into shared memory
+      for (int t = threadIdx.x; t < m * szt; t += blockDim.x)
+        stn_at<N>(panel, t, ldn_at<N>(Rm, (long)(rowoff + t / szt) * ncols + rowoff + t % szt));
+      __syncthreads();
+    }
     for (int L = 0; L < szt; ++L) {
       const int c = rowoff + L;
-      block_house<N>(n - c, Rm + (long)c * ncols * W + (long)c * W, ncols, S);
-      block_apply_reflector<N>(n, ncols, c, endcol, Rm, S);
+      if (panel) {
+        block_house<N>(n - c, panel + ((long)L * szt + L) * W, szt, S);
+        block_apply_reflector<N>(n, szt, c, endcol, panel, S, rowoff, rowoff);
+      } else {
+        block_house<N>(n - c, Rm + (long)c * ncols * W + (long)c * W, ncols, S);
+        block_apply_reflector<N>(n, ncols, c, endcol, Rm, S);
+      }
       if (threadIdx.x == 0) stn_at<RN>(S.beta, L, ldn_at<RN>(S.misc, 0));
       for (int i = threadIdx.x; i < m; i += blockDim.x)
         stn_at<N>(Y, (long)L * m + i, (i < L) ? N::zero() : ldn_at<N>(S.v, i - L));
+      __syncthreads();
+    }
+    if (panel) {
+      for (int t = threadIdx.x; t < m * szt; t += blockDim.x)
+        stn_at<N>(Rm, (long)(rowoff + t / szt) * ncols + rowoff + t % szt, ldn_at<N>(panel, t));
       __syncthreads();
     }
     // W from the betas and Y (Matrices/dbl2_baqr_host.cpp:13)
@@ -306,7 +334,6 @@ __device__ void block_houseqr(int n, int ncols, int szt, double *Q, double *Rm, 
       }
     }
     if constexpr (OZ && !N::is_complex) {
-      double *oz = work + dense_work_numbers(n, szt) * W;
       if (k < nbt - 1) {
         const int nc = ncols - endcol;
         // P = W^T C, then C += Y^T P

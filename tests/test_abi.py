@@ -41,11 +41,11 @@ def test_abi_version():
 def test_tuning_knobs_set_get_and_reject():
     # host-side state only: no device work
     lib = _lib.lib()
-    for knob, good, bad in ((0, 4, 9), (1, 2, 3), (2, 6, 33)):
+    for knob, good, bad in ((0, 4, 9), (1, 2, 3), (2, 6, 33), (3, 2, 3)):
         assert _lib.call("phc_tune_set", knob, good) == 0
         assert _lib.call("phc_tune_get", knob) == good
         assert lib.phc_tune_set(knob, bad) < 0
         assert _lib.call("phc_tune_get", knob) == good
         assert _lib.call("phc_tune_set", knob, 0) == 0
-    assert lib.phc_tune_set(3, 1) < 0 and lib.phc_tune_get(-1) < 0
+    assert lib.phc_tune_set(4, 1) < 0 and lib.phc_tune_get(-1) < 0
     assert lib.phc_tune_set(0, -1) < 0

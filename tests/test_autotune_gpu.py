@@ -82,7 +82,9 @@ def test_bals_tile_choice_is_valid_and_accurate():
     stream = torch.cuda.Stream()
     res = autotune.tune_bals_tile(torch, stream, prec, cplx, ninst, n, degp1, mat, rhs0, sol, Q, R, flags, flag0,
                                   work, wy=0, reps=1)
-    assert res["choice"] in (8, 16, 32) and set(res["seconds"]) == {8, 16, 32}
+    assert res["choice"] in (8, 16, 32) and res["stage"] in (1, 2)
+    assert set(res["seconds"]) == {f"{t}/{g}" for t in (8, 16, 32) for g in (1, 2)}
+    assert autotune.get_knob(autotune.KNOB_DENSE_STAGE) == res["stage"]
     # the solution with the chosen tile against the oracle
     sol_t, _ = dense.bals_solve_wy(prec, cplx, mat.cpu().numpy(), rhs0.cpu().numpy(), ninst, n, degp1,
                                    res["choice"], wy=0)
@@ -93,3 +95,21 @@ def test_bals_tile_choice_is_valid_and_accurate():
         s = lead(so, prec, cplx).reshape(degp1, n).max(axis=1)
         err = absdiff(got, so, prec, cplx).reshape(degp1, n).max(axis=1)
         assert np.all(err <= 1e4 * 1e-28 * np.maximum(1.0, s)), (q, err, s)
+
+
+@pytest.mark.parametrize("prec,cplx,n,szt", [(4, False, 64, 16), (2, True, 32, 8), (2, False, 64, 32)])
+def test_staged_panels_give_the_same_solution(prec, cplx, n, szt):
+    """The least squares with the WY panels and the column panel of R in
+    shared memory (knob 3 = 2) equals the one with them in global memory
+    (knob 3 = 1) bit for bit: the same operations in the same order."""
+    degp1, ninst = 3, 6
+    rng = np.random.default_rng(n + szt)
+    mat = np.concatenate([wl.random_numbers(rng, (degp1, n, n), prec, cplx, "normal").reshape(-1)
+                          for _ in range(ninst)])
+    rhs = np.concatenate([wl.random_numbers(rng, (degp1, n), prec, cplx, "normal").reshape(-1) for _ in range(ninst)])
+    out = {}
+    for g in (1, 2):
+        autotune.set_knob(autotune.KNOB_DENSE_STAGE, g)
+        out[g] = dense.bals_solve_host(prec, cplx, mat, rhs, ninst, n, degp1, szt)
+    for a, b in zip(out[1], out[2]):
+        assert np.array_equal(a, b)
