@@ -44,10 +44,9 @@ int phc_abi_version(void);
  *   knob 2: paths the tracker runs at once per SM, 1..32, at most what the
  *           occupancy allows (the rule: that maximum); the work queue hands
  *           out the other paths as paths finish;
- *   knob 3: blocked QR and least squares: 1 keeps the WY panels and the
- *           column panel of R in global memory, 2 stages them in shared
- *           memory whenever they fit (the rule: staged when they fit in
- *           200 KB, as for n = 64 and tile 16 in quad-double).
+ *   knob 3: blocked QR and least squares: 2 stages the WY panels and the
+ *           column panel of R in shared memory when they fit (one CTA per
+ *           SM), 0 or 1 keeps them in global memory (the rule: global).
  * phc_tune_get returns the value (>= 0) or an error. */
 int phc_tune_set(int knob, int value);
 int phc_tune_get(int knob);
@@ -244,8 +243,13 @@ int phc_newton_host(int prec, int cplx, int nsys, int dim, int deg, int szt, int
  *   and of the corrector's Jacobian and linear solves; the corrector's
  *   residuals and updates are double-double; rmode: refinement precision 2,
  *   4 (quad-double) or 8 (octo-double), all of its arithmetic.
- * step_mode 1 with a model (phc_mlp_*) uses the learned step proposer; a
- *   proposal whose feedback or corrector fails is redone with the plain step.
+ * step_mode: bit 1 (value 1) with a model (phc_mlp_*) uses the learned step
+ *   proposer; a proposal whose feedback or corrector fails is redone with
+ *   the plain step.  Bit 2 (value 2, pmode 1 only): the predictor inverts
+ *   J_0 by Householder QR in double (the reflectors of the reference's
+ *   complex convention, applied column by column) instead of LU, the QR
+ *   solve of the power-series Newton step (Newton/dbl2_newton_method.cpp
+ *   :429) in the predictor's double precision.
  * Output per path: xend maxdim complex quad-doubles, octo-doubles for rmode
  *   8 (lower limbs zero below rmode), info[6p..6p+5] = status (0 success,
  *   1 step below minsize, 2 maxsteps reached, 3 endpoint residual above

@@ -33,7 +33,9 @@
 //    counted as pole, curvature or maxsize step (Minimum,
 //    Curves/three_way_minima.adb:48-62); a step reaching 1 - minsize goes to
 //    t = 1 (Bounded_Update, three_way_minima.adb:96-109);
-//  * step_mode 1: the learned proposal plain step * exp(network(features))
+//  * step_mode bit 2 (double predictor): J_0 inverted by Householder QR
+//    (qr_inverse) instead of LU;
+//  * step_mode bit 1: the learned proposal plain step * exp(network(features))
 //    (the BF16 network of the model buffer, evaluated in float in the
 //    device's order of operations); a proposal whose feedback or corrector
 //    fails is redone with the plain step;
@@ -83,6 +85,9 @@ struct TrackPar {
 };
 
 template <class R> static cx<R> cplx(double re, double im) { return cx<R>(R(re), R(im)); }
+
+template <class T> struct is_double { static const bool v = false; };
+template <> struct is_double<cx<double> > { static const bool v = true; };
 
 // Evaluate h and, when jac != nullptr, J at a vector of series x (dim
 // series of degree w) at t = t0 + s: value series h[i][k], Jacobian series
@@ -256,6 +261,67 @@ template <class T> struct lu_solver {
   }
 };
 
+// M = A^{-1} by Householder QR (step_mode bit 2 of the double predictor),
+// the operations in the order of the GPU's warp_qrinverse: column k takes
+// sigma = sum_{i>k} |a_ik|^2, nu = sqrt(|a_kk|^2 + sigma), phase phi =
+// a_kk/|a_kk| (1 for a_kk = 0), v = (a_kk + phi nu, a_{k+1,k}, ...), tau =
+// 2/|v|^2, r_kk = -phi nu, then a_j -= tau v (v^H a_j) for j > k; M = Q^H
+// from the identity, then R X = M by back substitution.
+static void qr_inverse(int n, const std::vector<cx<double> > &A0, std::vector<cx<double> > &M) {
+  typedef cx<double> T;
+  typedef double R;
+  std::vector<T> a(A0.begin(), A0.begin() + (long)n * n), vk(n);
+  std::vector<R> tau(n, R(0.0));
+  for (int k = 0; k < n; ++k) {
+    R sig = R(0.0);
+    for (int i = k + 1; i < n; ++i) sig = sig + norm2(a[(long)i * n + k]);
+    const T xk = a[(long)k * n + k];
+    const R a2 = norm2(xk);
+    const R nu = std::sqrt(a2 + sig);
+    T v0, rkk;
+    R t = R(0.0);
+    if (nu != R(0.0)) {
+      T phi = T(R(1.0));
+      if (a2 != R(0.0)) {
+        const R ab = std::sqrt(a2);
+        phi = T(xk.re / ab, xk.im / ab);
+      }
+      v0 = T(xk.re + phi.re * nu, xk.im + phi.im * nu);
+      t = R(2.0) / (norm2(v0) + sig);
+      rkk = T(-(phi.re * nu), -(phi.im * nu));
+    }
+    vk[k] = v0;
+    tau[k] = t;
+    a[(long)k * n + k] = rkk;
+    for (int j = k + 1; j < n; ++j) {
+      T w = conj(v0) * a[(long)k * n + j];
+      for (int i = k + 1; i < n; ++i) w = w + conj(a[(long)i * n + k]) * a[(long)i * n + j];
+      w = T(w.re * t, w.im * t);
+      a[(long)k * n + j] = a[(long)k * n + j] - v0 * w;
+      for (int i = k + 1; i < n; ++i) a[(long)i * n + j] = a[(long)i * n + j] - a[(long)i * n + k] * w;
+    }
+  }
+  M.assign((long)n * n, T());
+  for (int c = 0; c < n; ++c) {
+    for (int i = 0; i < n; ++i) M[(long)i * n + c] = (i == c) ? T(R(1.0)) : T();
+    for (int k = 0; k < n; ++k) {
+      const R t = tau[k];
+      if (t == R(0.0)) continue;
+      const T v0 = vk[k];
+      T w = conj(v0) * M[(long)k * n + c];
+      for (int i = k + 1; i < n; ++i) w = w + conj(a[(long)i * n + k]) * M[(long)i * n + c];
+      w = T(w.re * t, w.im * t);
+      M[(long)k * n + c] = M[(long)k * n + c] - v0 * w;
+      for (int i = k + 1; i < n; ++i) M[(long)i * n + c] = M[(long)i * n + c] - a[(long)i * n + k] * w;
+    }
+    for (int i = n - 1; i >= 0; --i) {
+      T acc = M[(long)i * n + c];
+      for (int j = i + 1; j < n; ++j) acc = acc - a[(long)i * n + j] * M[(long)j * n + c];
+      M[(long)i * n + c] = acc / a[(long)i * n + i];
+    }
+  }
+}
+
 // The predictor's Taylor series: x[i] series of degree K, on entry the
 // constant terms hold the current point.  x_k = -J_0^{-1} [h(x truncated
 // below degree k)]_k for k = 1..K, with J_0 factored once by lufac and
@@ -273,8 +339,15 @@ static void taylor_series(const TrackSys &S, int s, const TrackPar &P, double t0
     std::vector<std::vector<T> > x0(n, std::vector<T>(1));
     for (int i = 0; i < n; ++i) x0[i][0] = x[i][0];
     hom_eval(S, s, 0, t0, x0, h, &jac);
-    lu.factor(n, jac);
-    lu.inverse(M);
+    bool by_qr = false;
+    if constexpr (is_double<T>::v) {
+      by_qr = (P.step_mode & 2) != 0;
+      if (by_qr) qr_inverse(n, jac, M);
+    }
+    if (!by_qr) {
+      lu.factor(n, jac);
+      lu.inverse(M);
+    }
   }
   for (int k = 1; k <= K; ++k) {
     std::vector<std::vector<T> > xw(n, std::vector<T>(k + 1));
@@ -581,7 +654,7 @@ static PathOut track_path(const TrackSys &S, int s, const TrackPar &P, const dou
   std::vector<PT> xp(n);
   std::vector<double> ax(n), rabs, mag((size_t)n * (K + 1));
   std::vector<int> pdeg(n), qdeg(n);
-  const bool use_model = P.step_mode == 1 && P.model != nullptr;
+  const bool use_model = (P.step_mode & 1) && P.model != nullptr;
   bool failed = false;
   int k;
   for (k = 0; k < P.maxsteps; ++k) {
@@ -957,8 +1030,9 @@ int orc_track(int nsys, const int *dim, int maxvar, const int *mono_off, const i
   P.learn_scale = dpar[7] > 0.0 ? dpar[7] : 1.0;
   P.cbeta = dpar[8];
   P.step_mode = step_mode;
-  P.model = step_mode == 1 ? static_cast<const unsigned char *>(model) : nullptr;
+  P.model = (step_mode & 1) ? static_cast<const unsigned char *>(model) : nullptr;
   if (P.numdeg + P.dendeg != P.deg || P.deg < 3 || !(P.cbeta > 0.0)) return -1;
+  if (step_mode < 0 || step_mode > 3 || ((step_mode & 2) && pmode != 1)) return -1;
   // rmode 1 (with pmode 1): everything in double, the FP64 run the
   // multiple-double results are compared with
   if ((pmode != 1 && pmode != 2) || (rmode != 1 && rmode != 2 && rmode != 4 && rmode != 8)) return -1;

@@ -139,7 +139,7 @@ int phc_track(int nsys, const int *dim, int maxvar, int maxdim, int nmono_max, c
   TrackDev S{nsys,      maxvar, maxdim, dim,    mono_off, mono_nvr, mono_idx, mono_exp,    eq_off,
              term_off,  term_mono, term_a, term_b, jg_off,  jg_term,  jg_slot,  gstaged != 0};
   return track(S, make_par(ipar, dpar, step_mode), nmono_max, npaths, path_sys, x0, pmode, rmode,
-               step_mode ? model : nullptr, xend, info, dinfo, log, log_cap, log_count, queue, one_per_launch,
+               (step_mode & 1) ? model : nullptr, xend, info, dinfo, log, log_cap, log_count, queue, one_per_launch,
                (cudaStream_t)stream);
 }
 
@@ -175,7 +175,7 @@ int phc_track_host(int nsys, const int *dim, int maxvar, const int *mono_off, co
       {term_off, (neq + 1) * 4ul}, {term_mono, nterm * 4ul}, {term_a, nterm * 16ul}, {term_b, nterm * 16ul},
       {jg_off.data(), jg_off.size() * 4}, {jg_term.data(), jg_term.size() * 4}, {jg_slot.data(), jg_slot.size() * 4},
       {path_sys, npaths * 4ul}, {x0, (size_t)npaths * maxdim * 16},
-      {model, step_mode && model ? (size_t)mlp_model_bytes() : 0ul}};
+      {model, (step_mode & 1) && model ? (size_t)mlp_model_bytes() : 0ul}};
   size_t total = 0;
   std::vector<size_t> off;
   for (size_t i = 0; i < ins.size(); ++i) {
@@ -229,7 +229,7 @@ int phc_track_host(int nsys, const int *dim, int maxvar, const int *mono_off, co
     auto Dp = [&](int i) { return (const double *)(b + off[i]); };
     out = phc_track(nsys, I(0), maxvar, maxdim, nmono_max, I(1), I(2), I(3), I(4), I(5), I(6), I(7), Dp(8), Dp(9),
                     I(10), I(11), I(12), staged, npaths, I(13), Dp(14), ipar, dpar, pmode, rmode, step_mode,
-                    step_mode && model ? (const void *)(b + off[15]) : nullptr, (double *)(b + o_xend),
+                    (step_mode & 1) && model ? (const void *)(b + off[15]) : nullptr, (double *)(b + o_xend),
                     (int *)(b + o_info), (double *)(b + o_dinfo), nullptr, 0, nullptr, (int *)(b + o_q), 0, st);
   }
   if (out == PHC_OK) {

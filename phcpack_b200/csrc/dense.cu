@@ -155,13 +155,14 @@ __global__ void __launch_bounds__(kDenseThreads)
   }
 }
 
-// Stage the WY panels and the column panel of R in shared memory?  When
-// they fit in 200 KB (knob 3 of phc_tune_set: 1 never, 2 whenever they fit).
+// Stage the WY panels and the column panel of R in shared memory?  Only on
+// request (knob 3 of phc_tune_set = 2) and when they fit: the staged kernel
+// runs one CTA per SM where the unstaged one runs two, and on the
+// quad-double least squares of dimension 64 (tile 16) it measured 38 %
+// slower (65.1 against 47.3 ms for 512 instances); the autotuner times both.
 static bool dense_stage(int n, int szt, int W) {
   const long staged = dense_smem_doubles_staged(n, szt, W) * (long)sizeof(double);
-  const int knob = tune_get(kTuneDenseStage);
-  if (knob == 1 || staged > 227L * 1024 - 1024) return false;
-  return knob == 2 || staged <= 200L * 1024;
+  return tune_get(kTuneDenseStage) == 2 && staged <= 227L * 1024 - 1024;
 }
 
 template <class N>

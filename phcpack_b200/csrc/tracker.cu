@@ -23,6 +23,8 @@ int track_check(const TrackParDev &P, int pmode, int rmode, int maxdim) {
   PHC_REQUIRE(P.deg >= 3 && P.deg <= kTrackKmax && P.numdeg + P.dendeg == P.deg && P.dendeg <= 8 && P.nit >= 1,
               "track: need 3 <= deg = numdeg + dendeg <= %d, dendeg <= 8", kTrackKmax);
   PHC_REQUIRE(P.cbeta > 0.0 && P.cbeta < INFINITY, "track: cbeta %g is not positive", P.cbeta);
+  PHC_REQUIRE(P.step_mode >= 0 && P.step_mode <= 3, "track: step_mode %d not in 0..3", P.step_mode);
+  PHC_REQUIRE(!(P.step_mode & 2) || pmode == 1, "track: the QR predictor (step_mode bit 2) needs pmode 1");
   return PHC_OK;
 }
 

@@ -417,9 +417,10 @@ __device__ TRACK_FN void hom_coef_cta(const TrackDev &S, int s, int k, double t0
 // limbs), rows k and ell swap in columns k..n-1, and the multipliers
 // -a_ik / a_kk overwrite column k below the diagonal.  Besides ipvt the
 // reciprocals dinv[k] = 1 / u_kk are kept for the back substitution (NaN
-// for a zero pivot).  One warp alone (lanes over the rows for the pivot and
-// the multipliers, over the entries for the trailing update): no CTA
-// barrier, the other warps of the CTA stay free.  Called by all lanes of the warp;
+// for a zero pivot).  One warp alone (lanes over the rows for the pivot, the
+// multipliers and the trailing update, each lane the columns of its row):
+// no CTA barrier, the other warps of the CTA stay free.  Called by all lanes
+// of the warp;
 // returns info to every lane: 0, or k + 1 for the first column k without a
 // nonzero pivot.
 template <class N>
@@ -456,14 +457,16 @@ __device__ TRACK_FN int warp_lufac(int n, double *A, int *ipvt, double *dinv) {
     __syncwarp();
     const T inv = N::div(N::one(), ldn_at<N>(A, (long)k * n + k));
     if (lane == 0) stn_at<N>(dinv, k, inv);
-    if (lane > k && lane < n) stn_at<N>(A, (long)lane * n + k, N::mul(N::neg(inv), ldn_at<N>(A, (long)lane * n + k)));
-    __syncwarp();
-    // trailing update, the (n-k-1)^2 entries spread over the lanes
-    const int m = n - k - 1;
-    for (int e = lane; e < m * m; e += 32) {
-      const int i = k + 1 + e / m, j = k + 1 + e % m;
-      const long o = (long)i * n + j;
-      stn_at<N>(A, o, N::add(ldn_at<N>(A, o), N::mul(ldn_at<N>(A, (long)k * n + j), ldn_at<N>(A, (long)i * n + k))));
+    // lane i - k - 1 forms the multiplier of row i > k and updates the row
+    // (the row's entries are independent: no index arithmetic by division)
+    const int i = k + 1 + lane;
+    if (i < n) {
+      const T l = N::mul(N::neg(inv), ldn_at<N>(A, (long)i * n + k));
+      stn_at<N>(A, (long)i * n + k, l);
+      for (int j = k + 1; j < n; ++j) {
+        const long o = (long)i * n + j;
+        stn_at<N>(A, o, N::add(ldn_at<N>(A, o), N::mul(ldn_at<N>(A, (long)k * n + j), l)));
+      }
     }
     __syncwarp();
   }
@@ -517,11 +520,13 @@ __device__ TRACK_FN void warp_luinverse(int n, const double *A, const int *ipvt,
         stn_at<N>(M, (long)k * n + c, t);
       }
     __syncwarp();
-    const int m = n - k - 1;
-    for (int e = lane; e < m * n; e += 32) {
-      const int i = k + 1 + e / n, c = e % n;
-      const long o = (long)i * n + c;
-      stn_at<N>(M, o, N::add(ldn_at<N>(M, o), N::mul(ldn_at<N>(M, (long)k * n + c), ldn_at<N>(A, (long)i * n + k))));
+    const int i = k + 1 + lane;  // lanes over the rows below k
+    if (i < n) {
+      const T l = ldn_at<N>(A, (long)i * n + k);
+      for (int c = 0; c < n; ++c) {
+        const long o = (long)i * n + c;
+        stn_at<N>(M, o, N::add(ldn_at<N>(M, o), N::mul(ldn_at<N>(M, (long)k * n + c), l)));
+      }
     }
     __syncwarp();
   }
@@ -529,13 +534,96 @@ __device__ TRACK_FN void warp_luinverse(int n, const double *A, const int *ipvt,
     for (int c = lane; c < n; c += 32)
       stn_at<N>(M, (long)kb * n + c, N::mul(ldn_at<N>(M, (long)kb * n + c), ldn_at<N>(dinv, kb)));
     __syncwarp();
-    for (int e = lane; e < kb * n; e += 32) {
-      const int j = e / n, c = e % n;
-      const long o = (long)j * n + c;
-      stn_at<N>(M, o, N::sub(ldn_at<N>(M, o), N::mul(ldn_at<N>(M, (long)kb * n + c), ldn_at<N>(A, (long)j * n + kb))));
+    if (lane < kb) {  // lanes over the rows above kb
+      const T u = ldn_at<N>(A, (long)lane * n + kb);
+      for (int c = 0; c < n; ++c) {
+        const long o = (long)lane * n + c;
+        stn_at<N>(M, o, N::sub(ldn_at<N>(M, o), N::mul(ldn_at<N>(M, (long)kb * n + c), u)));
+      }
     }
     __syncwarp();
   }
+}
+
+// M = A^{-1} by Householder QR, for the predictor's J_0 in complex double
+// (step_mode bit 2: the predictor's solves by QR instead of LU).  Column k:
+// sigma = sum_{i>k} |a_ik|^2, nu = sqrt(|a_kk|^2 + sigma), phase phi =
+// a_kk / |a_kk| (1 for a_kk = 0), reflector I - tau v v^H with v = (a_kk +
+// phi nu, a_{k+1,k}, ...) and tau = 2 / |v|^2, r_kk = -phi nu; the other
+// columns j > k get a_j -= tau v (v^H a_j).  Then M = Q^H (the reflectors
+// applied to the identity in order) and R X = M by back substitution.  A
+// holds R on and above the diagonal and v below it on return; vk, tau: n
+// numbers of N and n reals of scratch (shared memory).  One warp: lane 0
+// forms each reflector, the lanes then own the columns (each column's sums
+// run over the rows in order), so the operations and their order are those
+// of a column-by-column solve.  A zero column leaves r_kk = 0 (tau = 0) and
+// the inverse infinite or NaN, as a zero pivot of the LU does.
+template <class N>
+__device__ TRACK_FN void warp_qrinverse(int n, double *A, double *M, double *vk, double *tau) {
+  typedef typename N::T T;
+  typedef typename N::real R;
+  typedef typename N::tr tr;
+  const int lane = threadIdx.x & 31;
+  for (int k = 0; k < n; ++k) {
+    if (lane == 0) {
+      R sig = tr::zero();
+      for (int i = k + 1; i < n; ++i) sig = tr::add(sig, N::norm2(ldn_at<N>(A, (long)i * n + k)));
+      const T xk = ldn_at<N>(A, (long)k * n + k);
+      const R a2 = N::norm2(xk);
+      const R nu = tr::sqrt(tr::add(a2, sig));
+      T v0 = N::zero(), rkk = N::zero();
+      R t = tr::zero();
+      if (nu != tr::zero()) {
+        T phi = N::one();
+        if (a2 != tr::zero()) {
+          const R ab = tr::sqrt(a2);
+          phi = N::mkc(tr::div(xk.re, ab), tr::div(xk.im, ab));
+        }
+        v0 = N::mkc(tr::add(xk.re, tr::mul(phi.re, nu)), tr::add(xk.im, tr::mul(phi.im, nu)));
+        t = tr::div(tr::from(2.0), tr::add(N::norm2(v0), sig));
+        rkk = N::mkc(tr::neg(tr::mul(phi.re, nu)), tr::neg(tr::mul(phi.im, nu)));
+      }
+      stn_at<N>(vk, k, v0);
+      tau[k] = t;
+      stn_at<N>(A, (long)k * n + k, rkk);
+    }
+    __syncwarp();
+    const T v0 = ldn_at<N>(vk, k);
+    const R t = tau[k];
+    for (int j = k + 1 + lane; j < n; j += 32) {  // lanes over the columns to the right
+      T w = N::mul(N::conj(v0), ldn_at<N>(A, (long)k * n + j));
+      for (int i = k + 1; i < n; ++i)
+        w = N::add(w, N::mul(N::conj(ldn_at<N>(A, (long)i * n + k)), ldn_at<N>(A, (long)i * n + j)));
+      w = N::mkc(tr::mul(w.re, t), tr::mul(w.im, t));
+      stn_at<N>(A, (long)k * n + j, N::sub(ldn_at<N>(A, (long)k * n + j), N::mul(v0, w)));
+      for (int i = k + 1; i < n; ++i)
+        stn_at<N>(A, (long)i * n + j, N::sub(ldn_at<N>(A, (long)i * n + j), N::mul(ldn_at<N>(A, (long)i * n + k), w)));
+    }
+    __syncwarp();
+  }
+  // M = Q^H = H_{n-1} ... H_0 I, lanes over the columns
+  for (int c = lane; c < n; c += 32) {
+    for (int i = 0; i < n; ++i) stn_at<N>(M, (long)i * n + c, i == c ? N::one() : N::zero());
+    for (int k = 0; k < n; ++k) {
+      const R t = tau[k];
+      if (t == tr::zero()) continue;
+      const T v0 = ldn_at<N>(vk, k);
+      T w = N::mul(N::conj(v0), ldn_at<N>(M, (long)k * n + c));
+      for (int i = k + 1; i < n; ++i)
+        w = N::add(w, N::mul(N::conj(ldn_at<N>(A, (long)i * n + k)), ldn_at<N>(M, (long)i * n + c)));
+      w = N::mkc(tr::mul(w.re, t), tr::mul(w.im, t));
+      stn_at<N>(M, (long)k * n + c, N::sub(ldn_at<N>(M, (long)k * n + c), N::mul(v0, w)));
+      for (int i = k + 1; i < n; ++i)
+        stn_at<N>(M, (long)i * n + c, N::sub(ldn_at<N>(M, (long)i * n + c), N::mul(ldn_at<N>(A, (long)i * n + k), w)));
+    }
+    // R X = Q^H, column c
+    for (int i = n - 1; i >= 0; --i) {
+      T acc = ldn_at<N>(M, (long)i * n + c);
+      for (int j = i + 1; j < n; ++j) acc = N::sub(acc, N::mul(ldn_at<N>(A, (long)i * n + j), ldn_at<N>(M, (long)j * n + c)));
+      stn_at<N>(M, (long)i * n + c, N::div(acc, ldn_at<N>(A, (long)i * n + i)));
+    }
+  }
+  __syncwarp();
 }
 
 // ------------------------------------------------------------ singular values
@@ -804,7 +892,7 @@ __device__ void cta_matvec(int n, const double *M, const double *b, double *y) {
 // Shared-memory layout of a path's CTA (in doubles)
 struct TrackLayout {
   long xs, V, G, hs, J0, M, r, num, den, xp, xc, hc, Jc, Vc, Gc, red, piv, dinv, feat, mag, degs, hbuf, svd, xd, sv,
-      part, padw, xa, total;
+      part, padw, xa, qrw, total;
 };
 
 // Matrices of the singular-value jobs of a predictor step: one per warp
@@ -838,6 +926,7 @@ __host__ __device__ inline TrackLayout track_layout(int n, int K, int M, int nm,
   L.xd = take(2L * n);
   L.sv = take(n + 2);
   L.xa = take(n);  // |x_i| of the predicted point (mixed residual)
+  L.qrw = take(3L * n);  // the predictor's Householder scratch (2n doubles of v_kk, n of tau)
   // scratch of the Taylor series and the predictor feedback ...
   const long ov = o;
   L.V = take(nm * 2 * Wp);  // two coefficients per monomial (point evaluations use one)

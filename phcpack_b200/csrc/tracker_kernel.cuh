@@ -20,8 +20,9 @@
 //     converged when max |dx| <= tolres, plus one extra step; on failure
 //     halve the step;
 //   the step size comes from a learned model when one is given (step_mode
-//     1): a proposal whose corrector fails is rejected and the step is
-//     redone with the plain pole step;
+//     bit 1): a proposal whose corrector fails is rejected and the step is
+//     redone with the plain pole step; step_mode bit 2 (double predictor):
+//     J_0 is inverted by Householder QR instead of LU;
 //   at t = 1: refinement in RN precision (double-, quad- or octo-double) and
 //     classification by the max-norm residual.
 // Every loop is bounded (maxsteps, halvings down to minsize); nothing waits.
@@ -218,8 +219,15 @@ __global__ void __launch_bounds__(kTrackThreads, (track_min_blocks<PN, RN, WIDE>
       // warps form the Hessians at the point and their Frobenius norms, upper
       // bounds of their largest singular values (sv[i] = |H_i|_F^2)
       if (ctid() < 32) {
-        warp_lufac<PN>(n, sm + L.J0, piv, dinv);
-        warp_luinverse<PN>(n, sm + L.J0, piv, dinv, sm + L.M);
+        bool by_qr = false;  // step_mode bit 2: J_0 by Householder QR (double predictor)
+        if constexpr (PN::width == 2) {
+          by_qr = (P.step_mode & 2) != 0;
+          if (by_qr) warp_qrinverse<PN>(n, sm + L.J0, sm + L.M, sm + L.qrw, sm + L.qrw + 2 * n);
+        }
+        if (!by_qr) {
+          warp_lufac<PN>(n, sm + L.J0, piv, dinv);
+          warp_luinverse<PN>(n, sm + L.J0, piv, dinv, sm + L.M);
+        }
       } else {
         const int hw = (ctid() >> 5), nhw = kTrackThreads / 32 - 1;
         for (int i = hw - 1; i < n; i += nhw) {
@@ -331,11 +339,11 @@ __global__ void __launch_bounds__(kTrackThreads, (track_min_blocks<PN, RN, WIDE>
       double step = plain_step;
       bool learned = false;
       float *feat = reinterpret_cast<float *>(sm + L.feat);
-      if ((P.step_mode == 1 && model != nullptr) || log != nullptr) {
+      if (((P.step_mode & 1) && model != nullptr) || log != nullptr) {
         track_features(ctid(), n, K, t, plain_step, sm + L.mag, feat);
         __syncthreads();
       }
-      if (P.step_mode == 1 && model != nullptr) {
+      if ((P.step_mode & 1) && model != nullptr) {
         const float lr = mlp_forward_cta(model, feat, reinterpret_cast<float *>(sm + L.hbuf));
         const double prop = plain_step * exp((double)lr) * P.learn_scale;
         if (prop > P.minsize && prop == prop) {

@@ -367,7 +367,7 @@ class DeviceTracker:
                   _lib.ptr(a["term_off"]), _lib.ptr(a["term_mono"]), _lib.ptr(a["term_a"]), _lib.ptr(a["term_b"]),
                   _lib.ptr(a["jg_off"]), _lib.ptr(a["jg_term"]), _lib.ptr(a["jg_slot"]), self.gstaged, pb.npaths,
                   _lib.ptr(a["path_sys"]), _lib.ptr(a["x0"]), _lib.ptr(ipar), _lib.ptr(dpar), pmode, rmode, step_mode,
-                  _lib.ptr(self.model) if (step_mode and self.model is not None) else _lib.c_void_p(0),
+                  _lib.ptr(self.model) if ((step_mode & 1) and self.model is not None) else _lib.c_void_p(0),
                   _lib.ptr(self.xend), _lib.ptr(self.info), _lib.ptr(self.dinfo),
                   _lib.ptr(self.log) if self.log is not None else _lib.c_void_p(0), self.log_cap,
                   _lib.ptr(self.log_count), _lib.ptr(self.queue), int(one_per_launch), _lib.c_void_p(s))

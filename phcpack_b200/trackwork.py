@@ -200,7 +200,9 @@ class TrackWork:
         """The three patterns apart on the same 1024 paths, each batched:
         all double-double with the plain step, the precision split with the
         plain step, the precision split with the learned step (the measured
-        arm), and the plain one-path-per-launch all-dd arrangement."""
+        arm), the measured arm with the predictor's J_0 inverted by
+        Householder QR instead of LU, and the plain one-path-per-launch
+        all-dd arrangement."""
         n = self.pb.npaths
         out = {}
         t, r = self.timed(self.dt, stream, pmode=2, rmode=2, step_mode=0)
@@ -213,6 +215,11 @@ class TrackWork:
             out["batched_split_learned_step"] = self.summary(n, t, r)
             out["batched_split_learned_step"]["same_classification_as_plain"] = bool(
                 np.array_equal(r.status == 0, plain_split.status == 0))
+        # the predictor's J_0 by Householder QR instead of LU (step_mode bit 2)
+        t, r = self.timed(self.dt, stream, pmode=1, rmode=2, step_mode=2 | (1 if self.step_mode else 0))
+        key = "batched_split_qr_predictor_" + ("learned_step" if self.step_mode else "plain_step")
+        out[key] = dict(self.summary(n, t, r), same_classification_as_plain=bool(
+            np.array_equal(r.status == 0, plain_split.status == 0)))
         tp, rp = self.plain(stream)
         out["plain_one_path_per_launch"] = dict(self.summary(n, tp, rp), same_classification=bool(
             np.array_equal(rp.status == 0, plain_split.status == 0)))

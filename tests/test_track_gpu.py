@@ -63,6 +63,36 @@ def test_track_config4_all_paths_vs_oracle(step_mode):
     assert ok.all()
 
 
+@pytest.mark.parametrize("step_mode", [2, 3])
+def test_track_qr_predictor_vs_oracle(step_mode):
+    """The predictor's J_0 inverted by Householder QR in double (step_mode
+    bit 2; with bit 1 the learned step as well) on 256 paths of the dense
+    quadratic n = 10 workload against the oracle's run with the same QR:
+    same classification, end points and step counts as for the LU predictor,
+    and the QR predictor's series agree with the LU predictor's (the step
+    counts of the two modes are close)."""
+    from phcpack_b200 import trackwork
+    pb = hm.subset(hm.config4(), np.arange(0, 1024, 4))
+    ipar, dpar = hm.params()
+    model = trackwork.load_model_bytes() if step_mode & 1 else None
+    g = hm.track_host(pb, pmode=1, rmode=2, step_mode=step_mode, model=model)
+    xo, io, _ = pyoracle.track(ORC, pb, ipar, dpar, pmode=1, rmode=2, nthreads=16, step_mode=step_mode,
+                               model=model)
+    ok = compare_with_oracle(pb, g, xo, io, max_step_diff=4)
+    assert ok.all()
+    lu = hm.track_host(pb, pmode=1, rmode=2, step_mode=step_mode & 1, model=model)
+    assert np.array_equal(lu.status, g.status)
+    assert abs(lu.steps.mean() - g.steps.mean()) <= 0.05 * lu.steps.mean()
+    assert (endpoint_diff(pb, g.xend, lu.xend, 2)[ok] <= 1e-26).all()
+
+
+def test_track_qr_predictor_needs_the_double_predictor():
+    from phcpack_b200 import _lib
+    pb = hm.subset(hm.config4(), np.arange(4))
+    with pytest.raises(_lib.PhcError):
+        hm.track_host(pb, pmode=2, rmode=2, step_mode=2)
+
+
 @pytest.mark.parametrize("pmode", [1, 2])
 def test_track_config4_sample_vs_oracle(pmode):
     pb = hm.subset(hm.config4(), np.arange(0, 1024, 16))

@@ -50,3 +50,25 @@ def test_oracle_tracker_all_dd_predictor_same_endpoints():
     e1 = x1.reshape(-1, 8)
     e2 = x2.reshape(-1, 8)
     assert np.abs((e1[:, 0] - e2[:, 0]) + (e1[:, 1] - e2[:, 1])).max() < 1e-26
+
+
+def test_oracle_qr_predictor_matches_lu_predictor():
+    """The oracle's predictor with J_0 inverted by Householder QR (step_mode
+    bit 2) reaches the same end points as with LU, in about as many steps:
+    both give J_0^{-1} to double accuracy, only their rounding differs."""
+    pb = hm.subset(hm.config4(), np.arange(0, 1024, 128))
+    ipar, dpar = hm.params()
+    xl, il, dl = pyoracle.track(ORC, pb, ipar, dpar, pmode=1, rmode=2, nthreads=4, step_mode=0)
+    xq, iq, dq = pyoracle.track(ORC, pb, ipar, dpar, pmode=1, rmode=2, nthreads=4, step_mode=2)
+    il, iq = il.reshape(-1, 6), iq.reshape(-1, 6)
+    assert (iq[:, 0] == 0).all() and (il[:, 0] == 0).all()
+    assert np.abs(iq[:, 1] - il[:, 1]).max() <= 3
+    a = xl.reshape(-1, pb.maxdim, 8)
+    b = xq.reshape(-1, pb.maxdim, 8)
+    for part in (0, 4):
+        d = (a[..., part] - b[..., part]) + (a[..., part + 1] - b[..., part + 1])
+        assert np.abs(d).max() <= 1e-26
+    # the QR mode is refused with the double-double predictor
+    import pytest
+    with pytest.raises(AssertionError):
+        pyoracle.track(ORC, pb, ipar, dpar, pmode=2, rmode=2, nthreads=1, step_mode=2)
