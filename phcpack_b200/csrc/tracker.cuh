@@ -417,10 +417,10 @@ __device__ TRACK_FN void hom_coef_cta(const TrackDev &S, int s, int k, double t0
 // limbs), rows k and ell swap in columns k..n-1, and the multipliers
 // -a_ik / a_kk overwrite column k below the diagonal.  Besides ipvt the
 // reciprocals dinv[k] = 1 / u_kk are kept for the back substitution (NaN
-// for a zero pivot).  One warp alone (lanes over the rows for the pivot, the
-// multipliers and the trailing update, each lane the columns of its row):
-// no CTA barrier, the other warps of the CTA stay free.  Called by all lanes
-// of the warp;
+// for a zero pivot).  One warp alone (lanes over the rows for the pivot and
+// the multipliers, over the entries for the trailing update; a lane per row
+// with its row's columns in turn measured slower): no CTA barrier, the other
+// warps of the CTA stay free.  Called by all lanes of the warp;
 // returns info to every lane: 0, or k + 1 for the first column k without a
 // nonzero pivot.
 template <class N>
@@ -457,16 +457,14 @@ __device__ TRACK_FN int warp_lufac(int n, double *A, int *ipvt, double *dinv) {
     __syncwarp();
     const T inv = N::div(N::one(), ldn_at<N>(A, (long)k * n + k));
     if (lane == 0) stn_at<N>(dinv, k, inv);
-    // lane i - k - 1 forms the multiplier of row i > k and updates the row
-    // (the row's entries are independent: no index arithmetic by division)
-    const int i = k + 1 + lane;
-    if (i < n) {
-      const T l = N::mul(N::neg(inv), ldn_at<N>(A, (long)i * n + k));
-      stn_at<N>(A, (long)i * n + k, l);
-      for (int j = k + 1; j < n; ++j) {
-        const long o = (long)i * n + j;
-        stn_at<N>(A, o, N::add(ldn_at<N>(A, o), N::mul(ldn_at<N>(A, (long)k * n + j), l)));
-      }
+    if (lane > k && lane < n) stn_at<N>(A, (long)lane * n + k, N::mul(N::neg(inv), ldn_at<N>(A, (long)lane * n + k)));
+    __syncwarp();
+    // trailing update, the (n-k-1)^2 entries spread over the lanes
+    const int m = n - k - 1;
+    for (int e = lane; e < m * m; e += 32) {
+      const int i = k + 1 + e / m, j = k + 1 + e % m;
+      const long o = (long)i * n + j;
+      stn_at<N>(A, o, N::add(ldn_at<N>(A, o), N::mul(ldn_at<N>(A, (long)k * n + j), ldn_at<N>(A, (long)i * n + k))));
     }
     __syncwarp();
   }
@@ -520,13 +518,11 @@ __device__ TRACK_FN void warp_luinverse(int n, const double *A, const int *ipvt,
         stn_at<N>(M, (long)k * n + c, t);
       }
     __syncwarp();
-    const int i = k + 1 + lane;  // lanes over the rows below k
-    if (i < n) {
-      const T l = ldn_at<N>(A, (long)i * n + k);
-      for (int c = 0; c < n; ++c) {
-        const long o = (long)i * n + c;
-        stn_at<N>(M, o, N::add(ldn_at<N>(M, o), N::mul(ldn_at<N>(M, (long)k * n + c), l)));
-      }
+    const int m = n - k - 1;
+    for (int e = lane; e < m * n; e += 32) {
+      const int i = k + 1 + e / n, c = e % n;
+      const long o = (long)i * n + c;
+      stn_at<N>(M, o, N::add(ldn_at<N>(M, o), N::mul(ldn_at<N>(M, (long)k * n + c), ldn_at<N>(A, (long)i * n + k))));
     }
     __syncwarp();
   }
@@ -534,12 +530,10 @@ __device__ TRACK_FN void warp_luinverse(int n, const double *A, const int *ipvt,
     for (int c = lane; c < n; c += 32)
       stn_at<N>(M, (long)kb * n + c, N::mul(ldn_at<N>(M, (long)kb * n + c), ldn_at<N>(dinv, kb)));
     __syncwarp();
-    if (lane < kb) {  // lanes over the rows above kb
-      const T u = ldn_at<N>(A, (long)lane * n + kb);
-      for (int c = 0; c < n; ++c) {
-        const long o = (long)lane * n + c;
-        stn_at<N>(M, o, N::sub(ldn_at<N>(M, o), N::mul(ldn_at<N>(M, (long)kb * n + c), u)));
-      }
+    for (int e = lane; e < kb * n; e += 32) {
+      const int j = e / n, c = e % n;
+      const long o = (long)j * n + c;
+      stn_at<N>(M, o, N::sub(ldn_at<N>(M, o), N::mul(ldn_at<N>(M, (long)kb * n + c), ldn_at<N>(A, (long)j * n + kb))));
     }
     __syncwarp();
   }
