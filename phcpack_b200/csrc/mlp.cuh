@@ -53,6 +53,7 @@ __device__ __forceinline__ void track_features(int tid, int n, int K, double t, 
     const int q = tid;
     const int k = (q + 1 <= K) ? q + 1 : K;
     double mx = 0.0, rmin = 1e300;
+    #pragma unroll 1
     for (int i = 0; i < n; ++i) {
       const double a = mag[i * (K + 1) + k], b = mag[i * (K + 1) + k - 1];
       mx = fmax(mx, a);
@@ -66,6 +67,7 @@ __device__ __forceinline__ void track_features(int tid, int n, int K, double t, 
     const int q = tid - 8;
     const int k = q <= K ? q : K;
     double mx = 0.0;
+    #pragma unroll 1
     for (int i = 0; i < n; ++i) mx = fmax(mx, mag[i * (K + 1) + k]);
     f[20 + q] = (float)fmin(fmax(log(mx + tiny), -60.0), 60.0);
   } else if (tid == 12) {
@@ -88,6 +90,7 @@ __device__ __forceinline__ float mlp_forward_cta(const void *model, const float 
   if (j < kMlpH) {
     float a = M.b1[j];
     const uint4 *w = reinterpret_cast<const uint4 *>(M.W1 + j * kMlpIn);
+    #pragma unroll 1
     for (int c = 0; c < kMlpIn / 8; ++c) {
       const uint4 u = __ldg(w + c);
       const __nv_bfloat16 *e = reinterpret_cast<const __nv_bfloat16 *>(&u);
@@ -104,6 +107,7 @@ __device__ __forceinline__ float mlp_forward_cta(const void *model, const float 
   if (j < kMlpH) {
     float a = M.b2[j];
     const uint4 *w = reinterpret_cast<const uint4 *>(M.W2 + j * kMlpH);
+    #pragma unroll 1
     for (int c = 0; c < kMlpH / 8; ++c) {
       const uint4 u = __ldg(w + c);
       const __nv_bfloat16 *e = reinterpret_cast<const __nv_bfloat16 *>(&u);
@@ -114,6 +118,7 @@ __device__ __forceinline__ float mlp_forward_cta(const void *model, const float 
     contrib = __bfloat162float(M.W3[j]) * h2[j];
   }
   // sum over the 4 warps of the first 128 threads
+  #pragma unroll 1
   for (int o = 16; o > 0; o >>= 1) contrib += __shfl_xor_sync(0xffffffffu, contrib, o);
   if ((j & 31) == 0 && j < kMlpH) red[j >> 5] = contrib;
   __syncthreads();

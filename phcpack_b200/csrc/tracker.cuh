@@ -12,6 +12,15 @@ namespace phc {
 // shared by several kernel instantiations would otherwise become a call,
 // with registers spilled around it); TRACK_OUTLINE=1 compiles them as calls
 // instead (less code for the instruction cache).
+//
+// Loops stay rolled (#pragma unroll 1 on every loop of the tracker without
+// a pragma of its own).  Seven paths share an SM, each in another phase of
+// a step, so the code of all phases competes for the SM's instruction
+// cache: with the compiler's unrolled copies of the loops over terms,
+// monomials, rows and degrees the hot code of one kernel exceeded 400 KB,
+// the instruction cache hit 60 % of its requests and warps stalled on
+// instruction fetch about as often as on barriers; rolled, the same steps
+// (bit for bit) take two thirds of the time on the 1024-path workload.
 #ifndef TRACK_OUTLINE
 #define TRACK_OUTLINE 0
 #endif
@@ -48,9 +57,11 @@ __device__ __forceinline__ void track_pick_lead() {
   __syncthreads();
   if (threadIdx.x == 0) {
     int mn = slot[0];
+    #pragma unroll 1
     for (int v = 1; v < nw; ++v) mn = min(mn, slot[v]);
     const int want = (mn / nw) & 3;
     int lead = 0;
+    #pragma unroll 1
     for (int v = nw - 1; v >= 0; --v)
       if ((slot[v] & 3) == want) lead = v;
     track_rot = (kTrackThreads - 32 * lead) & (kTrackThreads - 1);
@@ -188,6 +199,7 @@ __device__ TRACK_FN void hom_eval_cta(const TrackDev &S, int s, int w, double t0
   const int nm = S.mono_off[s + 1] - m0;
   const int mv = S.maxvar;
   const bool stage = S.gstaged && J != nullptr;
+  #pragma unroll 1
   for (int m = ctid(); m < nm; m += blockDim.x) {
     const int gm = m0 + m;
     const int k = S.mono_nvr[gm];
@@ -199,10 +211,13 @@ __device__ TRACK_FN void hom_eval_cta(const TrackDev &S, int s, int w, double t0
       const double *xa = x + (long)ix[0] * xld * W;
       const double *xb = (k == 2) ? x + (long)ix[1] * xld * W : xa;
       if (k == 1 && ex[0] == 1) {
+        #pragma unroll 1
         for (int i = 0; i < n1; ++i) stn_at<N>(Vm, i, ldn_at<N>(xa, i));
       } else {
+        #pragma unroll 1
         for (int kk = 0; kk < n1; ++kk) {
           T a = N::zero();
+          #pragma unroll 1
           for (int i = 0; i <= kk; ++i) a = N::add(a, N::mul(ldn_at<N>(xa, i), ldn_at<N>(xb, kk - i)));
           stn_at<N>(Vm, kk, a);
         }
@@ -211,12 +226,17 @@ __device__ TRACK_FN void hom_eval_cta(const TrackDev &S, int s, int w, double t0
     }
     T F[kTrackKmax + 1], acc[kTrackKmax + 1];
     bool unitF = true;
+    #pragma unroll 1
     for (int i = 0; i < n1; ++i) F[i] = (i == 0) ? N::one() : N::zero();
+    #pragma unroll 1
     for (int v = 0; v < k; ++v)
+      #pragma unroll 1
       for (int e = 1; e < ex[v]; ++e) {
         const double *xv = x + (long)ix[v] * xld * W;
+        #pragma unroll 1
         for (int kk = w; kk >= 0; --kk) {  // in place: F[kk] only needs F[<= kk]
           T a = N::zero();
+          #pragma unroll 1
           for (int i = 0; i <= kk; ++i) a = N::add(a, N::mul(ldn_at<N>(xv, i), F[kk - i]));
           F[kk] = a;
         }
@@ -225,21 +245,28 @@ __device__ TRACK_FN void hom_eval_cta(const TrackDev &S, int s, int w, double t0
     double *Vm = V + (long)m * n1 * W;
     double *Gm = G + (long)m * mv * n1 * W;
     if (k == 0) {
+      #pragma unroll 1
       for (int i = 0; i < n1; ++i) stn_at<N>(Vm, i, F[i]);
       continue;
     }
+    #pragma unroll 1
     for (int v = 0; v < (stage ? k : 1); ++v) {
+      #pragma unroll 1
       for (int i = 0; i < n1; ++i) acc[i] = F[i];
       bool unit = unitF;
+      #pragma unroll 1
       for (int u = 0; u < k; ++u) {
         if (u == v) continue;
         const double *xu = x + (long)ix[u] * xld * W;
         if (unit) {
+          #pragma unroll 1
           for (int i = 0; i < n1; ++i) acc[i] = ldn_at<N>(xu, i);
           unit = false;
         } else {
+          #pragma unroll 1
           for (int kk = w; kk >= 0; --kk) {
             T a = N::zero();
+            #pragma unroll 1
             for (int i = 0; i <= kk; ++i) a = N::add(a, N::mul(ldn_at<N>(xu, i), acc[kk - i]));
             acc[kk] = a;
           }
@@ -247,26 +274,32 @@ __device__ TRACK_FN void hom_eval_cta(const TrackDev &S, int s, int w, double t0
       }
       if (v == 0) {
         const double *x0 = x + (long)ix[0] * xld * W;
+        #pragma unroll 1
         for (int kk = 0; kk < n1; ++kk) {
           T a = N::zero();
+          #pragma unroll 1
           for (int i = 0; i <= kk; ++i) a = N::add(a, N::mul(ldn_at<N>(x0, i), acc[kk - i]));
           stn_at<N>(Vm, kk, a);
         }
       }
       if (!stage) continue;
       const double e = (double)ex[v];
+      #pragma unroll 1
       for (int i = 0; i < n1; ++i) stn_at<N>(Gm + (long)v * n1 * W, i, e == 1.0 ? acc[i] : N::scale_d(acc[i], e));
     }
   }
   __syncthreads();
   const int e0 = S.eq_off[s];
   const int lane = ctid() & 31, warp = ctid() >> 5, nw = blockDim.x >> 5;
+  #pragma unroll 1
   for (int i = warp; i < n; i += nw) {
     const int tb = S.term_off[e0 + i], te = S.term_off[e0 + i + 1];
+    #pragma unroll 1
     for (int k0 = 0; k0 < n1; k0 += KC) {
       T acc[KC];
 #pragma unroll
       for (int r = 0; r < KC; ++r) acc[r] = N::zero();
+      #pragma unroll 1
       for (int tr = tb + lane; tr < te; tr += 32) {
         const T a = cnum<N>(S.term_a[2 * tr], S.term_a[2 * tr + 1]);
         const T b = N::sub(cnum<N>(S.term_b[2 * tr], S.term_b[2 * tr + 1]), a);  // d/dt
@@ -293,14 +326,17 @@ __device__ TRACK_FN void hom_eval_cta(const TrackDev &S, int s, int w, double t0
     }
   }
   if (J != nullptr) {
+    #pragma unroll 1
     for (int it = ctid(); it < n * n; it += blockDim.x) {
       const int i = it / n, j = it % n;
       const int g = (e0 + i) * S.maxdim + j;
       const int qb = S.jg_off[g], qe = S.jg_off[g + 1];
+      #pragma unroll 1
       for (int k0 = 0; k0 < n1; k0 += KC) {
         JT acc[KC];
 #pragma unroll
         for (int r = 0; r < KC; ++r) acc[r] = JN::zero();
+        #pragma unroll 1
         for (int q = qb; q < qe; ++q) {
           const int tr = S.jg_term[q];
           const int sl = S.jg_slot[q];
@@ -355,6 +391,7 @@ __device__ TRACK_FN void hom_coef_cta(const TrackDev &S, int s, int k, double t0
   const int m0 = S.mono_off[s];
   const int nm = S.mono_off[s + 1] - m0;
   const int mv = S.maxvar;
+  #pragma unroll 1
   for (int m = ctid(); m < nm; m += blockDim.x) {
     const int gm = m0 + m;
     const int kv = S.mono_nvr[gm];
@@ -370,17 +407,24 @@ __device__ TRACK_FN void hom_coef_cta(const TrackDev &S, int s, int k, double t0
         c1 = ldn_at<N>(xa, k - 1);
         c2 = ldn_at<N>(xa, k);
       } else {
+        #pragma unroll 1
         for (int i = 0; i <= k - 1; ++i) c1 = N::add(c1, N::mul(ldn_at<N>(xa, i), ldn_at<N>(xb, k - 1 - i)));
+        #pragma unroll 1
         for (int i = 0; i <= k; ++i) c2 = N::add(c2, N::mul(ldn_at<N>(xa, i), ldn_at<N>(xb, k - i)));
       }
     } else {
       T F[kTrackKmax + 1];
+      #pragma unroll 1
       for (int i = 0; i <= k; ++i) F[i] = (i == 0) ? N::one() : N::zero();
+      #pragma unroll 1
       for (int v = 0; v < kv; ++v)
+        #pragma unroll 1
         for (int e = 0; e < ex[v]; ++e) {
           const double *xv = x + (long)ix[v] * xld * W;
+          #pragma unroll 1
           for (int kk = k; kk >= 0; --kk) {  // in place: F[kk] only needs F[<= kk]
             T a = N::zero();
+            #pragma unroll 1
             for (int i = 0; i <= kk; ++i) a = N::add(a, N::mul(ldn_at<N>(xv, i), F[kk - i]));
             F[kk] = a;
           }
@@ -394,8 +438,10 @@ __device__ TRACK_FN void hom_coef_cta(const TrackDev &S, int s, int k, double t0
   __syncthreads();
   const int e0 = S.eq_off[s];
   const int lane = ctid() & 31, warp = ctid() >> 5, nw = blockDim.x >> 5;
+  #pragma unroll 1
   for (int i = warp; i < n; i += nw) {
     T acc = N::zero();
+    #pragma unroll 1
     for (int tr = S.term_off[e0 + i] + lane; tr < S.term_off[e0 + i + 1]; tr += 32) {
       const T a = cnum<N>(S.term_a[2 * tr], S.term_a[2 * tr + 1]);
       const T b = N::sub(cnum<N>(S.term_b[2 * tr], S.term_b[2 * tr + 1]), a);  // d/dt
@@ -428,6 +474,7 @@ __device__ TRACK_FN int warp_lufac(int n, double *A, int *ipvt, double *dinv) {
   typedef typename N::T T;
   const int lane = threadIdx.x & 31;
   int info = 0;
+  #pragma unroll 1
   for (int k = 0; k < n; ++k) {
     double v = -1.0;
     if (lane >= k && lane < n) {
@@ -436,6 +483,7 @@ __device__ TRACK_FN int warp_lufac(int n, double *A, int *ipvt, double *dinv) {
     }
     // the largest value, then the first row that holds it (one ballot)
     double mx = v;
+    #pragma unroll 1
     for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
     const unsigned hold = __ballot_sync(0xffffffffu, lane >= k && lane < n && v == mx);
     const int ix = hold ? __ffs(hold) - 1 : n;
@@ -449,6 +497,7 @@ __device__ TRACK_FN int warp_lufac(int n, double *A, int *ipvt, double *dinv) {
       continue;
     }
     if (ell != k)
+      #pragma unroll 1
       for (int j = k + lane; j < n; j += 32) {
         const T a = ldn_at<N>(A, (long)ell * n + j);
         stn_at<N>(A, (long)ell * n + j, ldn_at<N>(A, (long)k * n + j));
@@ -461,6 +510,7 @@ __device__ TRACK_FN int warp_lufac(int n, double *A, int *ipvt, double *dinv) {
     __syncwarp();
     // trailing update, the (n-k-1)^2 entries spread over the lanes
     const int m = n - k - 1;
+    #pragma unroll 1
     for (int e = lane; e < m * m; e += 32) {
       const int i = k + 1 + e / m, j = k + 1 + e % m;
       const long o = (long)i * n + j;
@@ -482,6 +532,7 @@ __device__ typename N::T warp_lusolve(int n, const double *A, const int *ipvt, c
                                       typename N::T v) {
   typedef typename N::T T;
   const int lane = threadIdx.x & 31;
+  #pragma unroll 1
   for (int k = 0; k < n - 1; ++k) {  // L y = P b
     const int ell = ipvt[k];
     const T t = md::shfl(v, ell);
@@ -490,6 +541,7 @@ __device__ typename N::T warp_lusolve(int n, const double *A, const int *ipvt, c
     if (lane == k) v = t;
     if (lane > k && lane < n) v = N::add(v, N::mul(t, ldn_at<N>(A, (long)lane * n + k)));
   }
+  #pragma unroll 1
   for (int kb = n - 1; kb >= 0; --kb) {  // U x = y
     if (lane == kb) v = N::mul(v, ldn_at<N>(dinv, kb));
     const T t = md::shfl(v, kb);
@@ -507,11 +559,14 @@ template <class N>
 __device__ TRACK_FN void warp_luinverse(int n, const double *A, const int *ipvt, const double *dinv, double *M) {
   typedef typename N::T T;
   const int lane = threadIdx.x & 31;
+  #pragma unroll 1
   for (int e = lane; e < n * n; e += 32) stn_at<N>(M, e, (e / n == e % n) ? N::one() : N::zero());
   __syncwarp();
+  #pragma unroll 1
   for (int k = 0; k < n - 1; ++k) {  // L y = P e_c
     const int ell = ipvt[k];
     if (ell != k)
+      #pragma unroll 1
       for (int c = lane; c < n; c += 32) {
         const T t = ldn_at<N>(M, (long)ell * n + c);
         stn_at<N>(M, (long)ell * n + c, ldn_at<N>(M, (long)k * n + c));
@@ -519,6 +574,7 @@ __device__ TRACK_FN void warp_luinverse(int n, const double *A, const int *ipvt,
       }
     __syncwarp();
     const int m = n - k - 1;
+    #pragma unroll 1
     for (int e = lane; e < m * n; e += 32) {
       const int i = k + 1 + e / n, c = e % n;
       const long o = (long)i * n + c;
@@ -526,10 +582,13 @@ __device__ TRACK_FN void warp_luinverse(int n, const double *A, const int *ipvt,
     }
     __syncwarp();
   }
+  #pragma unroll 1
   for (int kb = n - 1; kb >= 0; --kb) {  // U x = y
+    #pragma unroll 1
     for (int c = lane; c < n; c += 32)
       stn_at<N>(M, (long)kb * n + c, N::mul(ldn_at<N>(M, (long)kb * n + c), ldn_at<N>(dinv, kb)));
     __syncwarp();
+    #pragma unroll 1
     for (int e = lane; e < kb * n; e += 32) {
       const int j = e / n, c = e % n;
       const long o = (long)j * n + c;
@@ -558,9 +617,11 @@ __device__ TRACK_FN void warp_qrinverse(int n, double *A, double *M, double *vk,
   typedef typename N::real R;
   typedef typename N::tr tr;
   const int lane = threadIdx.x & 31;
+  #pragma unroll 1
   for (int k = 0; k < n; ++k) {
     if (lane == 0) {
       R sig = tr::zero();
+      #pragma unroll 1
       for (int i = k + 1; i < n; ++i) sig = tr::add(sig, N::norm2(ldn_at<N>(A, (long)i * n + k)));
       const T xk = ldn_at<N>(A, (long)k * n + k);
       const R a2 = N::norm2(xk);
@@ -584,35 +645,45 @@ __device__ TRACK_FN void warp_qrinverse(int n, double *A, double *M, double *vk,
     __syncwarp();
     const T v0 = ldn_at<N>(vk, k);
     const R t = tau[k];
+    #pragma unroll 1
     for (int j = k + 1 + lane; j < n; j += 32) {  // lanes over the columns to the right
       T w = N::mul(N::conj(v0), ldn_at<N>(A, (long)k * n + j));
+      #pragma unroll 1
       for (int i = k + 1; i < n; ++i)
         w = N::add(w, N::mul(N::conj(ldn_at<N>(A, (long)i * n + k)), ldn_at<N>(A, (long)i * n + j)));
       w = N::mkc(tr::mul(w.re, t), tr::mul(w.im, t));
       stn_at<N>(A, (long)k * n + j, N::sub(ldn_at<N>(A, (long)k * n + j), N::mul(v0, w)));
+      #pragma unroll 1
       for (int i = k + 1; i < n; ++i)
         stn_at<N>(A, (long)i * n + j, N::sub(ldn_at<N>(A, (long)i * n + j), N::mul(ldn_at<N>(A, (long)i * n + k), w)));
     }
     __syncwarp();
   }
   // M = Q^H = H_{n-1} ... H_0 I, lanes over the columns
+  #pragma unroll 1
   for (int c = lane; c < n; c += 32) {
+    #pragma unroll 1
     for (int i = 0; i < n; ++i) stn_at<N>(M, (long)i * n + c, i == c ? N::one() : N::zero());
+    #pragma unroll 1
     for (int k = 0; k < n; ++k) {
       const R t = tau[k];
       if (t == tr::zero()) continue;
       const T v0 = ldn_at<N>(vk, k);
       T w = N::mul(N::conj(v0), ldn_at<N>(M, (long)k * n + c));
+      #pragma unroll 1
       for (int i = k + 1; i < n; ++i)
         w = N::add(w, N::mul(N::conj(ldn_at<N>(A, (long)i * n + k)), ldn_at<N>(M, (long)i * n + c)));
       w = N::mkc(tr::mul(w.re, t), tr::mul(w.im, t));
       stn_at<N>(M, (long)k * n + c, N::sub(ldn_at<N>(M, (long)k * n + c), N::mul(v0, w)));
+      #pragma unroll 1
       for (int i = k + 1; i < n; ++i)
         stn_at<N>(M, (long)i * n + c, N::sub(ldn_at<N>(M, (long)i * n + c), N::mul(ldn_at<N>(A, (long)i * n + k), w)));
     }
     // R X = Q^H, column c
+    #pragma unroll 1
     for (int i = n - 1; i >= 0; --i) {
       T acc = ldn_at<N>(M, (long)i * n + c);
+      #pragma unroll 1
       for (int j = i + 1; j < n; ++j) acc = N::sub(acc, N::mul(ldn_at<N>(A, (long)i * n + j), ldn_at<N>(M, (long)j * n + c)));
       stn_at<N>(M, (long)i * n + c, N::div(acc, ldn_at<N>(A, (long)i * n + i)));
     }
@@ -653,6 +724,7 @@ static __device__ int gk_count(int n, double dk, double ek, double x) {
   double pm2 = 1.0, pm1 = -x;
   int cnt = pm1 < 0.0 ? 1 : 0;
   bool neg = pm1 < 0.0 || pm1 == 0.0;  // sign of p_{m-1} (a zero counts as a change)
+  #pragma unroll 1
   for (int m = 1; m < 2 * n; ++m) {
     const int k = (m - 1) >> 1;
     const double c = __shfl_sync(0xffffffffu, (m - 1) & 1 ? ek : dk, k);
@@ -679,6 +751,7 @@ static __device__ int gk_count(int n, double dk, double ek, double x) {
 // rounds); the decisions are uniform over the warp.
 static __device__ double gk_bisect(int n, double dk, double ek, double lo, double hi, int target) {
   const int lane = threadIdx.x & 31;
+  #pragma unroll 1
   for (int round = 0; round < 30 && hi - lo > 0x1p-52 * hi; ++round) {
     const double x = lo + (hi - lo) * (double)(lane + 1) * (1.0 / 33.0);
     const unsigned m = __ballot_sync(0xffffffffu, gk_count(n, dk, ek, x) >= target);
@@ -702,6 +775,7 @@ static __device__ double gk_bisect(int n, double dk, double ek, double lo, doubl
 static __device__ double2 warp_singular_extremes(int n, double2 *A, int want) {
   const int lane = threadIdx.x & 31;
   double amax = 0.0;
+  #pragma unroll 1
   for (int q = lane; q < n * n; q += 32) {
     const double2 a = A[q];
     const double m = fmax(fabs(a.x), fabs(a.y));
@@ -714,9 +788,11 @@ static __device__ double2 warp_singular_extremes(int n, double2 *A, int want) {
   int ex;
   frexp(amax, &ex);
   const double sc = ldexp(1.0, 1 - ex);
+  #pragma unroll 1
   for (int q = lane; q < n * n; q += 32) A[q] = make_double2(A[q].x * sc, A[q].y * sc);
   __syncwarp();
   double dk = 0.0, ek = 0.0;  // lane k keeps d_k and e_k of the bidiagonal
+  #pragma unroll 1
   for (int k = 0; k < n; ++k) {
     // left reflector on column k, rows k..n-1 (lanes over the rows)
     const double2 x = (lane >= k && lane < n) ? A[(long)k * n + lane] : make_double2(0.0, 0.0);
@@ -733,14 +809,17 @@ static __device__ double2 warp_singular_extremes(int n, double2 *A, int want) {
       __syncwarp();
       if (lane == k) A[(long)k * n + k] = make_double2(ph.x * vk, ph.y * vk);
       __syncwarp();
+      #pragma unroll 1
       for (int j = k + 1 + lane; j < n; j += 32) {  // lanes over the columns to the right
         double2 w = make_double2(0.0, 0.0);
+        #pragma unroll 1
         for (int r = k; r < n; ++r) {
           const double2 p = cx_conj_mul(A[(long)k * n + r], A[(long)j * n + r]);
           w.x += p.x;
           w.y += p.y;
         }
         w = make_double2(w.x * tau, w.y * tau);
+        #pragma unroll 1
         for (int r = k; r < n; ++r) {
           const double2 p = cx_mul(A[(long)k * n + r], w);
           A[(long)j * n + r] = make_double2(A[(long)j * n + r].x - p.x, A[(long)j * n + r].y - p.y);
@@ -764,14 +843,17 @@ static __device__ double2 warp_singular_extremes(int n, double2 *A, int want) {
       __syncwarp();
       if (lane == k) A[(long)(k + 1) * n + k] = make_double2(ph.x * uk, ph.y * uk);
       __syncwarp();
+      #pragma unroll 1
       for (int r = k + 1 + lane; r < n; r += 32) {  // lanes over the rows below
         double2 z = make_double2(0.0, 0.0);
+        #pragma unroll 1
         for (int c = k + 1; c < n; ++c) {
           const double2 p = cx_conj_mul(A[(long)c * n + k], A[(long)c * n + r]);
           z.x += p.x;
           z.y += p.y;
         }
         z = make_double2(z.x * tau, z.y * tau);
+        #pragma unroll 1
         for (int c = k + 1; c < n; ++c) {
           const double2 p = cx_mul(z, A[(long)c * n + k]);
           A[(long)c * n + r] = make_double2(A[(long)c * n + r].x - p.x, A[(long)c * n + r].y - p.y);
@@ -794,6 +876,7 @@ static __device__ double2 warp_singular_extremes(int n, double2 *A, int want) {
     // sigma_min in (0, min |d_k|] (a triangular matrix's smallest singular
     // value is at most its smallest diagonal entry)
     double hi = lane < n ? dk : INFINITY;
+    #pragma unroll 1
     for (int o = 16; o > 0; o >>= 1) hi = fmin(hi, __shfl_xor_sync(0xffffffffu, hi, o));
     smin = hi > 0.0 ? gk_bisect(n, dk, ek, 0.0, hi, n + 1) / sc : 0.0;
   }
@@ -809,9 +892,11 @@ static __device__ double2 warp_singular_extremes(int n, double2 *A, int want) {
 // cell has one writer and a fixed order.  One warp, n <= 32.
 static __device__ void warp_hessian_rows(const TrackDev &S, int s, int i, int n, double t, const double2 *x, double2 *H) {
   const int j = threadIdx.x & 31;
+  #pragma unroll 1
   for (int l = 0; l < n && j < n; ++l) H[(long)l * n + j] = make_double2(0.0, 0.0);
   if (j < n) {
     const int g = (S.eq_off[s] + i) * S.maxdim + j;
+    #pragma unroll 1
     for (int q = S.jg_off[g]; q < S.jg_off[g + 1]; ++q) {
       const int tr = S.jg_term[q], sl = S.jg_slot[q];
       if (sl == -1) continue;
@@ -829,11 +914,14 @@ static __device__ void warp_hessian_rows(const TrackDev &S, int s, int i, int n,
         const int nv = S.mono_nvr[gm];
         const int *ix = S.mono_idx + (long)gm * S.maxvar;
         const int *ex = S.mono_exp + (long)gm * S.maxvar;
+        #pragma unroll 1
         for (int u = 0; u < nv; ++u) {
           const double mult = u == sl ? (double)ex[u] * (ex[u] - 1) : (double)ex[u] * ex[sl];
           if (mult == 0.0) continue;
           double2 acc = make_double2(c.x * mult, c.y * mult);
+          #pragma unroll 1
           for (int w = 0; w < nv; ++w)
+            #pragma unroll 1
             for (int e = ex[w] - (w == u) - (w == sl); e > 0; --e) acc = cx_mul(acc, x[ix[w]]);
           double2 &h = H[(long)ix[u] * n + j];
           h = make_double2(h.x + acc.x, h.y + acc.y);
@@ -856,6 +944,7 @@ __device__ double pade_error_one(const double *c, int K, const double *num, int 
   typedef typename N::T T;
   const int endidx = min(pdeg + qdeg + 2, K);
   int top = -1;
+  #pragma unroll 1
   for (int i = endidx; i >= 0; --i)
     if (N::mag(ldn_at<N>(c, i)) > 1e-5) {
       top = i;
@@ -864,6 +953,7 @@ __device__ double pade_error_one(const double *c, int K, const double *num, int 
   T res = N::one();
   if (top >= 0) {
     res = ldn_at<N>(c, top);
+    #pragma unroll 1
     for (int i = 1; i <= qdeg && i <= top; ++i) res = N::add(res, N::mul(ldn_at<N>(den, i), ldn_at<N>(c, top - i)));
     if (top <= pdeg) res = N::sub(ldn_at<N>(num, top), res);
   }
@@ -875,8 +965,10 @@ __device__ double pade_error_one(const double *c, int K, const double *num, int 
 template <class N>
 __device__ void cta_matvec(int n, const double *M, const double *b, double *y) {
   typedef typename N::T T;
+  #pragma unroll 1
   for (int i = ctid(); i < n; i += blockDim.x) {
     T acc = N::zero();
+    #pragma unroll 1
     for (int j = 0; j < n; ++j) acc = N::add(acc, N::mul(ldn_at<N>(M, (long)i * n + j), ldn_at<N>(b, j)));
     stn_at<N>(y, i, acc);
   }
@@ -962,6 +1054,7 @@ __device__ TRACK_FN bool point_newton(const TrackDev &S, int s, int n, double t,
   bool conv = false;
   int extra_left = extra;
   *lastdx = 1e300;
+  #pragma unroll 1
   for (int it = 0; it < maxit + extra; ++it) {
     if (it >= maxit && !conv) break;
     hom_eval_cta<N, 1, JN>(S, s, 0, t, x, 1, Vc, Gc, h, Jm);
@@ -1083,13 +1176,16 @@ __device__ TRACK_FN bool point_newton_split(const TrackDev &S, int s, int n, dou
   int extra_left = extra;
   int info = 0;
   *lastdx = 1e300;
+  #pragma unroll 1
   for (int it = 0; it < maxit + extra; ++it) {
     if (it >= maxit && !conv) break;
     // J(x) in complex double, one entry per thread
+    #pragma unroll 1
     for (int e = ctid(); e < n * n; e += kTrackThreads) {
       const int i = e / n, j = e % n;
       const int g = (e0 + i) * S.maxdim + j;
       double2 acc = make_double2(0.0, 0.0);
+      #pragma unroll 1
       for (int q = S.jg_off[g]; q < S.jg_off[g + 1]; ++q) {
         const int tr = S.jg_term[q], sl = S.jg_slot[q];
         const double ar = S.term_a[2 * tr], ai = S.term_a[2 * tr + 1];
@@ -1104,6 +1200,7 @@ __device__ TRACK_FN bool point_newton_split(const TrackDev &S, int s, int n, dou
       reinterpret_cast<double2 *>(Jm)[e] = acc;
     }
     // the distinct monomials x^e in double-double, one per thread
+    #pragma unroll 1
     for (int m = ctid(); m < nm; m += kTrackThreads) {
       const int gm = m0 + m;
       const int nv = S.mono_nvr[gm];
@@ -1111,8 +1208,10 @@ __device__ TRACK_FN bool point_newton_split(const TrackDev &S, int s, int n, dou
       const int *ex = S.mono_exp + (long)gm * S.maxvar;
       T v = N::one();
       bool unit = true;
+      #pragma unroll 1
       for (int u = 0; u < nv; ++u) {
         const T xu = ldn_at<N>(x, ix[u]);
+        #pragma unroll 1
         for (int q = 0; q < ex[u]; ++q) {
           v = unit ? xu : N::mul(v, xu);
           unit = false;
@@ -1126,6 +1225,7 @@ __device__ TRACK_FN bool point_newton_split(const TrackDev &S, int s, int n, dou
     } else {
       sum2 pr, pi, qr, qi;
       pr.zero(); pi.zero(); qr.zero(); qi.zero();
+      #pragma unroll 1
       for (int tr = S.term_off[e0 + req] + rk; tr < S.term_off[e0 + req + 1]; tr += rg) {
         const T v = ldn_at<N>(V, S.term_mono[tr] - m0);
         const double ar = S.term_a[2 * tr], ai = S.term_a[2 * tr + 1];
@@ -1148,6 +1248,7 @@ __device__ TRACK_FN bool point_newton_split(const TrackDev &S, int s, int n, dou
       residual_warps_sync();
       if (rk == 0) {
         T acc = ldn_at<N>(part, ri);
+        #pragma unroll 1
         for (int k = 1; k < rg; ++k) acc = N::add(acc, ldn_at<N>(part, ri + k));
         stn_at<N>(h, req, acc);
       }
@@ -1195,47 +1296,60 @@ __device__ TRACK_FN int pade_one(int L, int M, int K, const double *c, double *n
   typedef typename N::T T;
   T A[kTrackKmax * kTrackKmax / 4 + 16], b[kTrackKmax / 2 + 8], q[kTrackKmax / 2 + 9];
   bool ok = true;
+  #pragma unroll 1
   for (int i = 1; i <= M; ++i) {
+    #pragma unroll 1
     for (int j = 1; j <= M; ++j) {
       const int k = L + i - j;
       A[(i - 1) * M + (j - 1)] = k >= 0 ? ldn_at<N>(c, k) : N::zero();
     }
     b[i - 1] = N::neg(ldn_at<N>(c, L + i));
   }
+  #pragma unroll 1
   for (int col = 0; col < M && ok; ++col) {
     int piv = col;
     double best = N::mag(A[col * M + col]);
+    #pragma unroll 1
     for (int r = col + 1; r < M; ++r) {
       const double m = N::mag(A[r * M + col]);
       if (m > best) { best = m; piv = r; }
     }
     if (!(best > 0.0)) { ok = false; break; }
     if (piv != col) {
+      #pragma unroll 1
       for (int j = 0; j < M; ++j) { T tt = A[piv * M + j]; A[piv * M + j] = A[col * M + j]; A[col * M + j] = tt; }
       T tt = b[piv]; b[piv] = b[col]; b[col] = tt;
     }
+    #pragma unroll 1
     for (int r = col + 1; r < M; ++r) {
       const T f = N::div(A[r * M + col], A[col * M + col]);
+      #pragma unroll 1
       for (int j = col; j < M; ++j) A[r * M + j] = N::sub(A[r * M + j], N::mul(f, A[col * M + j]));
       b[r] = N::sub(b[r], N::mul(f, b[col]));
     }
   }
   q[0] = N::one();
   if (ok) {
+    #pragma unroll 1
     for (int i = M - 1; i >= 0; --i) {
       T acc = b[i];
+      #pragma unroll 1
       for (int j = i + 1; j < M; ++j) acc = N::sub(acc, N::mul(A[i * M + j], q[j + 1]));
       q[i + 1] = N::div(acc, A[i * M + i]);
     }
+    #pragma unroll 1
     for (int i = 0; i <= M; ++i) stn_at<N>(den, i, q[i]);
+    #pragma unroll 1
     for (int i = 0; i <= L; ++i) {
       T acc = N::zero();
+      #pragma unroll 1
       for (int j = 0; j <= (i < M ? i : M); ++j) acc = N::add(acc, N::mul(q[j], ldn_at<N>(c, i - j)));
       stn_at<N>(num, i, acc);
     }
     return L;
   }
   stn_at<N>(den, 0, N::one());
+  #pragma unroll 1
   for (int i = 0; i <= K; ++i) stn_at<N>(num, i, ldn_at<N>(c, i));
   return K;
 }
@@ -1253,22 +1367,27 @@ __device__ TRACK_FN int pade_one_ws(int L, int M, int K, const double *c, double
   double *A = w, *b = w + (long)M * M * W, *q = w + (long)(M * M + M) * W;
   auto a_at = [&](int i, int j) { return ldn_at<N>(A, (long)i * M + j); };
   bool ok = true;
+  #pragma unroll 1
   for (int i = 1; i <= M; ++i) {
+    #pragma unroll 1
     for (int j = 1; j <= M; ++j) {
       const int k = L + i - j;
       stn_at<N>(A, (long)(i - 1) * M + (j - 1), k >= 0 ? ldn_at<N>(c, k) : N::zero());
     }
     stn_at<N>(b, i - 1, N::neg(ldn_at<N>(c, L + i)));
   }
+  #pragma unroll 1
   for (int col = 0; col < M && ok; ++col) {
     int piv = col;
     double best = N::mag(a_at(col, col));
+    #pragma unroll 1
     for (int r = col + 1; r < M; ++r) {
       const double m = N::mag(a_at(r, col));
       if (m > best) { best = m; piv = r; }
     }
     if (!(best > 0.0)) { ok = false; break; }
     if (piv != col) {
+      #pragma unroll 1
       for (int j = 0; j < M; ++j) {
         const T tt = a_at(piv, j);
         stn_at<N>(A, (long)piv * M + j, a_at(col, j));
@@ -1280,28 +1399,36 @@ __device__ TRACK_FN int pade_one_ws(int L, int M, int K, const double *c, double
     }
     const T acc = a_at(col, col);
     const T bc = ldn_at<N>(b, col);
+    #pragma unroll 1
     for (int r = col + 1; r < M; ++r) {
       const T f = N::div(a_at(r, col), acc);
+      #pragma unroll 1
       for (int j = col; j < M; ++j) stn_at<N>(A, (long)r * M + j, N::sub(a_at(r, j), N::mul(f, a_at(col, j))));
       stn_at<N>(b, r, N::sub(ldn_at<N>(b, r), N::mul(f, bc)));
     }
   }
   stn_at<N>(q, 0, N::one());
   if (ok) {
+    #pragma unroll 1
     for (int i = M - 1; i >= 0; --i) {
       T acc = ldn_at<N>(b, i);
+      #pragma unroll 1
       for (int j = i + 1; j < M; ++j) acc = N::sub(acc, N::mul(a_at(i, j), ldn_at<N>(q, j + 1)));
       stn_at<N>(q, i + 1, N::div(acc, a_at(i, i)));
     }
+    #pragma unroll 1
     for (int i = 0; i <= M; ++i) stn_at<N>(den, i, ldn_at<N>(q, i));
+    #pragma unroll 1
     for (int i = 0; i <= L; ++i) {
       T acc = N::zero();
+      #pragma unroll 1
       for (int j = 0; j <= (i < M ? i : M); ++j) acc = N::add(acc, N::mul(ldn_at<N>(q, j), ldn_at<N>(c, i - j)));
       stn_at<N>(num, i, acc);
     }
     return L;
   }
   stn_at<N>(den, 0, N::one());
+  #pragma unroll 1
   for (int i = 0; i <= K; ++i) stn_at<N>(num, i, ldn_at<N>(c, i));
   return K;
 }

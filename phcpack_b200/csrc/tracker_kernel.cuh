@@ -42,6 +42,7 @@ namespace phc {
 template <class N>
 __device__ double cta_maxmag(int n, const double *v, double *red) {
   double a = 0.0;
+  #pragma unroll 1
   for (int i = ctid(); i < n; i += blockDim.x) {
     const double m = N::mag(ldn_at<N>(v, i));
     a = (m != m) ? INFINITY : fmax(a, m);  // a NaN reads as infinity
@@ -60,6 +61,7 @@ __device__ double point_residual(const TrackDev &S, int s, int n, double t, cons
 template <class N>
 __device__ typename N::T horner(const double *a, int deg, const typename N::T &z) {
   typename N::T acc = ldn_at<N>(a, deg);
+  #pragma unroll 1
   for (int i = deg - 1; i >= 0; --i) acc = N::add(N::mul(acc, z), ldn_at<N>(a, i));
   return acc;
 }
@@ -74,6 +76,7 @@ __device__ TRACK_FN double pade_mixres(const TrackDev &S, int s, int n, int K, i
                               const double *num, const double *den, const int *degs, double *xp, double *xa,
                               double *V, double *G, double *hs, double *red) {
   const int Wp = PN::width;
+  #pragma unroll 1
   for (int i = ctid(); i < n; i += blockDim.x) {
     const typename PN::T z = PN::from(st);
     const typename PN::T nv = horner<PN>(num + (long)i * (K + 1) * Wp, degs[2 * i], z);
@@ -87,20 +90,25 @@ __device__ TRACK_FN double pade_mixres(const TrackDev &S, int s, int n, int K, i
   // one warp per equation, lanes over its terms
   const int lane = ctid() & 31, warp = ctid() >> 5, nw = blockDim.x >> 5;
   double part = 0.0;
+  #pragma unroll 1
   for (int i = warp; i < n; i += nw) {
     double ab = 0.0;
     const int eq = S.eq_off[s] + i;
+    #pragma unroll 1
     for (int tr = S.term_off[eq] + lane; tr < S.term_off[eq + 1]; tr += 32) {
       const int gm = S.term_mono[tr];
       // |(1 - t') a + t' b| at t' = t + st
       double v = hypot(fma(S.term_b[2 * tr] - S.term_a[2 * tr], t + st, S.term_a[2 * tr]),
                        fma(S.term_b[2 * tr + 1] - S.term_a[2 * tr + 1], t + st, S.term_a[2 * tr + 1]));
+      #pragma unroll 1
       for (int u = 0; u < S.mono_nvr[gm]; ++u) {
         const double xu = xa[S.mono_idx[(long)gm * S.maxvar + u]];
+        #pragma unroll 1
         for (int e = 0; e < S.mono_exp[(long)gm * S.maxvar + u]; ++e) v *= xu;
       }
       ab += v;
     }
+    #pragma unroll 1
     for (int o = 16; o > 0; o >>= 1) ab += __shfl_xor_sync(0xffffffffu, ab, o);
     if (lane == 0) part += PN::mag(ldn_at<PN>(hs, i)) / (ab + 1.0);
   }
@@ -150,6 +158,7 @@ __global__ void __launch_bounds__(kTrackThreads, (track_min_blocks<PN, RN, WIDE>
   const int Wp = PN::width, Wr = RN::width;
   const int n_max = S.maxdim;
   int nm_max = 0;
+  #pragma unroll 1
   for (int s = 0; s < S.nsys; ++s) nm_max = max(nm_max, S.mono_off[s + 1] - S.mono_off[s]);
   const TrackLayout L = track_layout(n_max, K, P.dendeg, nm_max, S.maxvar, Wp, Wr, S.gstaged);
   double *red = sm + L.red;
@@ -157,6 +166,7 @@ __global__ void __launch_bounds__(kTrackThreads, (track_min_blocks<PN, RN, WIDE>
   double *dinv = sm + L.dinv;
   track_pick_lead();
   int next_static = blockIdx.x;
+  #pragma unroll 1
   for (;;) {
     if (queue) {
       if (ctid() == 0) cur = atomicAdd(queue, 1);
@@ -174,6 +184,7 @@ __global__ void __launch_bounds__(kTrackThreads, (track_min_blocks<PN, RN, WIDE>
     const int n = S.dim[s];
     double *xc = sm + L.xc;
     // start point, refined at t = 0
+    #pragma unroll 1
     for (int i = ctid(); i < n; i += blockDim.x) {
       const double *z = x0 + ((long)path * n_max + i) * 2;
       stn_at<CN>(xc, i, cnum<CN>(z[0], z[1]));
@@ -183,6 +194,7 @@ __global__ void __launch_bounds__(kTrackThreads, (track_min_blocks<PN, RN, WIDE>
     corrector_newton<CN, PN>(S, s, n, 0.0, xc, sm, L, piv, dinv, red, P.corsteps, P.tolres, 1, &dxn);
     int status = 2, nsteps = 0, nrej = 0, nbpole = 0, nbhess = 0, nbmaxm = 0;
     bool failed = false;
+    #pragma unroll 1
     for (int step_it = 0; step_it < P.maxsteps; ++step_it) {
       // ---------------- predictor: the Taylor series of the path in PN
       // x(s) = x_0 + x_1 s + ... + x_K s^K solves h(x(s), t + s) = 0 to
@@ -194,6 +206,7 @@ __global__ void __launch_bounds__(kTrackThreads, (track_min_blocks<PN, RN, WIDE>
       // once by lufac) converges to, computed without the Jacobian series:
       // K coefficient evaluations and K products with J_0^{-1}.
       double *xs = sm + L.xs;
+      #pragma unroll 1
       for (int t2 = ctid(); t2 < n * (K + 1); t2 += blockDim.x) {
         const int i = t2 / (K + 1), k = t2 % (K + 1);
         typename PN::T v = PN::zero();
@@ -206,10 +219,12 @@ __global__ void __launch_bounds__(kTrackThreads, (track_min_blocks<PN, RN, WIDE>
       double2 *svd = reinterpret_cast<double2 *>(sm + L.svd);
       double2 *xd = reinterpret_cast<double2 *>(sm + L.xd);
       double *sv = sm + L.sv;
+      #pragma unroll 1
       for (int q = ctid(); q < n * n; q += blockDim.x) {
         const typename PN::T v = ldn_at<PN>(sm + L.J0, q);
         svd[(long)(kSvdSlots - 1) * n * n + q] = make_double2(md::lead(v.re), md::lead(v.im));
       }
+      #pragma unroll 1
       for (int i = ctid(); i < n; i += blockDim.x) {
         const typename PN::T v = ldn_at<PN>(xs, (long)i * (K + 1));
         xd[i] = make_double2(md::lead(v.re), md::lead(v.im));
@@ -230,20 +245,25 @@ __global__ void __launch_bounds__(kTrackThreads, (track_min_blocks<PN, RN, WIDE>
         }
       } else {
         const int hw = (ctid() >> 5), nhw = kTrackThreads / 32 - 1;
+        #pragma unroll 1
         for (int i = hw - 1; i < n; i += nhw) {
           double2 *H = svd + (long)hw * n * n;
           warp_hessian_rows(S, s, i, n, t, xd, H);
           double f = 0.0;
+          #pragma unroll 1
           for (int q = ctid() & 31; q < n * n; q += 32) f = fma(H[q].x, H[q].x, fma(H[q].y, H[q].y, f));
           f = warp_sum_d(f);
           if ((ctid() & 31) == 0) sv[i] = f;
         }
       }
       __syncthreads();
+      #pragma unroll 1
       for (int k = 1; k <= K; ++k) {
         hom_coef_cta<PN>(S, s, k, t, xs, K + 1, sm + L.V, sm + L.r);
+        #pragma unroll 1
         for (int i = ctid(); i < n; i += blockDim.x) {
           typename PN::T acc = PN::zero();
+          #pragma unroll 1
           for (int j = 0; j < n; ++j)
             acc = PN::add(acc, PN::mul(ldn_at<PN>(sm + L.M, (long)i * n + j), ldn_at<PN>(sm + L.r, j)));
           stn_at<PN>(xs, (long)i * (K + 1) + k, PN::neg(acc));
@@ -254,6 +274,7 @@ __global__ void __launch_bounds__(kTrackThreads, (track_min_blocks<PN, RN, WIDE>
       int pdeg_i = 0, qdeg_i = 0;
       double rmin = 1e300, perr2 = 0.0;
       double *num = sm + L.num, *den = sm + L.den;
+      #pragma unroll 1
       for (int i = ctid(); i < n; i += blockDim.x) {
         const double *ci = xs + (long)i * (K + 1) * Wp;
         double *numi = num + (long)i * (K + 1) * Wp, *deni = den + (long)i * (P.dendeg + 1) * Wp;
@@ -265,6 +286,7 @@ __global__ void __launch_bounds__(kTrackThreads, (track_min_blocks<PN, RN, WIDE>
         const double cd = PN::mag(ldn_at<PN>(ci, K - 2));
         if (cd != 0.0) rmin = fmin(rmin, PN::mag(ldn_at<PN>(ci, K - 3)) / cd);
         double *mg = sm + L.mag + (long)i * (K + 1);
+        #pragma unroll 1
         for (int k = 0; k <= K; ++k) mg[k] = PN::mag(ldn_at<PN>(ci, k));
       }
       // per-component Pade degrees go to shared memory for the evaluations
@@ -288,12 +310,14 @@ __global__ void __launch_bounds__(kTrackThreads, (track_min_blocks<PN, RN, WIDE>
       // with +inf, so the singular values are computed only otherwise (a 1 %
       // margin covers the rounding of the bounds).
       double mf2 = 0.0;
+      #pragma unroll 1
       for (int q = ctid(); q < n * n; q += blockDim.x) {
         const double a = PN::mag(ldn_at<PN>(sm + L.M, q));
         mf2 = fma(a, a, mf2);
       }
       mf2 = block_sum<md::num<double, false> >(mf2, red);
       double hf2 = 0.0;
+      #pragma unroll 1
       for (int i = 0; i < n; ++i) hf2 += sv[i];
       const double cap = fmin(pole_step, P.maxsize);
       double curv_step = INFINITY;
@@ -307,6 +331,7 @@ __global__ void __launch_bounds__(kTrackThreads, (track_min_blocks<PN, RN, WIDE>
         // Hessian of equation i, job n the smallest of the Jacobian (its copy
         // from before the LU); every thread has read the norms in sv
         __syncthreads();
+        #pragma unroll 1
         for (int job = ctid() >> 5; job <= n; job += kTrackThreads / 32) {
           if (job < n) {
             double2 *H = svd + (long)(ctid() >> 5) * n * n;
@@ -320,6 +345,7 @@ __global__ void __launch_bounds__(kTrackThreads, (track_min_blocks<PN, RN, WIDE>
         }
         __syncthreads();
         double hsum = 0.0;
+        #pragma unroll 1
         for (int i = 0; i < n; ++i) hsum = fma(sv[i], sv[i], hsum);
         const double eta = hsum > 0.0 ? 2.0 * sv[n] / sqrt(hsum) : INFINITY;
         curv_step = pow(P.cbeta * eta / perr, 1.0 / K);
@@ -353,6 +379,7 @@ __global__ void __launch_bounds__(kTrackThreads, (track_min_blocks<PN, RN, WIDE>
       }
       const double step0 = step;
       bool accepted = false;
+      #pragma unroll 1
       for (int attempt = 0; attempt < 2 && !accepted; ++attempt) {
         if (attempt == 1) {
           // the learned proposal was rejected: redo the step with the plain one
@@ -371,6 +398,7 @@ __global__ void __launch_bounds__(kTrackThreads, (track_min_blocks<PN, RN, WIDE>
         // predictor feedback on the mixed residual
         double *xp = sm + L.xp;
         bool ok = false;
+        #pragma unroll 1
         for (int h = 0; h < 64; ++h) {
           const double mixres = pade_mixres<PN>(S, s, n, K, P.dendeg, t, step, num, den, degs, xp, sm + L.xa,
                                                 sm + L.V, sm + L.G, sm + L.hs, red);
@@ -386,7 +414,9 @@ __global__ void __launch_bounds__(kTrackThreads, (track_min_blocks<PN, RN, WIDE>
         }
         // corrector with step halving
         bool cok = false;
+        #pragma unroll 1
         for (int h = 0; h < 64; ++h) {
+          #pragma unroll 1
           for (int i = ctid(); i < n; i += blockDim.x)
             stn_at<CN>(xc, i, conv_num<PN, CN>::go(ldn_at<PN>(xp, i)));
           __syncthreads();
@@ -399,6 +429,7 @@ __global__ void __launch_bounds__(kTrackThreads, (track_min_blocks<PN, RN, WIDE>
           if (learned) break;  // rejected proposal: retry with the plain step
           step *= 0.5;
           if (step < P.minsize) break;
+          #pragma unroll 1
           for (int i = ctid(); i < n; i += blockDim.x) {
             const typename PN::T z = PN::from(step);
             const int pd = degs[2 * i], qd = degs[2 * i + 1];
@@ -419,6 +450,7 @@ __global__ void __launch_bounds__(kTrackThreads, (track_min_blocks<PN, RN, WIDE>
       if (log != nullptr) {
         double best = step;
         const double mults[5] = {1.5, 2.0, 3.0, 4.0, 6.0};
+        #pragma unroll 1
         for (int q = 0; q < 5; ++q) {
           double sp = fmin(plain_step * mults[q], P.maxsize);
           if (t + sp > 1.0) sp = 1.0 - t;
@@ -431,12 +463,14 @@ __global__ void __launch_bounds__(kTrackThreads, (track_min_blocks<PN, RN, WIDE>
           const int slot = atomicAdd(log_count, 1);
           if (slot < log_cap) {
             float *f = log + (long)slot * 32;
+            #pragma unroll 1
             for (int q = 0; q < 24; ++q) f[q] = feat[q];
             f[24] = (float)step;
             f[25] = (float)plain_step;
             f[26] = (float)step0;
             f[27] = (float)t;
             f[28] = (float)best;
+            #pragma unroll 1
             for (int q = 29; q < 32; ++q) f[q] = 0.0f;
           }
         }
@@ -468,6 +502,7 @@ __global__ void __launch_bounds__(kTrackThreads, (track_min_blocks<PN, RN, WIDE>
     // end points as complex quad-doubles (octo-doubles for an octo-double
     // refinement), lower limbs zero below the refinement precision
     const int XL = RN::tr::limbs > 4 ? 8 : 4;
+    #pragma unroll 1
     for (int q = ctid(); q < n_max * 2 * XL; q += blockDim.x) {
       const int i = q / (2 * XL), c = q % (2 * XL);
       double v = 0.0;
@@ -515,6 +550,7 @@ static int track_launch(const TrackDev &S, const TrackParDev &P, int nmono_max, 
   const float *mdl = reinterpret_cast<const float *>(model);
   if (one_per_launch) {
     // the plain arrangement: one launch (one CTA) per path, back to back
+    #pragma unroll 1
     for (int p = 0; p < npaths; ++p) {
       kern<<<1, kTrackThreads, smem, st>>>(S, P, 1, p, path_sys, x0, nullptr, mdl, xend, info, dinfo, log, log_cap,
                                            log_count);
