@@ -456,6 +456,19 @@ __device__ TRACK_FN void hom_coef_cta(const TrackDev &S, int s, int k, double t0
   __syncthreads();
 }
 
+// Exact maximum over the warp of values that are non-negative (or -1 for
+// none, read as 0): doubles >= 0 order as their bit patterns, so two 32-bit
+// max reductions (redux.sync), over the high words and then over the low
+// words of the lanes that hold the largest high word, give the maximum
+// (two instructions in place of five rounds of shuffles).
+__device__ __forceinline__ double warp_max_nonneg(double v) {
+  const unsigned hi = (v >= 0.0) ? (unsigned)__double2hiint(v) : 0u;
+  const unsigned mhi = __reduce_max_sync(0xffffffffu, hi);
+  const unsigned lo = (v >= 0.0 && hi == mhi) ? (unsigned)__double2loint(v) : 0u;
+  const unsigned mlo = __reduce_max_sync(0xffffffffu, lo);
+  return __hiloint2double((int)mhi, (int)mlo);
+}
+
 // LU factorization with partial pivoting of the n x n matrix A (row-major,
 // shared memory, n <= 32), in place: lufac of
 // Math_Lib/Reduction/standard_complex_linear_solvers.adb:123-178 (LINPACK's
@@ -463,12 +476,17 @@ __device__ TRACK_FN void hom_coef_cta(const TrackDev &S, int s, int k, double t0
 // limbs), rows k and ell swap in columns k..n-1, and the multipliers
 // -a_ik / a_kk overwrite column k below the diagonal.  Besides ipvt the
 // reciprocals dinv[k] = 1 / u_kk are kept for the back substitution (NaN
-// for a zero pivot).  One warp alone (lanes over the rows for the pivot and
-// the multipliers, over the entries for the trailing update; a lane per row
-// with its row's columns in turn measured slower): no CTA barrier, the other
-// warps of the CTA stay free.  Called by all lanes of the warp;
-// returns info to every lane: 0, or k + 1 for the first column k without a
-// nonzero pivot.
+// for a zero pivot).  One warp alone, no CTA barrier (the other warps of the
+// CTA stay free).  Per column: lane i (k <= i < n) holds a_ik and forms its
+// reciprocal while the warp finds the largest candidate (warp_max_nonneg
+// and one ballot), so that 1 / a_kk is a shuffle away once the pivot row is
+// known; the rows swap (lanes over the columns); the (n-k-1)^2 entries of
+// the trailing update are spread over the lanes, each lane forming the
+// multiplier of its entry's row from column k; the multipliers are stored
+// last, a lane per row.  Every entry sees zgefa's operations in their order
+// (the results do not depend on the lane layout).  Called by all lanes of
+// the warp; returns info to every lane: 0, or k + 1 for the first column k
+// without a nonzero pivot.
 template <class N>
 __device__ TRACK_FN int warp_lufac(int n, double *A, int *ipvt, double *dinv) {
   typedef typename N::T T;
@@ -476,48 +494,64 @@ __device__ TRACK_FN int warp_lufac(int n, double *A, int *ipvt, double *dinv) {
   int info = 0;
   #pragma unroll 1
   for (int k = 0; k < n; ++k) {
+    const bool cand = lane >= k && lane < n;
+    T a = N::zero();
     double v = -1.0;
-    if (lane >= k && lane < n) {
-      v = N::lead(ldn_at<N>(A, (long)lane * n + k));
+    if (cand) {
+      a = ldn_at<N>(A, (long)lane * n + k);
+      v = N::lead(a);
       if (!(v == v)) v = INFINITY;  // a NaN pivot candidate reads as infinity
     }
+    const T r = cand ? N::div(N::one(), a) : N::zero();
     // the largest value, then the first row that holds it (one ballot)
-    double mx = v;
-    #pragma unroll 1
-    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-    const unsigned hold = __ballot_sync(0xffffffffu, lane >= k && lane < n && v == mx);
+    const double mx = warp_max_nonneg(v);
+    const unsigned hold = __ballot_sync(0xffffffffu, cand && v == mx);
     const int ix = hold ? __ffs(hold) - 1 : n;
-    v = mx;
     const int ell = ix < n ? ix : n - 1;
     if (lane == 0) ipvt[k] = ell;
-    if (v == 0.0) {
+    if (mx == 0.0) {
       if (info == 0) info = k + 1;  // this column is already triangularized
       if (lane == 0) stn_at<N>(dinv, k, N::from(NAN));
       __syncwarp();
       continue;
     }
+    const T inv = md::shfl(r, ell);
+    if (lane == 0) stn_at<N>(dinv, k, inv);
     if (ell != k)
       #pragma unroll 1
       for (int j = k + lane; j < n; j += 32) {
-        const T a = ldn_at<N>(A, (long)ell * n + j);
+        const T t = ldn_at<N>(A, (long)ell * n + j);
         stn_at<N>(A, (long)ell * n + j, ldn_at<N>(A, (long)k * n + j));
-        stn_at<N>(A, (long)k * n + j, a);
+        stn_at<N>(A, (long)k * n + j, t);
       }
+    // lane i's entry of column k after the swap (row ell holds the old row k)
+    const T ak = md::shfl(a, k);
+    const T ai = (lane == ell) ? ak : a;
+    const T ninv = N::neg(inv);
     __syncwarp();
-    const T inv = N::div(N::one(), ldn_at<N>(A, (long)k * n + k));
-    if (lane == 0) stn_at<N>(dinv, k, inv);
-    if (lane > k && lane < n) stn_at<N>(A, (long)lane * n + k, N::mul(N::neg(inv), ldn_at<N>(A, (long)lane * n + k)));
-    __syncwarp();
-    // trailing update, the (n-k-1)^2 entries spread over the lanes
+    // trailing update: entry (k+1+i, k+1+j) of the m x m block at e = i m + j
     const int m = n - k - 1;
-    #pragma unroll 1
-    for (int e = lane; e < m * m; e += 32) {
-      const int i = k + 1 + e / m, j = k + 1 + e % m;
-      const long o = (long)i * n + j;
-      stn_at<N>(A, o, N::add(ldn_at<N>(A, o), N::mul(ldn_at<N>(A, (long)k * n + j), ldn_at<N>(A, (long)i * n + k))));
+    if (m > 0) {
+      int i = lane / m, j = lane - (lane / m) * m;
+      const int qi = 32 / m, qj = 32 - (32 / m) * m;
+      #pragma unroll 1
+      for (int e = lane; e < m * m; e += 32) {
+        const long o = (long)(k + 1 + i) * n + (k + 1 + j);
+        const T mik = N::mul(ninv, ldn_at<N>(A, (long)(k + 1 + i) * n + k));
+        stn_at<N>(A, o, N::add(ldn_at<N>(A, o), N::mul(ldn_at<N>(A, (long)k * n + k + 1 + j), mik)));
+        i += qi;
+        j += qj;
+        if (j >= m) {
+          j -= m;
+          ++i;
+        }
+      }
     }
     __syncwarp();
+    // column k is not read again by this factorization
+    if (lane > k && lane < n) stn_at<N>(A, (long)lane * n + k, N::mul(ninv, ai));
   }
+  __syncwarp();
   return info;
 }
 
@@ -553,14 +587,32 @@ __device__ typename N::T warp_lusolve(int n, const double *A, const int *ipvt, c
 // M = A^{-1} from the factors of warp_lufac by one warp: lusolve applied to
 // the columns e_c of the identity, all columns at once, each substitution
 // step spread over the lanes (every entry sees the same operations in the
-// same order as a column-by-column solve).  Called by all lanes of one
-// warp; the caller synchronises before M is read by other warps.
+// same order as a column-by-column solve; an entry's row and column follow
+// from the previous pass's by adding 32 = qi n + qc, without divisions).
+// Called by all lanes of one warp; the caller synchronises before M is read
+// by other warps.
 template <class N>
 __device__ TRACK_FN void warp_luinverse(int n, const double *A, const int *ipvt, const double *dinv, double *M) {
   typedef typename N::T T;
   const int lane = threadIdx.x & 31;
-  #pragma unroll 1
-  for (int e = lane; e < n * n; e += 32) stn_at<N>(M, e, (e / n == e % n) ? N::one() : N::zero());
+  const int i0 = lane / n, c0 = lane - (lane / n) * n;  // entry e = i n + c of lane's first pass
+  const int qi = 32 / n, qc = 32 - (32 / n) * n;
+  auto next = [&](int &i, int &c) {
+    i += qi;
+    c += qc;
+    if (c >= n) {
+      c -= n;
+      ++i;
+    }
+  };
+  {
+    int i = i0, c = c0;
+    #pragma unroll 1
+    for (int e = lane; e < n * n; e += 32) {
+      stn_at<N>(M, e, (i == c) ? N::one() : N::zero());
+      next(i, c);
+    }
+  }
   __syncwarp();
   #pragma unroll 1
   for (int k = 0; k < n - 1; ++k) {  // L y = P e_c
@@ -574,11 +626,12 @@ __device__ TRACK_FN void warp_luinverse(int n, const double *A, const int *ipvt,
       }
     __syncwarp();
     const int m = n - k - 1;
+    int i = i0, c = c0;
     #pragma unroll 1
     for (int e = lane; e < m * n; e += 32) {
-      const int i = k + 1 + e / n, c = e % n;
-      const long o = (long)i * n + c;
-      stn_at<N>(M, o, N::add(ldn_at<N>(M, o), N::mul(ldn_at<N>(M, (long)k * n + c), ldn_at<N>(A, (long)i * n + k))));
+      const long o = (long)(k + 1 + i) * n + c;
+      stn_at<N>(M, o, N::add(ldn_at<N>(M, o), N::mul(ldn_at<N>(M, (long)k * n + c), ldn_at<N>(A, (long)(k + 1 + i) * n + k))));
+      next(i, c);
     }
     __syncwarp();
   }
@@ -588,11 +641,12 @@ __device__ TRACK_FN void warp_luinverse(int n, const double *A, const int *ipvt,
     for (int c = lane; c < n; c += 32)
       stn_at<N>(M, (long)kb * n + c, N::mul(ldn_at<N>(M, (long)kb * n + c), ldn_at<N>(dinv, kb)));
     __syncwarp();
+    int j = i0, c = c0;
     #pragma unroll 1
     for (int e = lane; e < kb * n; e += 32) {
-      const int j = e / n, c = e % n;
       const long o = (long)j * n + c;
       stn_at<N>(M, o, N::sub(ldn_at<N>(M, o), N::mul(ldn_at<N>(M, (long)kb * n + c), ldn_at<N>(A, (long)j * n + kb))));
+      next(j, c);
     }
     __syncwarp();
   }
@@ -1070,7 +1124,7 @@ __device__ TRACK_FN bool point_newton(const TrackDev &S, int s, int n, double t,
         if (!(m == m)) m = INFINITY;
         if (info == 0) stn_at<N>(x, lane, N::add(ldn_at<N>(x, lane), conv_num<JN, N>::go(v)));
       }
-      m = warp_max(m);
+      m = warp_max_nonneg(m);
       if (lane == 0) red[0] = info ? INFINITY : m;
     }
     __syncthreads();
@@ -1269,7 +1323,7 @@ __device__ TRACK_FN bool point_newton_split(const TrackDev &S, int s, int n, dou
           xj[lane] = to_d2(xn);
         }
       }
-      m = warp_max(m);
+      m = warp_max_nonneg(m);
       if (lane == 0) red[0] = info ? INFINITY : m;
     }
     __syncthreads();
