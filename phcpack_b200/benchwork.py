@@ -113,7 +113,7 @@ class EvalWork:
     kernel_tag = "k_system_evaldiff_config2"
     # DRAM bytes of one launch on the 4096 systems, from the ncu capture of
     # profiles/k_system_evaldiff_config2.md (512 systems, scaled by 8)
-    traffic_bytes_per_launch = 1.6408e10
+    traffic_bytes_per_launch = 1.0808e10
     l2_note = None
     dominant_launches_per_step = 1
 

@@ -62,7 +62,7 @@ class QRWork:
     kernel_tag = "k_bals_solve_qd64"
     # DRAM bytes of one launch on the 512 instances, from the ncu capture of
     # profiles/k_bals_solve_qd64.md (scaled to 512 instances)
-    traffic_bytes_per_launch = 3.7017e9
+    traffic_bytes_per_launch = 2.5731e9
     dominant_launches_per_step = 1
     l2_note = "inputs (2.1 GB of A_k) larger than L2"
 
