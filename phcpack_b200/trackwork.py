@@ -91,7 +91,7 @@ class TrackWork:
     kernel_tag = "k_track_config4"
     # DRAM bytes of one launch on the 1024 paths, from the ncu capture of
     # profiles/k_track_config4.md (dram__bytes_read.sum + dram__bytes_write.sum)
-    traffic_bytes_per_launch = 5.159e6
+    traffic_bytes_per_launch = 5.289e5
     dominant_launches_per_step = 1
 
     def __init__(self, torch, dev, rank, npaths=1024, tune=True):
@@ -312,6 +312,46 @@ def cpu_sample(seconds):
     _, info, _ = pyoracle.track(lib, sub, ipar, dpar, pmode=1, rmode=2, nthreads=cores)
     el = time.perf_counter() - t
     ok = int((info.reshape(-1, 6)[:, 0] == 0).sum())
-    return {"value": n / el, "unit": "paths/s", "cores": cores, "kind": "port",
-            "sample": f"{n} of the 1024 paths, {ok} successful, {cores} threads (std::thread), CPU: {model}; the "
-                      "reference's tracker is Ada (no GNAT here), so this is the C++ restatement"}
+    out = {"value": n / el, "unit": "paths/s", "cores": cores, "kind": "port",
+           "sample": f"{n} of the 1024 paths, {ok} successful, {cores} threads (std::thread), CPU: {model}; the "
+                     "reference's tracker is Ada (no GNAT here), so this is the C++ restatement"}
+    # the same restatement with the learned step (the GPU arm's algorithm):
+    # the ratio of the GPU arm to this one is the hardware alone
+    mdl = load_model_bytes()
+    if mdl is not None:
+        t = time.perf_counter()
+        _, info, _ = pyoracle.track(lib, sub, ipar, dpar, pmode=1, rmode=2, nthreads=cores, step_mode=1, model=mdl)
+        el = time.perf_counter() - t
+        out["learned_step_paths_per_s"] = n / el
+    cal = port_calibration()
+    if cal is not None:
+        out["calibration"] = cal
+    return out
+
+
+def port_calibration(reps=3):
+    """How fast the restatement's host code runs against PHCpack's own host
+    code on the same work: one complex double-double system of the eval/diff
+    workload (n = 32, degree 31) evaluated and differentiated by the oracle
+    (oracle/oracle_core.hpp, the code the CPU tracker is built on) and by the
+    reference's CPU_cmplx2_ routines (oracle/_ref), one thread each, best of
+    reps.  None where the reference's host code was not built."""
+    from oracle import pyoracle
+    from . import workloads as wl
+    ref = pyoracle.reference()
+    if ref is None:
+        return None
+    port = pyoracle.oracle()
+    b = wl.config2(nsys=1, seed=77)
+
+    def best(lib):
+        ts = []
+        for _ in range(reps):
+            t = time.perf_counter()
+            lib.system_evaldiff(b)
+            ts.append(time.perf_counter() - t)
+        return min(ts)
+
+    tp, tr = best(port), best(ref)
+    return {"work": "eval/diff of one complex double-double system (n=32, 32 monomials per polynomial, degree 31), "
+                    "one thread", "port_s": tp, "reference_s": tr, "port_time_over_reference_time": tp / tr}
