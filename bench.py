@@ -187,7 +187,7 @@ def main():
     if hasattr(work, "finish"):
         work.finish()
     # end to end through the host entry point (pinned host buffers in, results out)
-    e2e = work.e2e(stream, reps=max(1, min(3, args.steps)))
+    e2e = work.e2e(stream, reps=max(3, min(9, args.steps)))
     check = work.check()
 
     if dist is not None:
