@@ -233,6 +233,10 @@ def main():
     if args.workload == "track" and not args.no_blocks and world == 1:
         out["blocks"] = {name: benchwork.side_block(name, torch, dev, fp64, peaks.get("hbm_gbs"))
                          for name in ("eval", "qr")}
+        try:
+            out["blocks"]["newton_graph"] = benchwork.newton_graph_block(torch, dev)
+        except Exception as e:  # the block is informational; the line stands without it
+            out["blocks"]["newton_graph"] = {"error": str(e)[:200]}
     print(json.dumps(out), flush=True)
     return 0
 

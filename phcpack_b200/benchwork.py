@@ -253,6 +253,41 @@ def side_block(name, torch, dev, fp64_tflops, hbm_gbs, steps=3, warm=2):
     return out
 
 
+def newton_graph_block(torch, dev, nsteps=4, reps=20):
+    """The power-series Newton method on the shapes of the plain double-double
+    workload (one real system, n = 8, 8 monomials per polynomial over <= 3
+    variables, exponents {1, 2}, degree 15; 4 steps at fixed working degree
+    15, tile 8): a solve launched step by step against the same solve
+    captured once in a CUDA graph and replayed (newton.DeviceNewton), CUDA
+    events around each solve, median of reps; the replay's series must equal
+    the launched solve's bit for bit."""
+    from . import newton
+    b = wl.eval_batch(11, 1, 8, 15, 8, 3, 2, False, expmax=2)
+    dn = newton.DeviceNewton(b, szt=8, device=dev)
+    stream = torch.cuda.Stream(device=dev)
+
+    def timed(fn):
+        ts = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return float(np.median(ts))
+
+    t_eager = timed(lambda: dn.solve(nsteps, stream))
+    s_eager, _ = dn.result()
+    dn.capture(nsteps, stream)
+    t_graph = timed(lambda: dn.replay(stream))
+    s_graph, _ = dn.result()
+    return {"workload": "power-series Newton, one real double-double system n=8 (8 monomials over <=3 variables, "
+                        "exponents {1,2}), degree 15, 4 steps at fixed degree 15, tile 8",
+            "launched_ms_per_solve": t_eager, "graph_ms_per_solve": t_graph,
+            "graph_speedup": t_eager / t_graph, "same_series": bool(np.array_equal(s_eager, s_graph))}
+
+
 # ---------------------------------------------------------- CPU baseline
 def _threads_run(fn, nitems, nthreads):
     """Run fn(i) for i < nitems on nthreads Python threads (ctypes calls
