@@ -333,13 +333,15 @@ def eval_cpu_sample(seconds):
                       f"CPU: {model}"}
 
 
-def cpu_baseline(workload, seconds):
+def cpu_baseline(workload, seconds, extras=True):
+    """extras (track): also the learned-step restatement and the calibration
+    against the reference's host code."""
     try:
         if workload == "eval":
             return eval_cpu_sample(seconds)
         if workload == "track":
             from . import trackwork
-            return trackwork.cpu_sample(seconds)
+            return trackwork.cpu_sample(seconds, extras=extras)
         if workload == "qr":
             from . import qrwork
             return qrwork.cpu_sample(seconds)
@@ -354,8 +356,9 @@ def reference_arm(args):
     vals = []
     res = None
     per = max(2.0, min(20.0, 120.0 / max(1, args.steps + args.warmup)))
-    for k in range(args.warmup + args.steps):
-        res = cpu_baseline(args.workload, per)
+    nall = args.warmup + args.steps
+    for k in range(nall):
+        res = cpu_baseline(args.workload, per, extras=(k == nall - 1))
         if k >= args.warmup and res and res.get("value"):
             vals.append(res["value"])
     v = float(np.median(vals)) if vals else None

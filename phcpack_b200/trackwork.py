@@ -294,9 +294,10 @@ class TrackWork:
         return out
 
 
-def cpu_sample(seconds):
+def cpu_sample(seconds, extras=True):
     """The CPU tracker (oracle restatement of the Ada series-Pade tracker) on
-    a sample of the 1024 paths, all host cores."""
+    a sample of the 1024 paths, all host cores; with extras also the same
+    sample with the learned step and port_calibration()."""
     from oracle import pyoracle
     model, cores = cpu_info()
     pb = hm.config4()
@@ -317,6 +318,8 @@ def cpu_sample(seconds):
                      "reference's tracker is Ada (no GNAT here), so this is the C++ restatement"}
     # the same restatement with the learned step (the GPU arm's algorithm):
     # the ratio of the GPU arm to this one is the hardware alone
+    if not extras:
+        return out
     mdl = load_model_bytes()
     if mdl is not None:
         t = time.perf_counter()
