@@ -566,6 +566,9 @@ __device__ typename N::T warp_lusolve(int n, const double *A, const int *ipvt, c
                                       typename N::T v) {
   typedef typename N::T T;
   const int lane = threadIdx.x & 31;
+  // lane k's reciprocal pivot dinv[k], read once before the substitutions
+  // (off the dependent chain of the back substitution)
+  const T dl = (lane < n) ? ldn_at<N>(dinv, lane) : N::zero();
   #pragma unroll 1
   for (int k = 0; k < n - 1; ++k) {  // L y = P b
     const int ell = ipvt[k];
@@ -577,7 +580,7 @@ __device__ typename N::T warp_lusolve(int n, const double *A, const int *ipvt, c
   }
   #pragma unroll 1
   for (int kb = n - 1; kb >= 0; --kb) {  // U x = y
-    if (lane == kb) v = N::mul(v, ldn_at<N>(dinv, kb));
+    if (lane == kb) v = N::mul(v, dl);
     const T t = md::shfl(v, kb);
     if (lane < kb) v = N::sub(v, N::mul(t, ldn_at<N>(A, (long)lane * n + kb)));
   }
