@@ -69,7 +69,9 @@ int phc_tune_get(int knob);
  * output: nsys*dim*(dim+1) series; polynomial (s,p) occupies dim+1 series,
  *         series j < dim the derivative with respect to x_j, series dim the
  *         value (the reference's output[dim] convention).
- * Limit: deg <= 31. */
+ * Limit: deg <= 191 (the reference's largest degree); series of up to 32
+ * coefficients take one warp per product, longer ones a lane per
+ * coefficient (k, k + 32, ...). */
 int phc_system_evaldiff(int prec, int cplx, int nsys, int dim, int deg, int maxvar, const int *mon_off,
                         const int *nvr, const int *idx, const int *exps, const double *cst, const double *cff,
                         const double *input, double *output, void *stream);

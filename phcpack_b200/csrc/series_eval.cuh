@@ -236,4 +236,158 @@ __device__ void warp_poly_evaldiff(int dim, int deg, int maxvar, int m0, int m1,
     if (!((written >> r) & 1ull) && lane < n1) md::stn(out + r * S + lane * W, N::zero());
 }
 
+// ------------------------------------------------------- degrees 32..191
+// Series longer than a warp: each lane owns the coefficients k = lane,
+// lane + 32, ... of a product, each formed in the reference's order
+// x_0 y_k + x_1 y_{k-1} + ... + x_k y_0 (CPU_dbl2_product,
+// Convolutions/dbl2_convolutions_host.cpp:7); the lanes of a 32-coefficient
+// chunk differ by at most 32 terms.  Compiled once and called.
+template <class N>
+__device__ __noinline__ typename N::T conv_at(const double *x, const double *y, int k) {
+  typedef typename N::T T;
+  const int W = N::width;
+  T a = N::zero();
+  for (int i = 0; i <= k; ++i) {
+    T xi, yj;
+    md::ldn(x + i * W, xi);
+    md::ldn(y + (k - i) * W, yj);
+    a = N::add(a, N::mul(xi, yj));
+  }
+  return a;
+}
+
+// warp_poly_evaldiff for deg + 1 > 32 coefficients: the same monomial
+// method and the same outputs; the value accumulates in a series of the
+// warp's scratch (slot warp_slots(maxvar)), the products go through the
+// scratch coefficient by coefficient.
+template <class N>
+__device__ void warp_poly_evaldiff_big(int dim, int deg, int maxvar, int m0, int m1, const int *__restrict__ nvr,
+                                       const int *__restrict__ idx, const int *__restrict__ exps,
+                                       const double *__restrict__ cst, const double *__restrict__ cff,
+                                       const double *X,  // dim series (shared memory or global)
+                                       double *scr,      // shared: warp_slots(maxvar) + 1 series
+                                       double *out) {
+  typedef typename N::T T;
+  const int W = N::width;
+  const int n1 = deg + 1;
+  const int S = n1 * W;
+  const int lane = threadIdx.x & 31;
+  for (int r = 64; r < dim; ++r)
+    for (int k = lane; k < n1; k += 32) md::stn(out + r * S + k * W, N::zero());
+  unsigned long long written = 0ull;
+  auto first_touch = [&](int r) {
+    if (r >= 64) return false;
+    const bool f = !((written >> r) & 1ull);
+    written |= 1ull << r;
+    return f;
+  };
+  double *C = scr;
+  double *Tm = scr + S;
+  double *F = scr + 2 * S;                 // f_0 .. f_{k-2}
+  double *B = scr + (1 + maxvar) * S;      // b_0 .. b_{k-3}
+  double *Vs = scr + warp_slots(maxvar) * S;  // the value
+  for (int k = lane; k < n1; k += 32) {
+    T c;
+    md::ldn(cst + k * W, c);
+    md::stn(Vs + k * W, c);
+  }
+  // z = x y into the scratch series z (z is neither x nor y)
+  auto prod = [&](const double *x, const double *y, double *z) {
+    for (int k = lane; k < n1; k += 32) md::stn(z + k * W, conv_at<N>(x, y, k));
+    __syncwarp();
+  };
+  auto add_value = [&](const double *x, const double *y) {
+    for (int k = lane; k < n1; k += 32) {
+      const T z = conv_at<N>(x, y, k);
+      T v;
+      md::ldn(Vs + k * W, v);
+      md::stn(Vs + k * W, N::add(v, z));
+    }
+  };
+  // row += e x y (global memory; the first contribution is stored)
+  auto acc_prod = [&](double *row, const double *x, const double *y, int e, bool first) {
+    for (int k = lane; k < n1; k += 32) {
+      T z = conv_at<N>(x, y, k);
+      if (e > 1) z = N::scale_d(z, (double)e);
+      if (first) {
+        md::stn(row + k * W, z);
+      } else {
+        T v;
+        md::ldn(row + k * W, v);
+        md::stn(row + k * W, N::add(v, z));
+      }
+    }
+  };
+  // row += e src (src a scratch series)
+  auto acc_src = [&](double *row, const double *src, int e, bool first) {
+    for (int k = lane; k < n1; k += 32) {
+      T z;
+      md::ldn(src + k * W, z);
+      if (e > 1) z = N::scale_d(z, (double)e);
+      if (first) {
+        md::stn(row + k * W, z);
+      } else {
+        T v;
+        md::ldn(row + k * W, v);
+        md::stn(row + k * W, N::add(v, z));
+      }
+    }
+  };
+
+  for (int mon = m0; mon < m1; ++mon) {
+    const int k = nvr[mon];
+    const int *ix = idx + mon * maxvar;
+    const int *ex = exps + mon * maxvar;
+    bool ok = (k >= 1 && k <= maxvar);
+    for (int v = 0; ok && v < k; ++v) ok = (ix[v] >= 0 && ix[v] < dim && ex[v] >= 1);
+    if (!ok) continue;
+    for (int c = lane; c < n1; c += 32) {
+      T v;
+      md::ldn(cff + (long)mon * S + c * W, v);
+      md::stn(C + c * W, v);
+    }
+    __syncwarp();
+    // common factors: C <- x_v^(e_v - 1) * C
+    for (int v = 0; v < k; ++v)
+      for (int r = 1; r < ex[v]; ++r) {
+        prod(X + ix[v] * S, C, Tm);
+        double *t = C; C = Tm; Tm = t;
+      }
+    if (k == 1) {
+      add_value(X + ix[0] * S, C);
+      acc_src(out + ix[0] * S, C, ex[0], first_touch(ix[0]));
+    } else if (k == 2) {
+      prod(X + ix[0] * S, X + ix[1] * S, Tm);
+      add_value(Tm, C);
+      acc_prod(out + ix[1] * S, C, X + ix[0] * S, ex[1], first_touch(ix[1]));
+      acc_prod(out + ix[0] * S, C, X + ix[1] * S, ex[0], first_touch(ix[0]));
+    } else {
+      prod(C, X + ix[0] * S, F);
+      for (int i = 1; i < k - 1; ++i) prod(F + (i - 1) * S, X + ix[i] * S, F + i * S);
+      add_value(F + (k - 2) * S, X + ix[k - 1] * S);
+      acc_src(out + ix[k - 1] * S, F + (k - 2) * S, ex[k - 1], first_touch(ix[k - 1]));
+      prod(X + ix[k - 1] * S, X + ix[k - 2] * S, B);
+      for (int i = 1; i < k - 2; ++i) prod(B + (i - 1) * S, X + ix[k - 2 - i] * S, B + i * S);
+      prod(B + (k - 3) * S, C, Tm);  // b_{k-3} c: the derivative in x_0
+      acc_src(out + ix[0] * S, Tm, ex[0], first_touch(ix[0]));
+      if (k == 3) {
+        acc_prod(out + ix[1] * S, F, X + ix[2] * S, ex[1], first_touch(ix[1]));
+      } else {
+        for (int i = 0; i < k - 3; ++i)
+          acc_prod(out + ix[i + 1] * S, F + i * S, B + (k - 4 - i) * S, ex[i + 1], first_touch(ix[i + 1]));
+        acc_prod(out + ix[k - 2] * S, F + (k - 3) * S, X + ix[k - 1] * S, ex[k - 2], first_touch(ix[k - 2]));
+      }
+    }
+    __syncwarp();
+  }
+  for (int k = lane; k < n1; k += 32) {
+    T v;
+    md::ldn(Vs + k * W, v);
+    md::stn(out + dim * S + k * W, v);
+  }
+  for (int r = 0; r < dim && r < 64; ++r)
+    if (!((written >> r) & 1ull))
+      for (int k = lane; k < n1; k += 32) md::stn(out + r * S + k * W, N::zero());
+}
+
 }  // namespace phc

@@ -120,8 +120,20 @@ def test_eval_reference_shaped_single_polynomial():
     assert check_scaled(out, d["output"][:(b.dim + 1) * S], scale, 2, False, RTOL[2]) <= 1.0
 
 
+@pytest.mark.parametrize("deg,prec,cplx", [(32, 2, True), (47, 2, False), (63, 2, True), (100, 4, False),
+                                           (100, 1, True), (191, 2, True), (191, 4, True)])
+def test_eval_gpu_long_series_vs_oracle(deg, prec, cplx):
+    # series longer than a warp (the large-degree kernel), up to the
+    # reference's largest degree 191; exponents {1,2,3}, up to 4 variables
+    b = wl.eval_batch(200 + deg, 2, 6, deg, 5, 4, prec, cplx, expmax=3)
+    out = run_device(b)
+    ref = ORC.system_evaldiff(b)
+    scale = ORC.system_evaldiff(abs_batch(b))
+    assert check_scaled(out, ref, scale, prec, cplx, RTOL[prec]) <= 1.0
+
+
 def test_eval_rejects_degree_beyond_limit():
     from phcpack_b200._lib import PhcError
-    b = wl.eval_batch(1, 1, 3, 40, 2, 2, 2, False)
+    b = wl.eval_batch(1, 1, 3, 192, 2, 2, 2, False)
     with pytest.raises(PhcError):
         run_device(b)

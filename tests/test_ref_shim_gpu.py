@@ -17,7 +17,8 @@ from oracle import pyoracle
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("dim,nterms,deg,seed", [(8, 16, 15, 7), (16, 32, 31, 11), (32, 64, 31, 3)])
+@pytest.mark.parametrize("dim,nterms,deg,seed", [(8, 16, 15, 7), (16, 32, 31, 11), (32, 64, 31, 3), (8, 16, 63, 5),
+                                                   (8, 16, 191, 9)])
 def test_reference_tester_through_the_shim(dim, nterms, deg, seed):
     if not os.path.exists(pyoracle.SHIM_BIN):
         pytest.skip("the reference's test program was not built here")
@@ -160,7 +161,7 @@ def test_reference_quad_double_newton_tester_through_the_shim(cdata, dim, deg, p
     newton_tester("test_dbl4_newton", 1e-50, 1e-30, cdata, dim, deg, problem, extra, szt, nbt, nbsteps=12)
 
 
-@pytest.mark.parametrize("dim,nterms,deg,seed", [(8, 16, 15, 7), (16, 32, 31, 11)])
+@pytest.mark.parametrize("dim,nterms,deg,seed", [(8, 16, 15, 7), (16, 32, 31, 11), (8, 16, 100, 13)])
 def test_reference_quad_double_polynomial_tester_through_the_shim(dim, nterms, deg, seed):
     """PHCpack's test_dbl4_polynomials (Polynomials/, unchanged) with
     GPU_dbl4_poly_evaldiff, GPU_cmplx4_poly_evaldiff and
