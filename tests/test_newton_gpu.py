@@ -92,3 +92,14 @@ def test_newton_coefficients_equal_oracle_directly(prec, cplx, tol):
             first = 2 if prec == 2 else 1
             assert determined[:, :first].all(), eo[:, :first].max()
         assert (d[determined] <= tol * mag[determined]).all(), (nsteps, float((d / mag)[determined].max()))
+
+
+def test_newton_long_series_vs_oracle_known_answer():
+    # degree 63 (series longer than a warp in the evaluation): the
+    # reference's schedule reaches degree 63 in 11 steps; same skip-rule
+    # outcome as the oracle, errors within the criterion above
+    b, sol = exponential_test_system(9, 2, 8, 63, 8, 3, 2, False)
+    ser, fl = newton.newton_host(b, 12, szt=8, schedule=1)
+    so, flo = pyoracle.newton_steps(ORC, b, b.deg, 12, schedule=1)
+    assert np.array_equal(fl.reshape(-1, 5)[:, 4], flo.reshape(-1, 5)[:, 4])
+    assert check(ser, so, sol, 2, False, b.nsys, b.dim, b.deg + 1)
