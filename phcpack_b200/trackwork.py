@@ -91,7 +91,7 @@ class TrackWork:
     kernel_tag = "k_track_config4"
     # DRAM bytes of one launch on the 1024 paths, from the ncu capture of
     # profiles/k_track_config4.md (dram__bytes_read.sum + dram__bytes_write.sum)
-    traffic_bytes_per_launch = 5.289e5
+    traffic_bytes_per_launch = 5.716e5
     dominant_launches_per_step = 1
 
     def __init__(self, torch, dev, rank, npaths=1024, tune=True):
