@@ -5,7 +5,8 @@
 //
 // A persistent kernel: each CTA repeatedly takes the next path from an
 // on-device work queue (one atomicAdd; no waiting on other CTAs) and tracks
-// it from t = 0 to t = 1, so paths of uneven length balance across the SMs.
+// it from t = 0 to t = 1, so paths of uneven length balance across the SMs;
+// a batch that fits in one wave maps CTA b to path b instead.
 // Per step (the Ada Predictor_Corrector_Loop, predictor_corrector_loops.adb
 // :37-85, restated):
 //   predictor, in PN precision (double or double-double):
@@ -585,8 +586,12 @@ static int track_launch(const TrackDev &S, const TrackParDev &P, int nmono_max, 
   long grid = (long)nsm * per;
   if (grid > npaths) grid = npaths;
   if (grid < 1) return PHC_OK;
-  PHC_CUDA(cudaMemsetAsync(queue, 0, sizeof(int), st));
-  kern<<<(unsigned)grid, kTrackThreads, smem, st>>>(S, P, npaths, 0, path_sys, x0, queue, mdl, xend, info, dinfo, log,
+  // a batch that fits in one wave: CTA b tracks path b (the queue would
+  // balance nothing, and the fixed mapping makes the launch time steadier);
+  // otherwise the work queue hands out the paths as CTAs finish theirs
+  int *q = grid >= npaths ? nullptr : queue;
+  if (q) PHC_CUDA(cudaMemsetAsync(q, 0, sizeof(int), st));
+  kern<<<(unsigned)grid, kTrackThreads, smem, st>>>(S, P, npaths, 0, path_sys, x0, q, mdl, xend, info, dinfo, log,
                                                      log_cap, log_count);
   PHC_CHECK_LAUNCH();
   return PHC_OK;
