@@ -245,9 +245,10 @@ class TrackWork:
 
     def endpoint_errors(self, npaths=16):
         """The error of each result against FP64 and octo-double: end points
-        of a sample of paths against an octo-double run of the host oracle (same step rule; od refinement),
-        for the GPU's double-double end points and for an FP64 run of the
-        same tracker on the host (all double, corrector included)."""
+        of a sample of paths against an octo-double run of the host oracle
+        (same step rule; od refinement), for the GPU's double-double end
+        points and for an FP64 run of the same tracker on the host (all
+        double, corrector included)."""
         from oracle import pyoracle
         lib = pyoracle.oracle()
         sub = hm.subset(self.pb, np.arange(0, self.pb.npaths, self.pb.npaths // npaths)[:npaths])
