@@ -285,7 +285,7 @@ def newton_graph_block(torch, dev, nsteps=4, reps=20):
     return {"workload": "power-series Newton, one real double-double system n=8 (8 monomials over <=3 variables, "
                         "exponents {1,2}), degree 15, 4 steps at fixed degree 15, tile 8",
             "launched_ms_per_solve": t_eager, "graph_ms_per_solve": t_graph,
-            "graph_speedup": t_eager / t_graph, "same_series": bool(np.array_equal(s_eager, s_graph))}
+            "graph_speedup": t_eager / t_graph, "same_series": bool(np.array_equal(s_eager, s_graph, equal_nan=True))}
 
 
 # ---------------------------------------------------------- CPU baseline
